@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark: 2D radial acoustics, plain FP64, 4096^2 cells, t_final = 0.6.
+
+One "step" is one claw2 call over one output interval (dtout = t_final/20,
+the unit in which claw2ez hands the state back to the host), i.e. ~137
+time steps of the fused step2 kernel at 4096^2.  --steps 20 times the whole
+run from t=0 to t=0.6.  The metric is cell-updates/s: accepted time steps x
+cells / device time.
+
+  value    : state resident in HBM, frames driven through the library's
+             claw_advance (device-side dt control, CUDA-graph time loop)
+  e2e      : the same frames through claw_advance_host, i.e. with the
+             host->device copy of q (pinned) before and the device->host copy
+             after every frame inside the timed region
+  roofline : the step kernel's algorithmic bytes (read q + write q,
+             48 B per cell-update) / its average launch time, CUDA events on
+             the library's stream over the timed region
+  cpu_baseline : the CPU restatement of step2/flux2 (the oracle) timed on
+             this host on a bounded sample (whole 4096^2 steps)
+
+--impl reference times that CPU restatement alone on the same metric.
+Under torchrun with N > 1 each rank runs an independent replica (the
+north-star workload does not shard), value = all ranks' cell-updates / max
+time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 4096
+NOUT = 20
+TFINAL = 0.6
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return PEAKS_FALLBACK
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(n, nsteps):
+    """Time the CPU restatement (oracle, speed build) on nsteps whole n^2
+    steps of the workload; returns (cell-updates/s, seconds, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from classic_b200 import problems
+    from pyoracle import OracleGrid
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=n)
+    g = OracleGrid(rd.clawdata, solver, params, variant="fast")
+    g.set_q(q0)
+    dt = 0.9 * (2.0 / n) / 2.0
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        g.step(dt)
+    sec = time.perf_counter() - t0
+    return n * n * nsteps / sec, sec, 1
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    n = N_CELLS
+    for _ in range(args.warmup):
+        cpu_reference_sample(n, 1)
+    rates, secs = [], 0.0
+    for _ in range(args.steps):
+        r, s, cores = cpu_reference_sample(n, 1)
+        rates.append(r)
+        secs += s
+    value = n * n * args.steps / secs
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"2D radial acoustics FP64 {n}^2, MC, transverse 2",
+                   "step": f"one whole {n}^2 time step (bounded sample of a frame)"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} whole {n}^2 steps of the CPU restatement "
+                                   "(the reference's 2D step is serial)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=NOUT)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELLS)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t)
+        return float(t.item())
+
+    from classic_b200 import problems
+    from classic_b200.solver import Solver
+
+    n = args.n
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=n, nout=NOUT, tfinal=TFINAL)
+    cd = rd.clawdata
+    s = Solver(cd, solver, params, precision=args.precision)
+    cells = n * n
+    dtout = (TFINAL - 0.0) / float(np.float32(NOUT))
+
+    def frames(k, host_q=None):
+        """k claw2 calls (frames) from t=0; returns (accepted steps, kernel ms,
+        launches)."""
+        t, dt = 0.0, float(cd.dt_initial)
+        steps = launches = 0
+        kms = 0.0
+        for _ in range(k):
+            if host_q is None:
+                info, st = s.advance(t, t + dtout, dt)
+            else:
+                info, st = s.advance_host(host_q, t, t + dtout, dt)
+            if info != 0:
+                raise RuntimeError(f"advance info={info}")
+            t, dt = st["t_reached"], st["dt_next"]
+            steps += st["steps_taken"]
+            kms += st["device_ms"]
+            launches += st["launches"]
+        return steps, kms, launches
+
+    # ---- warm-up (then reset to the initial data)
+    s.set_q(q0)
+    frames(args.warmup)
+    s.set_q(q0)
+    torch.cuda.synchronize()
+    barrier()
+
+    # ---- timed region: device-resident state
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    steps, kms, launches = frames(args.steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    barrier()
+    ms_max = max_over_ranks(ms)
+    total_updates = sum_over_ranks(float(cells) * steps)
+    value = total_updates / (ms_max * 1e-3)
+
+    # ---- e2e: same frames with host q in / out per frame (pinned)
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(s.q_shape, dtype=torch.float64, pin_memory=True).numpy()
+        host[...] = q0
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        esteps, _, _ = frames(args.steps, host_q=host)
+        e1.record()
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        qbytes = 3 * cells * 8
+        e2e = {"value": sum_over_ranks(float(cells) * esteps) / (ems * 1e-3),
+               "unit": "cell-updates/s", "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,
+               "ms_per_step": ems / args.steps}
+
+    # ---- roofline of the step kernel (algorithmic bytes per launch)
+    es = 8 if args.precision == "fp64" else 4
+    bytes_per_launch = 2 * 3 * es * cells
+    per_launch_ms = kms / max(launches, 1)
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    peaks = load_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "step2_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(f"{args.precision}_{n}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                "peak_source": peaks["source"], "kernel": "step2_kernel",
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "avg_launch_ms": per_launch_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_steps > 0:
+        rate, sec, cores = cpu_reference_sample(n, args.cpu_steps)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_steps} whole {n}^2 steps of the CPU restatement "
+                         f"({sec:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+            "data": "synthetic",
+            "config": {"workload": f"2D radial acoustics {args.precision.upper()} {n}^2, "
+                                   "MC limiter, transverse 2, extrap BCs, t_final 0.6",
+                       "step": f"one claw2 call over dtout = {dtout:g} (~{steps / args.steps:.0f} "
+                               "time steps)",
+                       "time_steps_timed": steps, "cells": cells,
+                       "l2": "inputs larger than L2 (403 MB q per buffer)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

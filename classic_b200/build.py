@@ -1,0 +1,59 @@
+"""In-tree build of the CUDA library (sm_100a) and of the CPU oracle.
+
+``build_library()`` compiles classic_b200/csrc/claw_b200.cu with nvcc into
+classic_b200/libclawb200.so.  The FP64 path is built with --fmad=false so
+each multiply and add rounds separately, in the reference's operation order.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libclawb200.so")
+ARCH = "-gencode=arch=compute_100a,code=sm_100a"
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.sep not in cand or os.path.exists(cand)):
+            return cand
+    return "nvcc"
+
+
+def sources():
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)
+                  if f.endswith((".cu", ".cuh")))
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    hdr = os.path.join(os.path.dirname(HERE), "include", "claw_b200.h")
+    return all(os.path.getmtime(s) <= t for s in sources() + [hdr])
+
+
+def build_library(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    cmd = [_nvcc(), ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+           "-Xcompiler", "-fPIC", "-shared", "-o", LIB,
+           os.path.join(CSRC, "claw_b200.cu")]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_oracle():
+    root = os.path.dirname(HERE)
+    subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle")], check=True)
+
+
+if __name__ == "__main__":
+    build_library(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build_oracle()

@@ -1,0 +1,615 @@
+// Host side of the C ABI declared in include/claw_b200.h: device memory,
+// TMA descriptors, launch configuration, the CUDA-graph time loop and the
+// claw2-style argument checks.  Kernels live in step*d.cuh.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/claw_b200.h"
+#include "common.cuh"
+#include "riemann.cuh"
+#include "step1d.cuh"
+#include "step2d.cuh"
+
+using namespace clawb200;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(x)                                                                     \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(CLAW_E_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));      \
+    } while (0)
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult qr;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) ==
+                cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3D tiled map over an SoA array: dims (n0, n1, n2) with pitches p1, p2 (elements).
+int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, long long n2,
+              long long p1, long long p2, int box0, int box1, int box2) {
+    auto fn = encode_fn();
+    if (!fn) return fail(CLAW_E_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    const cuuint64_t dims[3] = {(cuuint64_t)n0, (cuuint64_t)n1, (cuuint64_t)n2};
+    const cuuint64_t strides[2] = {(cuuint64_t)(p1 * es), (cuuint64_t)(p2 * es)};
+    const cuuint32_t box[3] = {(cuuint32_t)box0, (cuuint32_t)box1, (cuuint32_t)box2};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                          3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(CLAW_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
+long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+struct Geometry {
+    int dim, mx, my, mz, meqn, maux, es;
+    long long ld, fstride, ald, afstride;  // pitches in elements
+    void* q[2];
+    void* aux;
+    ClawCtl* ctl;
+    double dx, dy, dz;
+};
+
+// ------------------------------------------------------------------ runners ---
+struct Runner {
+    virtual ~Runner() {}
+    virtual int prepare(const claw_config& cfg, const Geometry& g) = 0;
+    virtual cudaError_t launch(cudaStream_t s) = 0;
+};
+
+template <class S>
+struct Runner2D : Runner {
+    Step2Args<S> args;
+    int grid = 1, smem = 0;
+
+    explicit Runner2D(const S& s) { std::memset(&args, 0, sizeof(args)); args.solver = s; }
+
+    int prepare(const claw_config& cfg, const Geometry& g) override {
+        using R = Ring2D<S>;
+        args.q[0] = static_cast<typename S::real*>(g.q[0]);
+        args.q[1] = static_cast<typename S::real*>(g.q[1]);
+        args.aux = static_cast<const typename S::real*>(g.aux);
+        args.ld = g.ld;
+        args.fstride = g.fstride;
+        args.ald = g.ald;
+        args.afstride = g.afstride;
+        args.mx = g.mx;
+        args.my = g.my;
+        args.nstrips = (g.mx + STRIP - 1) / STRIP;
+        args.bc[0] = cfg.bc_lower[0];
+        args.bc[1] = cfg.bc_upper[0];
+        args.bc[2] = cfg.bc_lower[1];
+        args.bc[3] = cfg.bc_upper[1];
+        for (int k = 0; k < 8; ++k) args.mthlim[k] = k < cfg.num_waves ? cfg.limiter[k] : 0;
+        args.order = cfg.order;
+        args.trans = cfg.transverse_waves;
+        args.fwave = cfg.use_fwaves;
+        args.capa = cfg.capa_index;
+        args.dx = g.dx;
+        args.dy = g.dy;
+        args.ctl = g.ctl;
+        for (int k = 0; k < 2; ++k) {
+            int rc = make_map3(&args.tmq[k], g.q[k], g.es, g.mx, g.my, S::meqn, g.ld, g.fstride,
+                               R::W, 1, S::meqn);
+            if (rc) return rc;
+        }
+        if (S::maux > 0) {
+            int rc = make_map3(&args.tmaux, g.aux, g.es, g.mx + 4, g.my + 4, S::maux, g.ald,
+                               g.afstride, R::W, 1, S::maux);
+            if (rc) return rc;
+        }
+        smem = R::SMEM;
+        CUDA_TRY(cudaFuncSetAttribute(step2_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+        int dev = 0, nsm = 0, per_sm = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_kernel<S>,
+                                                               32 * WARPS2D, smem));
+        if (per_sm < 1) return fail(CLAW_E_CUDA, "step2 kernel cannot be resident on an SM");
+        args.units = (long long)args.nstrips * g.my;
+        // every warp gets at least ~48 rows of one strip so the 4-row march
+        // prologue stays a small fraction of its work
+        const long long want = std::max(1LL, args.units / 48);
+        const long long full = (long long)nsm * per_sm * WARPS2D;
+        const long long nw = std::min(full, want);
+        grid = (int)((nw + WARPS2D - 1) / WARPS2D);
+        args.nwarps = (int)nw;
+        return 0;
+    }
+
+    cudaError_t launch(cudaStream_t s) override {
+        step2_kernel<S><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        return cudaGetLastError();
+    }
+};
+
+template <class S>
+struct Runner1D : Runner {
+    Step1Args<S> args;
+    int smem = 0;
+
+    explicit Runner1D(const S& s) { std::memset(&args, 0, sizeof(args)); args.solver = s; }
+
+    int prepare(const claw_config& cfg, const Geometry& g) override {
+        args.q[0] = static_cast<typename S::real*>(g.q[0]);
+        args.q[1] = static_cast<typename S::real*>(g.q[1]);
+        args.aux = static_cast<const typename S::real*>(g.aux);
+        args.fstride = g.fstride;
+        args.afstride = g.afstride;
+        args.mx = g.mx;
+        args.bc[0] = cfg.bc_lower[0];
+        args.bc[1] = cfg.bc_upper[0];
+        for (int k = 0; k < 8; ++k) args.mthlim[k] = k < cfg.num_waves ? cfg.limiter[k] : 0;
+        args.order = cfg.order;
+        args.fwave = cfg.use_fwaves;
+        args.capa = cfg.capa_index;
+        args.dx = g.dx;
+        args.ctl = g.ctl;
+        smem = step1_smem_bytes<S>(g.mx);
+        if (smem > 200 * 1024)
+            return fail(CLAW_E_UNSUPPORTED, "1D grid of %d cells exceeds the single-CTA kernel", g.mx);
+        CUDA_TRY(cudaFuncSetAttribute(step1_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+        return 0;
+    }
+
+    cudaError_t launch(cudaStream_t s) override {
+        step1_kernel<S><<<1, STEP1_THREADS, smem, s>>>(args);
+        return cudaGetLastError();
+    }
+};
+
+template <typename real>
+std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
+    const int id = cfg.solver_id;
+    if (id == CLAW_SOLVER_ACOUSTICS_2D || id == CLAW_SOLVER_ACOUSTICS_1D) {
+        const double rho = cfg.solver_params[0], bulk = cfg.solver_params[1];
+        const double cc = std::sqrt(bulk / rho), zz = rho * cc, hz = 0.5 / zz;
+        if (id == CLAW_SOLVER_ACOUSTICS_2D) {
+            Acoustics2D<real> s{(real)cc, (real)zz, (real)hz};
+            return std::unique_ptr<Runner>(new Runner2D<Acoustics2D<real>>(s));
+        }
+        Acoustics1D<real> s{(real)cc, (real)zz, (real)hz};
+        return std::unique_ptr<Runner>(new Runner1D<Acoustics1D<real>>(s));
+    }
+    if (id == CLAW_SOLVER_VC_ADVECTION_2D)
+        return std::unique_ptr<Runner>(new Runner2D<VCAdvection2D<real>>(VCAdvection2D<real>{}));
+    if (id == CLAW_SOLVER_VC_ACOUSTICS_1D)
+        return std::unique_ptr<Runner>(new Runner1D<VCAcoustics1D<real>>(VCAcoustics1D<real>{}));
+    return nullptr;
+}
+
+struct SolverShape { int dim, meqn, mwaves, maux; };
+
+bool solver_shape(int id, SolverShape* sh) {
+    switch (id) {
+        case CLAW_SOLVER_ACOUSTICS_2D: *sh = {2, 3, 2, 0}; return true;
+        case CLAW_SOLVER_VC_ADVECTION_2D: *sh = {2, 1, 1, 3}; return true;
+        case CLAW_SOLVER_ACOUSTICS_1D: *sh = {1, 2, 2, 0}; return true;
+        case CLAW_SOLVER_VC_ACOUSTICS_1D: *sh = {1, 2, 2, 2}; return true;
+        default: return false;
+    }
+}
+
+__global__ void widen_to_double(const float* src, double* dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+__global__ void narrow_to_float(const double* src, float* dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+}  // namespace
+
+struct claw_handle {
+    claw_config cfg;
+    Geometry g;
+    int cur = 0;
+    cudaStream_t stream = nullptr;
+    ClawCtl* ctl_h = nullptr;  // pinned mirror
+    double* stage = nullptr;   // device staging (doubles) for FP32 conversion
+    std::unique_ptr<Runner> runner;
+    cudaGraphExec_t gexec = nullptr;
+    int gsteps = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    long long launches = 0;
+    int device = 0;
+};
+
+extern "C" {
+
+const char* claw_last_error(void) { return g_err.c_str(); }
+
+const char* claw_build_info(void) {
+    return "clawb200 sm_100a; fp64 path built with --fmad=false (reference operation order)";
+}
+
+static int validate(const claw_config* c, SolverShape* sh) {
+    if (!c) return fail(CLAW_E_INVALID, "null config");
+    if (!solver_shape(c->solver_id, sh)) return fail(CLAW_E_UNSUPPORTED, "solver %d is not built", c->solver_id);
+    if (c->num_dim != sh->dim) return fail(CLAW_E_INVALID, "num_dim %d does not match solver", c->num_dim);
+    if (c->num_eqn != sh->meqn || c->num_waves != sh->mwaves || c->num_aux != sh->maux)
+        return fail(CLAW_E_INVALID, "num_eqn/num_waves/num_aux (%d,%d,%d) do not match solver (%d,%d,%d)",
+                    c->num_eqn, c->num_waves, c->num_aux, sh->meqn, sh->mwaves, sh->maux);
+    if (c->num_ghost != 2) return fail(CLAW_E_INVALID, "num_ghost must be 2");
+    for (int d = 0; d < c->num_dim; ++d) {
+        if (c->num_cells[d] < 2) return fail(CLAW_E_INVALID, "num_cells[%d] must be >= 2", d);
+        if (!(c->upper[d] > c->lower[d])) return fail(CLAW_E_INVALID, "upper[%d] <= lower[%d]", d, d);
+        for (int side = 0; side < 2; ++side) {
+            const int b = side ? c->bc_upper[d] : c->bc_lower[d];
+            if (b == 0) return fail(CLAW_E_UNSUPPORTED, "user boundary conditions are not built");
+            if (b < 1 || b > 3) return fail(CLAW_E_INVALID, "bad boundary condition %d", b);
+            if (b == 3 && c->num_eqn < d + 2)
+                return fail(CLAW_E_INVALID, "wall BC needs a velocity component %d", d + 2);
+        }
+        if ((c->bc_lower[d] == 2) != (c->bc_upper[d] == 2))
+            return fail(CLAW_E_INVALID, "periodic BCs must be set on both sides");
+    }
+    if (c->order < 1 || c->order > 2) return fail(CLAW_E_INVALID, "order must be 1 or 2");
+    if (c->dimensional_split != 0) return fail(CLAW_E_UNSUPPORTED, "dimensional splitting is not built");
+    if (c->source_split != 0) return fail(CLAW_E_UNSUPPORTED, "source terms are not built");
+    if (c->capa_index < 0) return fail(CLAW_E_INVALID, "capa_index < 0");
+    for (int k = 0; k < c->num_waves; ++k)
+        if (c->limiter[k] < 0 || c->limiter[k] > 5) return fail(CLAW_E_INVALID, "invalid limiter %d", c->limiter[k]);
+    if (c->precision < CLAW_FP64 || c->precision > CLAW_FP32) return fail(CLAW_E_INVALID, "bad precision");
+    if (c->precision == CLAW_FP64_FMA) return fail(CLAW_E_UNSUPPORTED, "FMA variant is not built");
+    return 0;
+}
+
+int claw_create(const claw_config* cfg, claw_handle** out) {
+    if (!out) return fail(CLAW_E_INVALID, "null out");
+    *out = nullptr;
+    SolverShape sh;
+    int rc = validate(cfg, &sh);
+    if (rc) return rc;
+    std::unique_ptr<claw_handle> h(new claw_handle());
+    h->cfg = *cfg;
+    Geometry& g = h->g;
+    std::memset(&g, 0, sizeof(g));
+    g.dim = cfg->num_dim;
+    g.mx = cfg->num_cells[0];
+    g.my = g.dim >= 2 ? cfg->num_cells[1] : 1;
+    g.mz = g.dim >= 3 ? cfg->num_cells[2] : 1;
+    g.meqn = cfg->num_eqn;
+    g.maux = cfg->num_aux;
+    g.es = cfg->precision == CLAW_FP32 ? 4 : 8;
+    // dx = (xupper - xlower)/float(mx), src/2d/claw2ez.f:191-192
+    g.dx = (cfg->upper[0] - cfg->lower[0]) / (double)(float)g.mx;
+    g.dy = g.dim >= 2 ? (cfg->upper[1] - cfg->lower[1]) / (double)(float)g.my : 1.0;
+    g.dz = g.dim >= 3 ? (cfg->upper[2] - cfg->lower[2]) / (double)(float)g.mz : 1.0;
+    g.ld = g.dim == 1 ? g.mx : round_up(g.mx, 32);
+    g.fstride = g.ld * g.my * g.mz;
+    const int ax = g.mx + 4;
+    g.ald = g.dim == 1 ? ax : round_up(ax, 4);
+    g.afstride = g.ald * (g.dim >= 2 ? g.my + 4 : 1) * (g.dim >= 3 ? g.mz + 4 : 1);
+    CUDA_TRY(cudaGetDevice(&h->device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&h->ev0));
+    CUDA_TRY(cudaEventCreate(&h->ev1));
+    const size_t qbytes = (size_t)g.fstride * g.meqn * g.es;
+    for (int k = 0; k < 2; ++k) {
+        CUDA_TRY(cudaMalloc(&g.q[k], qbytes));
+        CUDA_TRY(cudaMemsetAsync(g.q[k], 0, qbytes, h->stream));
+    }
+    if (g.maux > 0) {
+        const size_t abytes = (size_t)g.afstride * g.maux * g.es;
+        CUDA_TRY(cudaMalloc(&g.aux, abytes));
+        CUDA_TRY(cudaMemsetAsync(g.aux, 0, abytes, h->stream));
+    }
+    CUDA_TRY(cudaMalloc(&g.ctl, sizeof(ClawCtl)));
+    CUDA_TRY(cudaMallocHost(&h->ctl_h, sizeof(ClawCtl)));
+    std::memset(h->ctl_h, 0, sizeof(ClawCtl));
+    h->ctl_h->done = 1;
+    CUDA_TRY(cudaMemcpyAsync(g.ctl, h->ctl_h, sizeof(ClawCtl), cudaMemcpyHostToDevice, h->stream));
+    if (g.es == 4) {
+        const size_t n = std::max((size_t)g.fstride * g.meqn, (size_t)g.afstride * g.maux);
+        CUDA_TRY(cudaMalloc(&h->stage, n * sizeof(double)));
+    }
+    h->runner = g.es == 8 ? make_runner<double>(*cfg) : make_runner<float>(*cfg);
+    if (!h->runner) return fail(CLAW_E_UNSUPPORTED, "no kernel for solver %d", cfg->solver_id);
+    rc = h->runner->prepare(*cfg, g);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    *out = h.release();
+    return 0;
+}
+
+int claw_destroy(claw_handle* h) {
+    if (!h) return 0;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    for (int k = 0; k < 2; ++k)
+        if (h->g.q[k]) cudaFree(h->g.q[k]);
+    if (h->g.aux) cudaFree(h->g.aux);
+    if (h->g.ctl) cudaFree(h->g.ctl);
+    if (h->stage) cudaFree(h->stage);
+    if (h->ctl_h) cudaFreeHost(h->ctl_h);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return 0;
+}
+
+// Copy a dense host field block [nfields][rows][width] to a pitched device array.
+static int copy_fields(claw_handle* h, void* dev, long long pitch_el, long long fpitch_el,
+                       const double* host, int nfields, long long width, long long rows,
+                       bool to_device) {
+    const Geometry& g = h->g;
+    if (g.es == 8) {
+        for (int m = 0; m < nfields; ++m) {
+            char* d = static_cast<char*>(dev) + (size_t)m * fpitch_el * 8;
+            const double* hp = host + (size_t)m * width * rows;
+            if (to_device)
+                CUDA_TRY(cudaMemcpy2DAsync(d, pitch_el * 8, hp, width * 8, width * 8, rows,
+                                           cudaMemcpyHostToDevice, h->stream));
+            else
+                CUDA_TRY(cudaMemcpy2DAsync(const_cast<double*>(hp), width * 8, d, pitch_el * 8,
+                                           width * 8, rows, cudaMemcpyDeviceToHost, h->stream));
+        }
+    } else {
+        // FP32 storage: stage as doubles on the device, convert there.
+        const long long n = (long long)nfields * fpitch_el;
+        for (int m = 0; m < nfields; ++m) {
+            double* sd = h->stage + (size_t)m * fpitch_el;
+            const double* hp = host + (size_t)m * width * rows;
+            if (to_device)
+                CUDA_TRY(cudaMemcpy2DAsync(sd, pitch_el * 8, hp, width * 8, width * 8, rows,
+                                           cudaMemcpyHostToDevice, h->stream));
+        }
+        if (to_device) {
+            narrow_to_float<<<592, 256, 0, h->stream>>>(h->stage, static_cast<float*>(dev), n);
+        } else {
+            widen_to_double<<<592, 256, 0, h->stream>>>(static_cast<const float*>(dev), h->stage, n);
+            for (int m = 0; m < nfields; ++m) {
+                const double* sd = h->stage + (size_t)m * fpitch_el;
+                double* hp = const_cast<double*>(host) + (size_t)m * width * rows;
+                CUDA_TRY(cudaMemcpy2DAsync(hp, width * 8, sd, pitch_el * 8, width * 8, rows,
+                                           cudaMemcpyDeviceToHost, h->stream));
+            }
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+    return 0;
+}
+
+int claw_set_q(claw_handle* h, const double* q) {
+    if (!h || !q) return fail(CLAW_E_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const Geometry& g = h->g;
+    int rc = copy_fields(h, g.q[h->cur], g.ld, g.fstride, q, g.meqn, g.mx, (long long)g.my * g.mz, true);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int claw_get_q(claw_handle* h, double* q) {
+    if (!h || !q) return fail(CLAW_E_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const Geometry& g = h->g;
+    int rc = copy_fields(h, g.q[h->cur], g.ld, g.fstride, q, g.meqn, g.mx, (long long)g.my * g.mz, false);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int claw_set_aux(claw_handle* h, const double* aux) {
+    if (!h || !aux) return fail(CLAW_E_INVALID, "null argument");
+    const Geometry& g = h->g;
+    if (g.maux == 0) return 0;
+    CUDA_TRY(cudaSetDevice(h->device));
+    const long long rows = (long long)(g.dim >= 2 ? g.my + 4 : 1) * (g.dim >= 3 ? g.mz + 4 : 1);
+    int rc = copy_fields(h, g.aux, g.ald, g.afstride, aux, g.maux, g.mx + 4, rows, true);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->cfg.capa_index > 0) {
+        // the reference stops on a non-positive capacity (src/1d/step1.f90:67-70)
+        const long long n = (long long)g.mx + 4;
+        const double* cap = aux + (size_t)(h->cfg.capa_index - 1) * n * rows;
+        for (long long i = 0; i < n * rows; ++i)
+            if (!(cap[i] > 0.0)) return fail(CLAW_E_INVALID, "capacity must be positive");
+    }
+    return 0;
+}
+
+static int push_ctl(claw_handle* h) {
+    CUDA_TRY(cudaMemcpyAsync(h->g.ctl, h->ctl_h, sizeof(ClawCtl), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+static int pull_ctl(claw_handle* h) {
+    CUDA_TRY(cudaMemcpyAsync(h->ctl_h, h->g.ctl, sizeof(ClawCtl), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int claw_step(claw_handle* h, double dt, double* cfl) {
+    if (!h) return fail(CLAW_E_INVALID, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    ClawCtl* c = h->ctl_h;
+    std::memset(c, 0, sizeof(ClawCtl));
+    c->mode = CTL_SINGLE;
+    c->dt = dt;
+    c->cur = h->cur;
+    c->maxn = 1;
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    CUDA_TRY(h->runner->launch(h->stream));
+    h->launches++;
+    rc = pull_ctl(h);
+    if (rc) return rc;
+    h->cur = c->cur;
+    if (cfl) *cfl = c->cfl_last;
+    if (c->err & CTL_ERR_TMA_TIMEOUT) return fail(CLAW_E_DEVICE, "device wait timed out");
+    return 0;
+}
+
+static int ensure_graph(claw_handle* h, int steps) {
+    if (h->gexec && h->gsteps == steps) return 0;
+    if (h->gexec) {
+        cudaGraphExecDestroy(h->gexec);
+        h->gexec = nullptr;
+    }
+    cudaGraph_t graph;
+    CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < steps; ++k) {
+        cudaError_t e = h->runner->launch(h->stream);
+        if (e != cudaSuccess) {
+            cudaStreamEndCapture(h->stream, &graph);
+            return fail(CLAW_E_CUDA, "launch during capture: %s", cudaGetErrorString(e));
+        }
+    }
+    CUDA_TRY(cudaStreamEndCapture(h->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&h->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(CLAW_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    h->gsteps = steps;
+    return 0;
+}
+
+int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, claw_stats* st) {
+    if (!h) return fail(CLAW_E_INVALID, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const claw_config& cfg = h->cfg;
+    ClawCtl* c = h->ctl_h;
+    std::memset(c, 0, sizeof(ClawCtl));
+    c->t = c->told = tstart;
+    c->tstart = tstart;
+    c->tend = tend;
+    c->dt = dt_initial;
+    c->dt_max = cfg.dt_max;
+    c->cfl_max = cfg.cfl_max;
+    c->cfl_desired = cfg.cfl_desired;
+    c->dtmin = c->dtmax = dt_initial;
+    c->mode = CTL_ADVANCE;
+    c->dt_variable = cfg.dt_variable ? 1 : 0;
+    c->cur = h->cur;
+    int maxn = cfg.steps_max;
+    int info = 0;
+    // argument checks of claw2 (src/2d/claw2.f:508-543)
+    if (!cfg.dt_variable) {
+        if (tend < tstart) maxn = 1;
+        else {
+            maxn = (int)std::lround((tend - tstart) / dt_initial);
+            if (std::fabs(maxn * dt_initial - (tend - tstart)) > 1e-5 * (tend - tstart)) info = 2;
+        }
+    }
+    if (!info && cfg.dt_variable && cfg.cfl_desired > cfg.cfl_max) info = 3;
+    if (!info && cfg.capa_index > cfg.num_aux) info = 5;
+    if (!info && cfg.order < cfg.transverse_waves && cfg.num_dim == 2) info = 6;
+    c->maxn = maxn;
+    c->done = (info != 0 || maxn == 0) ? 1 : 0;
+    if (!c->done && c->told + c->dt > tend && tstart < tend) c->dt = tend - c->told;
+    int rc = push_ctl(h);
+    if (rc) return rc;
+    const long long launches0 = h->launches;
+    CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+    if (!c->done) {
+        if (h->g.dim == 1) {
+            // the 1D kernel runs the whole time loop inside one launch
+            CUDA_TRY(h->runner->launch(h->stream));
+            h->launches++;
+            rc = pull_ctl(h);
+            if (rc) return rc;
+        } else {
+            // steps per graph chunk: one host check per chunk
+            const long long cells = (long long)h->g.mx * h->g.my * h->g.mz;
+            const int chunk = cells >= (1LL << 22) ? 8 : 32;
+            rc = ensure_graph(h, chunk);
+            if (rc) return rc;
+            for (;;) {
+                CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
+                h->launches += chunk;
+                rc = pull_ctl(h);
+                if (rc) return rc;
+                if (c->done) break;
+            }
+        }
+    }
+    CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+    CUDA_TRY(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->cur = c->cur;
+    if (!info && cfg.dt_variable && c->t < tend && c->n == maxn) info = 11;
+    if (!info && !cfg.dt_variable && c->cflmax_seen > cfg.cfl_max) info = 12;
+    if (c->err & CTL_ERR_TMA_TIMEOUT) info = CLAW_E_DEVICE;
+    else if (c->err & CTL_ERR_NAN_CFL) info = CLAW_E_NAN;
+    if (st) {
+        st->t_reached = c->t;
+        st->dt_min = c->dtmin;
+        st->dt_max_taken = c->dtmax;
+        st->dt_next = c->dt;
+        st->cfl_max_seen = c->cflmax_seen;
+        st->cfl_last = c->cfl_last;
+        st->steps_taken = c->n;
+        st->steps_rejected = c->nrej;
+        st->info = info;
+        st->device_error = c->err;
+        st->device_ms = ms;
+        st->launches = h->launches - launches0;
+    }
+    if (info < 0) return fail(info, "device error flags 0x%x", c->err);
+    return info;
+}
+
+int claw_advance_host(claw_handle* h, double* q, double tstart, double tend, double dt_initial,
+                      claw_stats* st) {
+    int rc = claw_set_q(h, q);
+    if (rc) return rc;
+    const int info = claw_advance(h, tstart, tend, dt_initial, st);
+    if (info < 0) return info;
+    rc = claw_get_q(h, q);
+    if (rc) return rc;
+    return info;
+}
+
+int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld, long long* fp) {
+    if (!h) return fail(CLAW_E_INVALID, "null handle");
+    if (ptr) *ptr = h->g.q[h->cur];
+    if (elem_bytes) *elem_bytes = h->g.es;
+    if (ld) *ld = h->g.ld;
+    if (fp) *fp = h->g.fstride;
+    return 0;
+}
+
+long long claw_launch_count(claw_handle* h) { return h ? h->launches : 0; }
+
+}  // extern "C"

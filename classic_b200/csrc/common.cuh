@@ -1,0 +1,195 @@
+// Shared device-side pieces of the wave-propagation kernels: the device
+// control block (time/dt/CFL state of the claw2-style time loop), mbarrier and
+// TMA helpers written directly in PTX for sm_100a, and the wave limiter.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clawb200 {
+
+// ----------------------------------------------------------- control block ---
+// Device-resident state of one claw2-style advance (src/2d/claw2.f:494-784).
+// Every step kernel reads dt / cur at entry; the last CTA to finish a step
+// folds the CFL maximum and runs the accept/reject + next-dt logic here, so a
+// whole time loop runs without a host round trip per step.
+struct ClawCtl {
+    double t, told, dt, tstart, tend;
+    double dt_max, cfl_max, cfl_desired;
+    double cflmax_seen, dtmin, dtmax, cfl_last;
+    unsigned long long cfl_bits;   // atomicMax target (bit pattern of a double >= 0)
+    unsigned int ctas_done;        // last-CTA counter, reset by the last CTA
+    int cur;                       // index of the buffer holding the current q
+    int n, maxn, nrej;             // accepted steps, step limit, rejected steps
+    int done, info;
+    int mode;                      // CTL_ADVANCE or CTL_SINGLE
+    int dt_variable;
+    int err;                       // device error flags (CTL_ERR_*)
+    int pad;
+};
+
+enum { CTL_ADVANCE = 0, CTL_SINGLE = 1 };
+
+// Boundary-condition codes (mthbc in claw.data).
+enum { BC_USER = 0, BC_EXTRAP = 1, BC_PERIODIC = 2, BC_WALL = 3 };
+enum { CTL_ERR_TMA_TIMEOUT = 1, CTL_ERR_NAN_CFL = 2 };
+
+// Controller step: identical decisions to claw2's main loop.  Runs in exactly
+// one thread after every CTA of the step has published its CFL maximum.
+__device__ __forceinline__ void ctl_finish_step(ClawCtl* c) {
+    const double cfl = __longlong_as_double((long long)atomicAdd(&c->cfl_bits, 0ull));
+    c->cfl_bits = 0ull;
+    c->ctas_done = 0u;
+    c->cfl_last = cfl;
+    if (c->mode == CTL_SINGLE) {
+        c->cur ^= 1;
+        return;
+    }
+    if (cfl != cfl) {  // NaN: stop instead of retrying forever
+        c->err |= CTL_ERR_NAN_CFL;
+        c->done = 1;
+        return;
+    }
+    c->t = c->told + c->dt;
+    if (cfl <= c->cfl_max) {
+        c->cflmax_seen = fmax(cfl, c->cflmax_seen);
+        c->cur ^= 1;
+        if (c->dt_variable) {
+            if (cfl == 0.0) c->dt = c->dt_max;
+            else c->dt = fmin(c->dt_max, c->dt * c->cfl_desired / cfl);
+            c->dtmin = fmin(c->dt, c->dtmin);
+            c->dtmax = fmax(c->dt, c->dtmax);
+        }
+        c->n += 1;
+        if (c->t >= c->tend || c->n >= c->maxn) {
+            c->done = 1;
+        } else {
+            c->told = c->t;
+            if (c->told + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->told;
+        }
+    } else {
+        c->t = c->told;
+        c->nrej += 1;
+        if (c->dt_variable) {
+            c->dt = fmin(c->dt_max, c->dt * c->cfl_desired / cfl);
+        } else {
+            c->cflmax_seen = fmax(cfl, c->cflmax_seen);
+            c->done = 1;
+        }
+    }
+}
+
+// Publish one CTA's CFL maximum and, in the last CTA, run the controller.
+// Call with all threads of the CTA; red must hold >= blockDim/32 doubles.
+__device__ __forceinline__ void cta_cfl_and_control(ClawCtl* ctl, double cfl, double* red) {
+    for (int off = 16; off > 0; off >>= 1) cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) red[warp] = cfl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        if (!(m > 0.0)) m = (m != m) ? m : 0.0;  // canonical +0, keep NaN
+        atomicMax(&ctl->cfl_bits, (unsigned long long)__double_as_longlong(m));
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->ctas_done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl_finish_step(ctl);
+            __threadfence();
+        }
+    }
+}
+
+// ----------------------------------------------------------- PTX helpers ---
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase: gives up after ~2 s of wall time and
+// reports failure instead of hanging the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 0u && globaltimer_ns() - t0 > 2000000000ull) return false;
+    }
+}
+
+// 3D tiled TMA load (no multicast): box -> shared memory, completion on bar.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            int w, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// ------------------------------------------------------------- limiter ---
+// Limiter function phi(r) of src/2d/inlinelimiter.f90:71-97
+// (1 minmod, 2 superbee, 3 van Leer, 4 MC, 5 Beam-Warming).
+template <typename real>
+__device__ __forceinline__ real phi_limiter(int meth, real r) {
+    const real zero = real(0), one = real(1), two = real(2);
+    switch (meth) {
+        case 1: return fmax(zero, fmin(one, r));
+        case 2: return fmax(fmax(zero, fmin(one, two * r)), fmin(two, r));
+        case 3: return (r + fabs(r)) / (one + fabs(r));
+        case 4: {
+            const real c = (one + r) / two;
+            return fmax(zero, fmin(fmin(c, two), two * r));
+        }
+        case 5: return r;
+        default: return one;
+    }
+}
+
+}  // namespace clawb200

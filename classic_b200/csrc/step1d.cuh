@@ -1,0 +1,250 @@
+// 1D wave-propagation path: the whole claw1 time loop in ONE persistent CTA.
+//
+// Reference: src/1d/step1.f90:4-170 (in-place Godunov update, limiter,
+// correction flux f), src/1d/bc1.f, src/1d/claw1.f:450-583 (time loop; the
+// next dt is chosen before the Courant check, unlike claw2).
+//
+// 1D grids in this code family are small (hundreds to ~2000 cells), so the
+// B200 shape is one CTA holding the grid, its ghost cells, the saved copy for
+// rejected steps and all interface quantities in shared memory; each time
+// step is four barrier-separated phases and the dt controller runs in thread
+// 0.  One launch replaces ~10^3 step launches and host round trips.
+#pragma once
+#include "common.cuh"
+
+namespace clawb200 {
+
+constexpr int STEP1_THREADS = 512;
+
+template <class S>
+struct Step1Args {
+    typename S::real* q[2];
+    const typename S::real* aux;  // [maux][mx+4]
+    long long fstride, afstride;
+    int mx;
+    int bc[2];
+    int mthlim[8];
+    int order, fwave, capa;
+    double dx;
+    ClawCtl* ctl;
+    S solver;
+};
+
+template <class S>
+__host__ __device__ constexpr int step1_smem_doubles(int mx) {
+    // q, saved q, aux, dtdx, per-interface wave/s/amdq/apdq/f, reduction
+    return (2 * S::meqn + S::maux + 1) * (mx + 4) +
+           (S::mwaves * S::meqn + S::mwaves + 3 * S::meqn) * (mx + 4) + 32;
+}
+
+template <class S>
+int step1_smem_bytes(int mx) {
+    return step1_smem_doubles<S>(mx) * (int)sizeof(typename S::real) + 64 * 8;
+}
+
+template <class S>
+__global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_constant__ Step1Args<S> A) {
+    using real = typename S::real;
+    constexpr int ME = S::meqn, MW = S::mwaves, MA = S::maux;
+    constexpr int MAX = MA > 0 ? MA : 1;
+    ClawCtl* ctl = A.ctl;
+    const int mx = A.mx, n = mx + 4;  // cell k (0-based) lives at k+2
+    const int ne = mx + 4;            // interface e in [-1, mx+1] lives at e+1
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    real* qs = reinterpret_cast<real*>(smem_raw);
+    real* qsave = qs + ME * n;
+    real* as = qsave + ME * n;
+    real* dtdx = as + MA * n;
+    real* wv = dtdx + n;            // [MW][ME][ne]
+    real* sv = wv + MW * ME * ne;   // [MW][ne]
+    real* amd = sv + MW * ne;       // [ME][ne]
+    real* apd = amd + ME * ne;
+    real* fl = apd + ME * ne;       // [ME][ne]
+    __shared__ double red[STEP1_THREADS / 32];
+    __shared__ double sh_dt, sh_cfl;
+    __shared__ int sh_state;  // 0 continue, 1 retry, 2 stop
+
+    const int tid = threadIdx.x;
+    const int cur = ctl->cur;
+    const real* qin = A.q[cur];
+    for (int i = tid; i < ME * mx; i += blockDim.x) {
+        const int m = i / mx, k = i % mx;
+        qs[m * n + k + 2] = qin[m * A.fstride + k];
+    }
+    for (int i = tid; i < MA * n; i += blockDim.x) as[i] = A.aux[(i / n) * A.afstride + (i % n)];
+    double t = ctl->t, dt = ctl->dt;
+    const double tstart = ctl->tstart, tend = ctl->tend;
+    const double dxd = A.dx;
+    bool limit = false;
+    for (int k = 0; k < MW; ++k) limit |= A.mthlim[k] != 0;
+    __syncthreads();
+
+    double cflmax = 0.0, dtmin = ctl->dtmin, dtmaxs = ctl->dtmax, cfl = 0.0;
+    int nacc = 0, nrej = 0;
+    bool stop = false;
+    const int maxn = ctl->maxn;
+    for (int step = 0; step < maxn && !stop; ++step) {
+        const double told = t;
+        if (told + dt > tend && tstart < tend) dt = tend - told;
+        for (int i = tid; i < ME * n; i += blockDim.x) qsave[i] = qs[i];
+        __syncthreads();
+        for (;;) {
+            t = told + dt;
+            // ---- bc1 (src/1d/bc1.f): ghosts -1,-2 and mx,mx+1; wall negates q(2)
+            if (tid < 4 * ME) {
+                const int side = tid / (2 * ME), r = tid % (2 * ME), ibc = 1 + r / ME, m = r % ME;
+                const int bcode = A.bc[side];
+                int dst, src;
+                if (side == 0) {
+                    dst = -ibc;
+                    src = bcode == BC_PERIODIC ? mx - ibc : (bcode == BC_WALL ? ibc - 1 : 0);
+                } else {
+                    dst = mx - 1 + ibc;
+                    src = bcode == BC_PERIODIC ? ibc - 1 : (bcode == BC_WALL ? mx - ibc : mx - 1);
+                }
+                real v = qs[m * n + src + 2];
+                if (bcode == BC_WALL && m == 1) v = -v;
+                qs[m * n + dst + 2] = v;
+            }
+            for (int k = tid; k < n; k += blockDim.x) {
+                if (A.capa > 0) dtdx[k] = (real)(dt / (dxd * (double)as[(A.capa - 1) * n + k]));
+                else dtdx[k] = (real)(dt / dxd);
+            }
+            __syncthreads();
+            // ---- rp1 at interfaces e = -1 .. mx+1 (src/1d/step1.f90:82) + CFL
+            double c_loc = 0.0;
+            for (int e = tid - 1; e <= mx + 1; e += blockDim.x) {
+                real qL[ME], qR[ME], aL[MAX], aR[MAX];
+                for (int m = 0; m < ME; ++m) { qL[m] = qs[m * n + e + 1]; qR[m] = qs[m * n + e + 2]; }
+                for (int k = 0; k < MA; ++k) { aL[k] = as[k * n + e + 1]; aR[k] = as[k * n + e + 2]; }
+                real w[MW][ME], s[MW], am[ME], ap[ME];
+                A.solver.rp1(qL, qR, aL, aR, w, s, am, ap);
+                for (int mw = 0; mw < MW; ++mw) {
+                    for (int m = 0; m < ME; ++m) wv[(mw * ME + m) * ne + e + 1] = w[mw][m];
+                    sv[mw * ne + e + 1] = s[mw];
+                }
+                for (int m = 0; m < ME; ++m) { amd[m * ne + e + 1] = am[m]; apd[m * ne + e + 1] = ap[m]; }
+                if (e >= 0 && e <= mx) {
+                    const double dR = (double)dtdx[e + 2], dL = (double)dtdx[e + 1];
+                    for (int mw = 0; mw < MW; ++mw)
+                        c_loc = fmax(fmax(c_loc, dR * (double)s[mw]), -dL * (double)s[mw]);
+                }
+            }
+            __syncthreads();
+            // ---- Godunov update of cells 0..mx-1 (in place) and the limited
+            //      correction flux f at interfaces 0..mx
+            for (int k = tid; k < mx; k += blockDim.x) {
+                const real d = dtdx[k + 2];
+                for (int m = 0; m < ME; ++m)
+                    qs[m * n + k + 2] = (qs[m * n + k + 2] - d * apd[m * ne + k + 1]) - d * amd[m * ne + k + 2];
+            }
+            if (A.order != 1) {
+                for (int e = tid; e <= mx; e += blockDim.x) {
+                    real w[MW][ME];
+                    for (int mw = 0; mw < MW; ++mw)
+                        for (int m = 0; m < ME; ++m) w[mw][m] = wv[(mw * ME + m) * ne + e + 1];
+                    if (limit) {
+                        for (int mw = 0; mw < MW; ++mw) {
+                            const int ml = A.mthlim[mw];
+                            if (ml == 0) continue;
+                            real nn = real(0), dl = real(0), dr = real(0);
+                            for (int m = 0; m < ME; ++m) {
+                                const real wl = wv[(mw * ME + m) * ne + e];
+                                const real wr = wv[(mw * ME + m) * ne + e + 2];
+                                nn = nn + w[mw][m] * w[mw][m];
+                                dr = dr + w[mw][m] * wr;
+                                dl = dl + wl * w[mw][m];
+                            }
+                            if (nn == real(0)) continue;
+                            const real r = (sv[mw * ne + e + 1] > real(0) ? dl : dr) / nn;
+                            const real ph = phi_limiter<real>(ml, r);
+                            for (int m = 0; m < ME; ++m) w[mw][m] = ph * w[mw][m];
+                        }
+                    }
+                    const real ave = real(0.5) * (dtdx[e + 1] + dtdx[e + 2]);
+                    real f[ME];
+                    for (int m = 0; m < ME; ++m) f[m] = real(0);
+                    for (int mw = 0; mw < MW; ++mw) {
+                        const real sm = sv[mw * ne + e + 1], as_ = fabs(sm);
+                        const real coef = A.fwave ? real(0.5) * copysign(real(1), sm) * (real(1) - as_ * ave)
+                                                  : real(0.5) * as_ * (real(1) - as_ * ave);
+                        for (int m = 0; m < ME; ++m) f[m] = f[m] + coef * w[mw][m];
+                    }
+                    for (int m = 0; m < ME; ++m) fl[m * ne + e + 1] = f[m];
+                }
+            }
+            // CFL reduction
+            for (int off = 16; off > 0; off >>= 1) c_loc = fmax(c_loc, __shfl_xor_sync(0xffffffffu, c_loc, off));
+            if ((tid & 31) == 0) red[tid >> 5] = c_loc;
+            __syncthreads();
+            if (A.order != 1) {
+                for (int k = tid; k < mx; k += blockDim.x) {
+                    const real d = dtdx[k + 2];
+                    for (int m = 0; m < ME; ++m)
+                        qs[m * n + k + 2] = qs[m * n + k + 2] - d * (fl[m * ne + k + 2] - fl[m * ne + k + 1]);
+                }
+            }
+            if (tid == 0) {
+                double cm = 0.0;
+                for (int w = 0; w < STEP1_THREADS / 32; ++w) cm = fmax(cm, red[w]);
+                sh_cfl = cm;
+                // claw1: choose the next dt first (src/1d/claw1.f:520-529) ...
+                double dtn = dt;
+                if (ctl->dt_variable) {
+                    if (cm > 0.0) {
+                        dtn = fmin(ctl->dt_max, dt * ctl->cfl_desired / cm);
+                        dtmin = fmin(dtn, dtmin);
+                        dtmaxs = fmax(dtn, dtmaxs);
+                    } else {
+                        dtn = ctl->dt_max;
+                    }
+                }
+                sh_dt = dtn;
+                // ... then check the Courant number (src/1d/claw1.f:533-554)
+                if (cm != cm) sh_state = 3;
+                else if (cm <= ctl->cfl_max) sh_state = 0;
+                else sh_state = ctl->dt_variable ? 1 : 2;
+            }
+            __syncthreads();
+            cfl = sh_cfl;
+            dt = sh_dt;
+            const int st = sh_state;
+            if (st == 0) {
+                cflmax = fmax(cfl, cflmax);
+                break;
+            }
+            t = told;
+            for (int i = tid; i < ME * n; i += blockDim.x) qs[i] = qsave[i];
+            __syncthreads();
+            if (st == 1) { ++nrej; continue; }
+            if (st == 3) { if (tid == 0) ctl->err |= CTL_ERR_NAN_CFL; stop = true; break; }
+            cflmax = fmax(cfl, cflmax);
+            stop = true;
+            break;
+        }
+        if (stop) break;
+        ++nacc;
+        if (t >= tend) break;
+        __syncthreads();
+    }
+    __syncthreads();
+    real* qout = A.q[cur ^ 1];
+    for (int i = tid; i < ME * mx; i += blockDim.x) {
+        const int m = i / mx, k = i % mx;
+        qout[m * A.fstride + k] = qs[m * n + k + 2];
+    }
+    if (tid == 0) {
+        ctl->t = t;
+        ctl->dt = dt;
+        ctl->cflmax_seen = cflmax;
+        ctl->cfl_last = cfl;
+        ctl->dtmin = dtmin;
+        ctl->dtmax = dtmaxs;
+        ctl->n = nacc;
+        ctl->nrej = nrej;
+        ctl->cur = cur ^ 1;
+        ctl->done = 1;
+    }
+}
+
+}  // namespace clawb200

@@ -1,0 +1,198 @@
+"""Problem setups: the reference examples that carry regression pins, and the
+synthetic workloads (seeded or analytic initial data of the stated shapes).
+
+Each builder returns ``(rundata, solver, params, q0, aux)`` with q0 in the
+SoA interior layout [meqn][my][mx] and aux (or None) as [maux][my+4][mx+4].
+Cell centres follow the reference's qinit: x_i = xlower + (i - 0.5)*dx for
+1-based i.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .data import ClawRunData
+
+
+def _centres(lower, upper, n, ghost=0):
+    dx = (upper - lower) / float(np.float32(n))
+    i = np.arange(1 - ghost, n + ghost + 1, dtype=np.float64)
+    return lower + (i - 0.5) * dx, dx
+
+
+# ------------------------------------------------------------------- 1D ---
+def acoustics_1d_example1(mx=400, beta=200.0, nout=2, tfinal=1.0, output_t0=False):
+    """examples/acoustics_1d_example1 (setrun.py, qinit.f90, setprob.f90) with
+    the regression test's overrides (test_acoustics_1d_example1.py:17-19)."""
+    rd = ClawRunData("classic", 1)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("rho", 1.0)
+    pd.add_param("K", 4.0)
+    pd.add_param("beta", beta)
+    cd = rd.clawdata
+    cd.lower[0], cd.upper[0], cd.num_cells[0] = -1.0, 1.0, mx
+    cd.num_eqn, cd.num_aux, cd.capa_index = 2, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = output_t0
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 0.1, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 500
+    cd.order, cd.num_waves, cd.limiter = 2, 2, ["mc", "mc"]
+    cd.bc_lower[0], cd.bc_upper[0] = "extrap", "extrap"
+    x, _ = _centres(-1.0, 1.0, mx)
+    q0 = np.zeros((2, mx))
+    q0[0] = np.exp(-beta * (x - 0.3) ** 2)
+    return rd, "acoustics_1d", {"rho": 1.0, "bulk": 4.0}, q0, None
+
+
+def acoustics_1d_config(mx=800, nout=10, tfinal=1.0):
+    """1D linear acoustics workload: rho=1, K=4, [-1,1], p0=exp(-100(x-0.3)^2),
+    u0=0, order 2, MC, cfl 0.9, wall left / extrapolation right, 10 outputs
+    to t=1 (dt_initial 0.1 as in the reference example)."""
+    rd, solver, params, _, _ = acoustics_1d_example1(mx=mx, beta=100.0, nout=nout, tfinal=tfinal)
+    rd.clawdata.bc_lower[0] = "wall"
+    rd.clawdata.output_t0 = True
+    x, _ = _centres(-1.0, 1.0, mx)
+    q0 = np.zeros((2, mx))
+    q0[0] = np.exp(-100.0 * (x - 0.3) ** 2)
+    rd.clawdata.steps_max = 5000
+    return rd, solver, params, q0, None
+
+
+def acoustics_1d_heterogeneous(mx=500, nout=2, tfinal=5.0, ic=1, beta=5.0):
+    """examples/acoustics_1d_heterogeneous (setrun.py, qinit.f, setaux.f,
+    setprob.f) with the test's overrides (test_acoustics_1d_heterogeneous.py:23-25)."""
+    rd = ClawRunData("classic", 1)
+    cd = rd.clawdata
+    cd.lower[0], cd.upper[0], cd.num_cells[0] = -5.0, 5.0, mx
+    cd.num_eqn, cd.num_aux, cd.capa_index = 2, 2, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = False
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 1.0, 1e9
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.num_waves, cd.limiter = 2, 2, [4, 4]
+    cd.bc_lower[0], cd.bc_upper[0] = "extrap", "extrap"
+    rhol, cl, rhor, cr = 1.0, 1.0, 4.0, 0.5
+    zl, zr = rhol * cl, rhor * cr
+    x, _ = _centres(-5.0, 5.0, mx)
+    q0 = np.zeros((2, mx))
+    if ic == 1:
+        inside = (x > -4.0) & (x < -2.0)
+        q0[0] = np.where(inside, np.sqrt(np.where(inside, 1.0 - (x + 3.0) ** 2, 0.0)), 0.0)
+    elif ic == 2:
+        q0[0] = np.where(x < -2.0, 1.0, 0.0)
+    else:
+        g = np.exp(-beta * (x + 2.0) ** 2)
+        g[np.abs(g) < 1e-30] = 0.0
+        q0[0] = g + np.where((x > -4.0) & (x < -3.0), 0.5, 0.0)
+    q0[1] = q0[0]
+    xg, _ = _centres(-5.0, 5.0, mx, ghost=2)
+    aux = np.zeros((2, mx + 4))
+    aux[0] = np.where(xg < 0.0, zl, zr)
+    aux[1] = np.where(xg < 0.0, cl, cr)
+    return rd, "vc_acoustics_1d", {}, q0, aux
+
+
+# ------------------------------------------------------------------- 2D ---
+def radial_acoustics_2d(n=1024, nout=20, tfinal=0.6, limiter="mc", dt_initial=0.01):
+    """2D radial acoustics workload: rho=1, K=4 on [-1,1]^2 with n^2 cells;
+    p0 = 1 + cos(pi (r-0.5)/0.1) for |r-0.5| < 0.1 else 1, u=v=0; order 2,
+    transverse_waves 2, MC limiter, cfl 0.9, extrapolation BCs, t_final 0.6.
+    (examples/acoustics_2d_radial is the same solver with a narrower pulse.)"""
+    rd = ClawRunData("classic", 2)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("rho", 1.0)
+    pd.add_param("bulk", 4.0)
+    cd = rd.clawdata
+    cd.lower, cd.upper, cd.num_cells = [-1.0, -1.0], [1.0, 1.0], [n, n]
+    cd.num_eqn, cd.num_aux, cd.capa_index = 3, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, dt_initial, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.transverse_waves, cd.dimensional_split = 2, 2, "unsplit"
+    cd.num_waves, cd.limiter = 2, [limiter, limiter]
+    cd.bc_lower, cd.bc_upper = ["extrap", "extrap"], ["extrap", "extrap"]
+    x, _ = _centres(-1.0, 1.0, n)
+    X, Y = np.meshgrid(x, x, indexing="xy")  # [j][i]
+    r = np.sqrt(X * X + Y * Y)
+    q0 = np.zeros((3, n, n))
+    q0[0] = np.where(np.abs(r - 0.5) < 0.1, 1.0 + np.cos(np.pi * (r - 0.5) / 0.1), 1.0)
+    return rd, "acoustics_2d", {"rho": 1.0, "bulk": 4.0}, q0, None
+
+
+def advection_2d_annulus(mx=40, my=120, nout=2, tfinal=0.5):
+    """examples/advection_2d_annulus (setrun.py, qinit.f, setaux.f, mapc2p.f,
+    stream.f) with the test's overrides (test_advection_2d_annulus.py:16-17):
+    polar grid r in [0.2,1], theta in [0,2pi], capacity = cell area / (dr dtheta),
+    edge velocities from differences of the stream function pi*(x^2+y^2)."""
+    rd = ClawRunData("classic", 2)
+    cd = rd.clawdata
+    cd.lower, cd.upper, cd.num_cells = [0.2, 0.0], [1.0, 2.0 * np.pi], [mx, my]
+    cd.num_eqn, cd.num_aux, cd.capa_index = 1, 3, 3
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 0.1, 1e9
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.transverse_waves, cd.dimensional_split = 2, "all", "unsplit"
+    cd.num_waves, cd.limiter = 1, ["vanleer"]
+    cd.bc_lower, cd.bc_upper = ["extrap", "periodic"], ["extrap", "periodic"]
+    xlo, ylo = 0.2, 0.0
+    dxc = (1.0 - 0.2) / float(np.float32(mx))
+    dyc = (2.0 * np.pi - 0.0) / float(np.float32(my))
+
+    def mapc2p(xc, yc):
+        return xc * np.cos(yc), xc * np.sin(yc)
+
+    def stream(x, y):
+        return 3.1415926535897931 * (x ** 2 + y ** 2)
+
+    ig = np.arange(-1, mx + 3, dtype=np.float64)  # 1-based i = -1 .. mx+2
+    jg = np.arange(-1, my + 3, dtype=np.float64)
+    XC1 = xlo + (ig[None, :] - 1.0) * dxc
+    YC1 = ylo + (jg[:, None] - 1.0) * dyc
+    XC1, YC1 = np.broadcast_arrays(XC1, YC1)
+    xp1, yp1 = mapc2p(XC1, YC1)
+    xp2, yp2 = mapc2p(XC1, YC1 + dyc)
+    xp3, yp3 = mapc2p(XC1 + dxc, YC1 + dyc)
+    xp4, yp4 = mapc2p(XC1 + dxc, YC1)
+    aux = np.zeros((3, my + 4, mx + 4))
+    aux[0] = (stream(xp2, yp2) - stream(xp1, yp1)) / dyc
+    aux[1] = -(stream(xp4, yp4) - stream(xp1, yp1)) / dxc
+    xs = [xp1, xp2, xp3, xp4, xp1]
+    ys = [yp1, yp2, yp3, yp4, yp1]
+    area = np.zeros_like(xp1)
+    for k in range(4):
+        area = area + 0.5 * (ys[k] + ys[k + 1]) * (xs[k + 1] - xs[k])
+    aux[2] = area / (dxc * dyc)
+    x = xlo + (np.arange(1, mx + 1) - 0.5) * dxc
+    y = ylo + (np.arange(1, my + 1) - 0.5) * dyc
+    XC, YC = np.meshgrid(x, y, indexing="xy")
+    xp, yp = mapc2p(XC, YC)
+    A1, b1, x1, y1 = 1.0, 40.0, -0.5, 0.0
+    A2, b2, x2, y2 = -1.0, 40.0, 0.5, 0.0
+    q0 = np.zeros((1, my, mx))
+    q0[0] = (A1 * np.exp(-b1 * ((xp - x1) ** 2 + (yp - y1) ** 2))
+             + A2 * np.exp(-b2 * ((xp - x2) ** 2 + (yp - y2) ** 2)))
+    return rd, "vc_advection_2d", {}, q0, aux
+
+
+def random_acoustics_2d(mx, my, seed=0, bc=("extrap", "extrap", "extrap", "extrap"),
+                        limiter="mc", order=2, trans=2, nout=1, tfinal=0.05):
+    """Seeded random 2D acoustics state (smooth + noise) for parity tests on
+    ragged sizes and every boundary-condition kind."""
+    rng = np.random.default_rng(seed)
+    rd, solver, params, _, _ = radial_acoustics_2d(n=8, nout=nout, tfinal=tfinal)
+    cd = rd.clawdata
+    cd.num_cells = [mx, my]
+    cd.bc_lower = [bc[0], bc[2]]
+    cd.bc_upper = [bc[1], bc[3]]
+    cd.limiter = [limiter, limiter]
+    cd.order = order
+    cd.transverse_waves = trans
+    x, _ = _centres(-1.0, 1.0, mx)
+    y, _ = _centres(-1.0, 1.0, my)
+    X, Y = np.meshgrid(x, y, indexing="xy")
+    q0 = np.zeros((3, my, mx))
+    q0[0] = 1.0 + np.exp(-20.0 * ((X - 0.2) ** 2 + (Y + 0.1) ** 2)) + 0.1 * rng.standard_normal((my, mx))
+    q0[1] = 0.2 * rng.standard_normal((my, mx))
+    q0[2] = 0.2 * rng.standard_normal((my, mx))
+    return rd, solver, params, q0, None

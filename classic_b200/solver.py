@@ -1,0 +1,249 @@
+"""Host-side mirror of the reference's driver layer.
+
+``Solver`` wraps one handle of the C ABI (include/claw_b200.h): the device
+state of one grid plus the claw2 analogue ``advance``.  ``run`` is the
+claw{1,2}ez frame loop (src/2d/claw2ez.f:265-324): tend accumulates
+``dtout`` per frame, the last dt of a frame seeds the next (dtv(1)=dtv(5),
+src/2d/claw2ez.f:290), and each output frame applies out2's in-place flush
+of |q| < 1e-99 (src/2d/out2.f:70) before the run continues.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import ClawConfig, ClawStats, SOLVER_IDS, PRECISIONS, check
+from .data import ClawInputData, ClawRunData
+
+# Problem parameters each solver reads (the setprob values), in C order.
+SOLVER_PARAMS = {
+    "acoustics_2d": ("rho", "bulk"),
+    "acoustics_1d": ("rho", "bulk"),
+    "euler_roe_2d": ("gamma",),
+    "vc_advection_2d": (),
+    "vc_acoustics_1d": (),
+    "vc_acoustics_3d": (),
+}
+
+
+def make_config(cd: ClawInputData, solver: str, params: dict | None = None,
+                precision: str = "fp64") -> ClawConfig:
+    """Map clawdata + solver choice onto the C ``claw_config``."""
+    if solver not in SOLVER_IDS:
+        raise ValueError(f"unknown solver {solver!r}; built: {sorted(SOLVER_IDS)}")
+    params = params or {}
+    c = ClawConfig()
+    nd = int(cd.num_dim)
+    c.num_dim = nd
+    for d in range(3):
+        c.num_cells[d] = int(cd.num_cells[d]) if d < nd else 1
+        c.lower[d] = float(cd.lower[d]) if d < nd else 0.0
+        c.upper[d] = float(cd.upper[d]) if d < nd else 1.0
+    c.num_eqn = int(cd.num_eqn)
+    c.num_waves = int(cd.num_waves)
+    c.num_aux = int(cd.num_aux)
+    c.capa_index = int(cd.capa_index)
+    c.dt_variable = 1 if cd.dt_variable else 0
+    c.order = int(cd.order)
+    c.transverse_waves = cd.transverse_code() if nd > 1 else 0
+    c.dimensional_split = cd.split_code() if nd > 1 else 0
+    c.verbosity = int(cd.verbosity)
+    c.source_split = cd.source_code()
+    c.use_fwaves = 1 if cd.use_fwaves else 0
+    lim = cd.limiter_codes()
+    if len(lim) != c.num_waves:
+        raise ValueError(f"{len(lim)} limiters for {c.num_waves} waves")
+    for k, v in enumerate(lim):
+        c.limiter[k] = v
+    c.num_ghost = int(cd.num_ghost)
+    lo, hi = cd.bc_codes()
+    for d in range(3):
+        c.bc_lower[d] = lo[d] if d < nd else 1
+        c.bc_upper[d] = hi[d] if d < nd else 1
+    c.dt_initial = float(cd.dt_initial)
+    c.dt_max = float(cd.dt_max)
+    c.cfl_max = float(cd.cfl_max)
+    c.cfl_desired = float(cd.cfl_desired)
+    c.steps_max = int(cd.steps_max)
+    c.solver_id = SOLVER_IDS[solver]
+    for k, name in enumerate(SOLVER_PARAMS.get(solver, ())):
+        if name not in params:
+            raise ValueError(f"solver {solver} needs parameter {name!r}")
+        c.solver_params[k] = float(params[name])
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    c.precision = PRECISIONS[precision]
+    return c
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """Device state of one grid and the step / advance entry points."""
+
+    def __init__(self, clawdata, solver: str, params: dict | None = None,
+                 precision: str = "fp64"):
+        if isinstance(clawdata, ClawRunData):
+            clawdata = clawdata.clawdata
+        self.lib = _lib.load()
+        self.clawdata = clawdata
+        self.solver = solver
+        self.precision = precision
+        self.cfg = make_config(clawdata, solver, params, precision)
+        self.ndim = self.cfg.num_dim
+        self.meqn = self.cfg.num_eqn
+        self.maux = self.cfg.num_aux
+        cells = [self.cfg.num_cells[d] for d in range(self.ndim)]
+        self.q_shape = (self.meqn,) + tuple(reversed(cells))
+        self.aux_shape = (self.maux,) + tuple(n + 4 for n in reversed(cells))
+        h = ctypes.c_void_p()
+        check(self.lib.claw_create(ctypes.byref(self.cfg), ctypes.byref(h)), "claw_create")
+        self._h = h
+
+    # -- state --------------------------------------------------------------
+    def set_q(self, q: np.ndarray):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        if q.shape != self.q_shape:
+            raise ValueError(f"q shape {q.shape} != {self.q_shape}")
+        check(self.lib.claw_set_q(self._h, _dptr(q)), "claw_set_q")
+
+    def get_q(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.q_shape, dtype=np.float64)
+        check(self.lib.claw_get_q(self._h, _dptr(out)), "claw_get_q")
+        return out
+
+    def set_aux(self, aux: np.ndarray):
+        aux = np.ascontiguousarray(aux, dtype=np.float64)
+        if aux.shape != self.aux_shape:
+            raise ValueError(f"aux shape {aux.shape} != {self.aux_shape}")
+        check(self.lib.claw_set_aux(self._h, _dptr(aux)), "claw_set_aux")
+
+    # -- stepping -----------------------------------------------------------
+    def step(self, dt: float) -> float:
+        """One step of length dt (bc2 + step2); returns the Courant number."""
+        cfl = ctypes.c_double(0.0)
+        check(self.lib.claw_step(self._h, float(dt), ctypes.byref(cfl)), "claw_step")
+        return cfl.value
+
+    def advance(self, tstart: float, tend: float, dt_initial: float):
+        """claw2: advance with dt control; returns (info, stats dict)."""
+        st = ClawStats()
+        info = check(self.lib.claw_advance(self._h, float(tstart), float(tend),
+                                           float(dt_initial), ctypes.byref(st)), "claw_advance")
+        return info, st.as_dict()
+
+    def advance_host(self, q: np.ndarray, tstart: float, tend: float, dt_initial: float):
+        """The whole claw2 call on a host array (q in, q out, in place)."""
+        if q.dtype != np.float64 or not q.flags.c_contiguous or q.shape != self.q_shape:
+            raise ValueError("q must be a C-contiguous float64 array of the grid's shape")
+        st = ClawStats()
+        info = check(self.lib.claw_advance_host(self._h, _dptr(q), float(tstart), float(tend),
+                                                float(dt_initial), ctypes.byref(st)),
+                     "claw_advance_host")
+        return info, st.as_dict()
+
+    def launch_count(self) -> int:
+        return int(self.lib.claw_launch_count(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.claw_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+@dataclass
+class Frame:
+    frame: int
+    t: float
+    q: np.ndarray
+    stats: dict = field(default_factory=dict)
+
+
+def frame_times(cd: ClawInputData):
+    """(nout, nstepout, tend generator) of claw2ez's output loop."""
+    style = int(cd.output_style)
+    if style == 1:
+        return int(cd.num_output_times), 1
+    if style == 2:
+        return len(cd.output_times), 1
+    if style == 3:
+        return int(cd.total_steps), int(cd.output_step_interval)
+    raise ValueError(f"bad output_style {style}")
+
+
+def run(rundata, solver: str, params: dict | None, q0: np.ndarray,
+        aux: np.ndarray | None = None, precision: str = "fp64",
+        on_frame: Callable[[Frame], None] | None = None, keep_frames: bool = True,
+        flush_tiny: bool = True, solver_obj: Solver | None = None):
+    """claw{1,2}ez's frame loop on the GPU.  Returns the list of frames
+    (frame 0 included when output_t0); raises on a nonzero info."""
+    cd = rundata.clawdata if isinstance(rundata, ClawRunData) else rundata
+    s = solver_obj or Solver(cd, solver, params, precision)
+    q = np.array(q0, dtype=np.float64, copy=True)
+    if flush_tiny:
+        q[np.abs(q) < 1e-99] = 0.0
+    s.set_q(q)
+    if aux is not None:
+        s.set_aux(aux)
+    frames = []
+    t0 = float(cd.t0)
+    if cd.output_t0 or int(cd.output_style) == 2:
+        f0 = Frame(0, t0, q.copy())
+        if on_frame:
+            on_frame(f0)
+        if keep_frames:
+            frames.append(f0)
+    nout, nstepout = frame_times(cd)
+    # dtout = (tfinal - t0)/float(nout), src/2d/claw2ez.f:197-199
+    dtout = (float(cd.tfinal) - t0) / float(np.float32(nout)) if int(cd.output_style) == 1 else None
+    tend = t0
+    dt = float(cd.dt_initial)
+    for n in range(1, nout + 1):
+        tstart = tend
+        style = int(cd.output_style)
+        if style == 1:
+            tend = tstart + dtout
+        elif style == 2:
+            tend = float(cd.output_times[n - 1])
+        else:
+            tend = tstart - 1.0
+        info, st = s.advance(tstart, tend, dt)
+        if info != 0:
+            raise RuntimeError(f"claw advance returned info={info} (stats {st})")
+        dt = st["dt_next"]
+        tend = st["t_reached"]
+        iframe = n // nstepout
+        if iframe * nstepout == n:
+            q = s.get_q()
+            if flush_tiny:
+                tiny = np.abs(q) < 1e-99
+                if tiny.any():
+                    q[tiny] = 0.0
+                    s.set_q(q)
+            fr = Frame(iframe, tend, q, st)
+            if on_frame:
+                on_frame(fr)
+            if keep_frames:
+                frames.append(fr)
+    if solver_obj is None:
+        s.close()
+    return frames

@@ -1,0 +1,162 @@
+/*
+ * claw_b200.h — C ABI of the B200-native Clawpack Classic wave-propagation
+ * step.  Plain C types only; every function returns an int status:
+ *
+ *     0        success
+ *     2..12    the reference's claw2 info codes (src/2d/claw2.f:288-310):
+ *              2  fixed dt does not divide (tend - tstart)
+ *              3  cfl_desired > cfl_max with variable dt
+ *              5  capa_index > num_aux
+ *              6  transverse_waves > order
+ *              11 too many time steps (steps_max reached before tend)
+ *              12 Courant number too large with fixed dt
+ *     < 0      CLAW_E_* below (invalid argument, CUDA failure, ...)
+ *
+ * Arrays crossing this boundary are host arrays in structure-of-arrays order:
+ *     q   : [num_eqn][mz][my][mx]          interior cells only, C order
+ *     aux : [num_aux][mz+4][my+4][mx+4]    two ghost layers on every side
+ * (1D / 2D drop the absent dimensions.)  The reference's arrays are the
+ * Fortran q(meqn, 1-mbc:mx+mbc, 1-mbc:my+mbc): the same values, equation
+ * index fastest and ghost cells included; ghost cells of q are produced by
+ * the boundary conditions inside the step, exactly as bc2 fills them.
+ *
+ * A handle owns its device memory and is tied to one CUDA device and one
+ * stream; calls on one handle are not reentrant (the reference's step2 /
+ * claw2 are not reentrant either, through their COMMON blocks).
+ */
+#ifndef CLAW_B200_H
+#define CLAW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLAW_MAX_WAVES 8
+
+/* Riemann solver plugins (compile-time device functors implementing the
+ * rpn2/rpt2 contract of src/2d/claw2.f:312-404 in pointwise form). */
+enum claw_solver_id {
+    CLAW_SOLVER_ACOUSTICS_2D = 1,    /* q=(p,u,v); params: rho, bulk            */
+    CLAW_SOLVER_VC_ADVECTION_2D = 2, /* q=(q); aux=(u edge, v edge, capa)       */
+    CLAW_SOLVER_EULER_ROE_2D = 3,    /* q=(rho,rhou,rhov,E); params: gamma      */
+    CLAW_SOLVER_ACOUSTICS_1D = 11,   /* q=(p,u); params: rho, bulk              */
+    CLAW_SOLVER_VC_ACOUSTICS_1D = 12,/* q=(p,u); aux=(Z,c)                      */
+    CLAW_SOLVER_VC_ACOUSTICS_3D = 21 /* q=(p,u,v,w); aux=(Z,c)                  */
+};
+
+/* Arithmetic of the Riemann/limiter/update path. */
+enum claw_precision {
+    CLAW_FP64 = 0,      /* every multiply and add rounded separately: same
+                           operation order as the reference, bit-identical to
+                           the CPU restatement                                  */
+    CLAW_FP64_FMA = 1,  /* fused multiply-add allowed (within 1e-12 relative)  */
+    CLAW_FP32 = 2       /* FP32 update; CFL / dt / time stay FP64              */
+};
+
+enum claw_error {
+    CLAW_E_INVALID = -1,     /* invalid configuration or argument            */
+    CLAW_E_CUDA = -2,        /* CUDA runtime failure (see claw_last_error)   */
+    CLAW_E_UNSUPPORTED = -3, /* valid for the reference, not built here      */
+    CLAW_E_DEVICE = -4,      /* device-side wait gave up (no hang)           */
+    CLAW_E_NAN = -5          /* Courant number is NaN                        */
+};
+
+/* Mirror of the clawdata fields of ClawRunData that reach claw2ez
+ * (src/2d/claw2ez.f:39-156); integer codes as claw.data stores them. */
+typedef struct claw_config {
+    int num_dim;              /* 1, 2 or 3                                         */
+    int num_cells[3];         /* mx, my, mz                                        */
+    double lower[3];          /* xlower, ylower, zlower                            */
+    double upper[3];          /* xupper, yupper, zupper                            */
+    int num_eqn;              /* meqn                                              */
+    int num_waves;            /* mwaves                                            */
+    int num_aux;              /* maux  (method(7))                                 */
+    int capa_index;           /* method(6), 1-based, 0 = none                      */
+    int dt_variable;          /* method(1)                                         */
+    int order;                /* method(2): 1 or 2                                 */
+    int transverse_waves;     /* method(3): 0,1,2 (2D); 0,10,11,20,21,22 (3D)      */
+    int dimensional_split;    /* 0 unsplit (only unsplit is built)                 */
+    int verbosity;            /* method(4)                                         */
+    int source_split;         /* method(5): 0 (source terms are not built)         */
+    int use_fwaves;
+    int limiter[CLAW_MAX_WAVES]; /* mthlim: 0 none,1 minmod,2 superbee,3 vanleer,4 MC,5 BW */
+    int num_ghost;            /* mbc, must be 2                                    */
+    int bc_lower[3];          /* mthbc: 0 user, 1 extrap, 2 periodic, 3 wall       */
+    int bc_upper[3];
+    double dt_initial;        /* dtv(1)                                            */
+    double dt_max;            /* dtv(2)                                            */
+    double cfl_max;           /* cflv(1)                                           */
+    double cfl_desired;       /* cflv(2)                                           */
+    int steps_max;            /* nv(1)                                             */
+    int solver_id;            /* enum claw_solver_id                               */
+    double solver_params[8];  /* problem parameters of the solver (setprob)        */
+    int precision;            /* enum claw_precision                               */
+    int reserved[7];
+} claw_config;
+
+/* What claw2 returns through dtv / cflv / nv (src/2d/claw2.f:776-781). */
+typedef struct claw_stats {
+    double t_reached;         /* tend on return (time actually reached)            */
+    double dt_min;            /* dtv(3)                                            */
+    double dt_max_taken;      /* dtv(4)                                            */
+    double dt_next;           /* dtv(5): dt to start the next call with            */
+    double cfl_max_seen;      /* cflv(3)                                           */
+    double cfl_last;          /* cflv(4)                                           */
+    int steps_taken;          /* nv(2)                                             */
+    int steps_rejected;
+    int info;
+    int device_error;
+    double device_ms;         /* device time of the call (CUDA events on the
+                                 handle's stream), host copies excluded           */
+    long long launches;       /* step-kernel launches issued by the call          */
+} claw_stats;
+
+typedef struct claw_handle claw_handle;
+
+/* Allocate device state for one grid.  Replaces the allocation of q, aux and
+ * work in claw2ez (src/2d/claw2ez.f:182-263). */
+int claw_create(const claw_config* cfg, claw_handle** out);
+int claw_destroy(claw_handle* h);
+
+/* Copy the interior of q from / to the host (pageable or pinned).  Replaces
+ * qinit's fill of q (src/2d/claw2ez.f:244) and the read of q by out2. */
+int claw_set_q(claw_handle* h, const double* q);
+int claw_get_q(claw_handle* h, double* q);
+/* aux with its two ghost layers, as setaux fills it (src/2d/claw2ez.f:224). */
+int claw_set_aux(claw_handle* h, const double* aux);
+
+/* One step of length dt from the current q, ghost cells from the boundary
+ * conditions: bc2 + copyq2 + step2 (src/2d/claw2.f:622-668,
+ * src/2d/step2.f90:2-251).  Writes the Courant number to *cfl and makes the
+ * new q current; no accept/reject. */
+int claw_step(claw_handle* h, double dt, double* cfl);
+
+/* Advance from tstart to tend with claw2's variable/fixed dt control,
+ * rejection and retry (src/2d/claw2.f:494-784; src/1d/claw1.f:394-583 in
+ * 1D).  dt_initial plays dtv(1); the returned stats carry dtv/cflv/nv. */
+int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial,
+                 claw_stats* stats);
+
+/* claw_set_q + claw_advance + claw_get_q: the whole claw2 call on host arrays
+ * (q in, q out), as claw2ez makes it once per output frame. */
+int claw_advance_host(claw_handle* h, double* q, double tstart, double tend,
+                      double dt_initial, claw_stats* stats);
+
+/* Device view of the current q (for zero-copy users): pointer, element size,
+ * row pitch and field pitch in elements. */
+int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld,
+                  long long* field_pitch);
+
+/* Number of step-kernel launches issued on this handle so far. */
+long long claw_launch_count(claw_handle* h);
+
+/* Last error message of the calling thread ("" if none). */
+const char* claw_last_error(void);
+
+/* Library / build identification. */
+const char* claw_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLAW_B200_H */

@@ -1,0 +1,22 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def cuda_lib():
+    """The in-tree CUDA library, built if it is missing (nvcc cross-compiles
+    without a GPU)."""
+    from classic_b200 import build
+    build.build_library()
+    from classic_b200 import _lib
+    return _lib.load()

@@ -1,0 +1,25 @@
+"""Shared helpers for the parity tests (oracle = the CPU restatement)."""
+import numpy as np
+
+
+def e26(q):
+    """Round to the 16 significant digits Fortran e26.16 writes."""
+    f = np.vectorize(lambda v: float(f"{v:.15e}"))
+    return f(np.asarray(q, dtype=np.float64))
+
+
+def rel_diff(a, b):
+    """Normwise relative difference per field: max|a-b| / max|b|."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    out = []
+    for m in range(a.shape[0]):
+        den = np.max(np.abs(b[m]))
+        num = np.max(np.abs(a[m] - b[m]))
+        out.append(num / den if den > 0 else num)
+    return np.array(out)
+
+
+def same(a, b):
+    """Bit-for-bit value equality (+0 == -0), NaN never equal."""
+    return bool(np.array_equal(np.asarray(a), np.asarray(b)))

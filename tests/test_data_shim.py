@@ -1,0 +1,67 @@
+"""The ClawRunData drop-in: string codes, claw.data round trip, and the
+reference examples' unchanged setrun.py files (when the reference tree is
+present in this checkout)."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from classic_b200 import data
+from classic_b200.solver import make_config
+
+REF = "/root/reference/examples"
+
+
+def test_codes_and_config():
+    rd = data.ClawRunData("classic", 2)
+    cd = rd.clawdata
+    cd.limiter = ["mc", "vanleer"]
+    cd.num_waves = 2
+    cd.bc_lower = ["wall", "periodic"]
+    cd.bc_upper = ["extrap", "periodic"]
+    cd.transverse_waves = "all"
+    cfg = make_config(cd, "acoustics_2d", {"rho": 1.0, "bulk": 4.0})
+    assert list(cfg.limiter)[:2] == [4, 3]
+    assert list(cfg.bc_lower)[:2] == [3, 2] and list(cfg.bc_upper)[:2] == [1, 2]
+    assert cfg.transverse_waves == 2 and cfg.solver_id == 1
+    with pytest.raises(ValueError):
+        cd.limiter = ["nope", "mc"]
+        make_config(cd, "acoustics_2d", {"rho": 1.0, "bulk": 4.0})
+
+
+def test_claw_data_round_trip(tmp_path):
+    rd = data.ClawRunData("classic", 2)
+    cd = rd.clawdata
+    cd.num_cells = [40, 120]
+    cd.lower, cd.upper = [0.2, 0.0], [1.0, 6.283185307179586]
+    cd.num_aux, cd.capa_index = 3, 3
+    cd.limiter, cd.num_waves = ["vanleer"], 1
+    cd.bc_lower, cd.bc_upper = ["extrap", "periodic"], ["extrap", "periodic"]
+    p = rd.new_UserData("probdata", "setprob.data")
+    p.add_param("A1", 1.0, "amplitude")
+    rd.write(str(tmp_path))
+    back = data.read_claw_data(str(tmp_path / "claw.data"))
+    assert back.num_cells == [40, 120]
+    assert back.lower == [0.2, 0.0] and back.upper[1] == 6.283185307179586
+    assert back.limiter == [3] and back.bc_lower == [1, 2] and back.bc_upper == [1, 2]
+    assert back.capa_index == 3 and back.num_aux == 3
+    assert "A1" in (tmp_path / "setprob.data").read_text()
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.parametrize("example", ["acoustics_1d_example1", "acoustics_1d_heterogeneous",
+                                     "acoustics_2d_radial", "advection_2d_annulus",
+                                     "acoustics_3d_heterogeneous", "advection_1d_example1",
+                                     "euler_1d_wcblast"])
+def test_reference_setrun_runs_unchanged(example, tmp_path):
+    data.install_clawutil_alias()
+    path = os.path.join(REF, example, "setrun.py")
+    spec = importlib.util.spec_from_file_location(f"setrun_{example}", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    rd = mod.setrun("classic")
+    rd.write(str(tmp_path))
+    back = data.read_claw_data(str(tmp_path / "claw.data"))
+    assert back.num_cells == list(rd.clawdata.num_cells)
+    assert back.limiter == rd.clawdata.limiter_codes()

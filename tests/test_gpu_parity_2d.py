@@ -1,0 +1,162 @@
+"""2D step / advance on the GPU against the CPU oracle, through the C ABI.
+
+The FP64 path is built with separately rounded multiplies and adds in the
+reference's order of operations, so the comparison is bit-for-bit (value
+equality, +0 == -0) for q, the Courant number and the dt sequence."""
+import numpy as np
+import pytest
+
+from classic_b200 import problems
+from classic_b200.solver import Solver
+from helpers import rel_diff, same
+from pyoracle import OracleGrid
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(7, 5), (29, 31), (57, 100), (130, 67), (3, 64), (64, 2)]
+BCS = [("extrap", "extrap", "extrap", "extrap"),
+       ("wall", "wall", "wall", "wall"),
+       ("periodic", "periodic", "periodic", "periodic"),
+       ("wall", "extrap", "periodic", "periodic"),
+       ("periodic", "periodic", "extrap", "wall")]
+
+
+def _pair(rd, solver, params, q0, aux=None, precision="fp64"):
+    g = Solver(rd.clawdata, solver, params, precision)
+    o = OracleGrid(rd.clawdata, solver, params)
+    g.set_q(q0)
+    o.set_q(q0)
+    if aux is not None:
+        g.set_aux(aux)
+        o.set_aux(aux)
+    return g, o
+
+
+@pytest.mark.parametrize("mx,my", SIZES)
+@pytest.mark.parametrize("bc", BCS)
+def test_single_step_bitwise(mx, my, bc):
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(mx, my, seed=mx * 131 + my, bc=bc)
+    g, o = _pair(rd, solver, params, q0)
+    for dt in (0.004, 0.006):
+        cg, co = g.step(dt), o.step(dt)
+        assert cg == co
+        assert same(g.get_q(), o.get_q())
+    g.close()
+
+
+@pytest.mark.parametrize("lim", ["none", "minmod", "superbee", "vanleer", "mc", 5])
+@pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 0), (2, 1), (2, 2)])
+def test_methods_bitwise(lim, order, trans):
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(45, 38, seed=7, limiter=lim,
+                                                            order=order, trans=trans,
+                                                            bc=("wall", "extrap", "extrap", "wall"))
+    g, o = _pair(rd, solver, params, q0)
+    for _ in range(3):
+        assert g.step(0.005) == o.step(0.005)
+    assert same(g.get_q(), o.get_q())
+    g.close()
+
+
+def test_advance_matches_dt_sequence_and_reject_path():
+    """claw2 control on the device: first dt too large -> rejected and
+    retried; variable dt; stats equal to claw2's dtv/cflv/nv."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=96, nout=3, tfinal=0.3,
+                                                            dt_initial=0.5)
+    g, o = _pair(rd, solver, params, q0)
+    t, dt = 0.0, 0.5
+    for k in range(3):
+        ig, sg = g.advance(t, t + 0.1, dt)
+        io, so = o.advance(t, t + 0.1, dt)
+        assert ig == io == 0
+        for key in ("t_reached", "dt_min", "dt_max_taken", "dt_next", "cfl_max_seen",
+                    "cfl_last", "steps_taken"):
+            assert sg[key] == so[key], key
+        if k == 0:
+            assert sg["steps_rejected"] >= 1
+        assert same(g.get_q(), o.get_q())
+        t, dt = sg["t_reached"], sg["dt_next"]
+    g.close()
+
+
+def test_fixed_dt_and_info_codes():
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(40, 40, seed=1)
+    cd = rd.clawdata
+    cd.dt_variable = False
+    g, o = _pair(rd, solver, params, q0)
+    ig, sg = g.advance(0.0, 0.02, 0.005)
+    io, so = o.advance(0.0, 0.02, 0.005)
+    assert ig == io == 0 and sg["steps_taken"] == so["steps_taken"] == 4
+    assert same(g.get_q(), o.get_q())
+    assert g.advance(0.0, 0.1, 0.03)[0] == 2
+    assert g.advance(0.0, 0.4, 0.2)[0] == 12
+    g.close()
+
+
+def test_radial_full_run_bitwise():
+    """The 2D radial acoustics workload (MC, transverse 2) to t_final = 0.6
+    at 128^2: every frame bit-identical to the oracle."""
+    from classic_b200.solver import run
+    from pyoracle import run_oracle
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=128, nout=4, tfinal=0.6)
+    fg = run(rd, solver, params, q0)
+    fo = run_oracle(rd, solver, params, q0)
+    assert len(fg) == len(fo)
+    for a, b in zip(fg, fo):
+        assert a.t == b[1]
+        assert same(a.q, b[2])
+
+
+def test_annulus_capacity_bitwise():
+    """Capacity, aux-dependent solver, periodic y: the reference's only 2D
+    regression case, bit-identical to the oracle frame by frame."""
+    from classic_b200.solver import run
+    from pyoracle import run_oracle
+    rd, solver, params, q0, aux = problems.advection_2d_annulus()
+    fg = run(rd, solver, params, q0, aux)
+    fo = run_oracle(rd, solver, params, q0, aux)
+    for a, b in zip(fg, fo):
+        assert a.t == b[1]
+        assert same(a.q, b[2])
+
+
+def test_full_size_4096_step_bitwise():
+    """The benchmark size (4096^2) for two steps: bit-identical to the oracle."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
+    g, o = _pair(rd, solver, params, q0)
+    dx = 2.0 / 4096
+    for dt in (0.9 * dx / 2.0, 0.85 * dx / 2.0):
+        assert g.step(dt) == o.step(dt)
+    assert same(g.get_q(), o.get_q())
+    g.close()
+
+
+def test_determinism_and_symmetry_1024():
+    """Size-independent properties at 1024^2 over 50 steps: two runs are
+    bit-identical; the radially symmetric data stays mirror symmetric
+    (p even, u odd in x) to roundoff."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=1024)
+    runs = []
+    for _ in range(2):
+        g = Solver(rd.clawdata, solver, params)
+        g.set_q(q0)
+        for _ in range(50):
+            g.step(0.9 * (2.0 / 1024) / 2.0)
+        runs.append(g.get_q())
+        g.close()
+    assert same(runs[0], runs[1])
+    q = runs[0]
+    assert np.max(np.abs(q[0] - q[0][:, ::-1])) < 1e-12
+    assert np.max(np.abs(q[1] + q[1][:, ::-1])) < 1e-12
+    assert np.max(np.abs(q[0] - q[0].T)) < 1e-12
+
+
+def test_fp32_variant_tracks_fp64():
+    """FP32 update path, FP64 CFL/dt/time: within single-precision error of
+    the FP64 oracle after 20 steps."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=256, nout=1, tfinal=0.05)
+    g, o = _pair(rd, solver, params, q0, precision="fp32")
+    ig, sg = g.advance(0.0, 0.05, 0.01)
+    io, so = o.advance(0.0, 0.05, 0.01)
+    assert ig == io == 0 and sg["steps_taken"] == so["steps_taken"]
+    assert np.all(rel_diff(g.get_q(), o.get_q()) < 2e-5)
+    g.close()
