@@ -90,7 +90,7 @@ struct Runner {
     virtual cudaError_t launch(cudaStream_t s) = 0;
 };
 
-template <class S>
+template <class S, class M>
 struct Runner2D : Runner {
     Step2Args<S> args;
     int grid = 1, smem = 0;
@@ -132,12 +132,12 @@ struct Runner2D : Runner {
             if (rc) return rc;
         }
         smem = R::SMEM;
-        CUDA_TRY(cudaFuncSetAttribute(step2_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(cudaFuncSetAttribute(step2_kernel<S, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_kernel<S>,
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_kernel<S, M>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "step2 kernel cannot be resident on an SM");
         args.units = (long long)args.nstrips * g.my;
@@ -152,7 +152,7 @@ struct Runner2D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_kernel<S><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        step2_kernel<S, M><<<grid, 32 * WARPS2D, smem, s>>>(args);
         return cudaGetLastError();
     }
 };
@@ -193,6 +193,23 @@ struct Runner1D : Runner {
     }
 };
 
+// True when every wave uses the same limiter `lim`.
+bool all_limiters(const claw_config& cfg, int lim) {
+    for (int k = 0; k < cfg.num_waves; ++k)
+        if (cfg.limiter[k] != lim) return false;
+    return true;
+}
+
+// The hot method (order 2, transverse 2, MC on every wave, no capacity, no
+// f-waves) runs a fully specialised kernel; every other method the generic one.
+template <class S>
+std::unique_ptr<Runner> runner2d(const claw_config& cfg, const S& s) {
+    if (cfg.order == 2 && cfg.transverse_waves == 2 && all_limiters(cfg, 4) &&
+        cfg.capa_index == 0 && !cfg.use_fwaves)
+        return std::unique_ptr<Runner>(new Runner2D<S, MethodMC2D>(s));
+    return std::unique_ptr<Runner>(new Runner2D<S, MethodGeneric2D>(s));
+}
+
 template <typename real>
 std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
     const int id = cfg.solver_id;
@@ -201,13 +218,13 @@ std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
         const double cc = std::sqrt(bulk / rho), zz = rho * cc, hz = 0.5 / zz;
         if (id == CLAW_SOLVER_ACOUSTICS_2D) {
             Acoustics2D<real> s{(real)cc, (real)zz, (real)hz};
-            return std::unique_ptr<Runner>(new Runner2D<Acoustics2D<real>>(s));
+            return runner2d(cfg, s);
         }
         Acoustics1D<real> s{(real)cc, (real)zz, (real)hz};
         return std::unique_ptr<Runner>(new Runner1D<Acoustics1D<real>>(s));
     }
     if (id == CLAW_SOLVER_VC_ADVECTION_2D)
-        return std::unique_ptr<Runner>(new Runner2D<VCAdvection2D<real>>(VCAdvection2D<real>{}));
+        return std::unique_ptr<Runner>(new Runner2D<VCAdvection2D<real>, MethodGeneric2D>(VCAdvection2D<real>{}));
     if (id == CLAW_SOLVER_VC_ACOUSTICS_1D)
         return std::unique_ptr<Runner>(new Runner1D<VCAcoustics1D<real>>(VCAcoustics1D<real>{}));
     return nullptr;

@@ -184,7 +184,7 @@ __device__ __forceinline__ real phi_limiter(int meth, real r) {
         case 2: return fmax(fmax(zero, fmin(one, two * r)), fmin(two, r));
         case 3: return (r + fabs(r)) / (one + fabs(r));
         case 4: {
-            const real c = (one + r) / two;
+            const real c = (one + r) * real(0.5);  // == (1+r)/2 exactly
             return fmax(zero, fmin(fmin(c, two), two * r));
         }
         case 5: return r;

@@ -34,6 +34,13 @@ struct Acoustics2D {
     static constexpr int meqn = 3, mwaves = 2, maux = 0;
     real cc, zz, hz;
 
+    // Structurally zero components (the kernels skip arithmetic on them; the
+    // skipped terms are exact zeros, so results are value-identical):
+    // waves and fluctuations of an ixy-slice carry no transverse velocity,
+    // transverse splits carry no normal velocity.
+    __host__ __device__ static constexpr bool wave_zero(int ixy, int m) { return m == (ixy == 1 ? 2 : 1); }
+    __host__ __device__ static constexpr bool trans_zero(int ixy, int m) { return m == (ixy == 1 ? 1 : 2); }
+
     __device__ __forceinline__ void rpn(int ixy, const real* qL, const real* qR, const real*,
                                         const real*, real wave[mwaves][meqn], real s[mwaves],
                                         real amdq[meqn], real apdq[meqn]) const {
@@ -68,6 +75,8 @@ template <typename real_>
 struct VCAdvection2D {
     using real = real_;
     static constexpr int meqn = 1, mwaves = 1, maux = 3;
+    __host__ __device__ static constexpr bool wave_zero(int, int) { return false; }
+    __host__ __device__ static constexpr bool trans_zero(int, int) { return false; }
 
     __device__ __forceinline__ void rpn(int ixy, const real* qL, const real* qR, const real*,
                                         const real* auxR, real wave[mwaves][meqn], real s[mwaves],

@@ -23,19 +23,40 @@
 // (cp.async.bulk.tensor, one box of 34(36) x 1 x meqn per row, ghost rows
 // loaded from their mapped source row), completion on an mbarrier per slot,
 // prefetching RING-3 rows ahead.  q is read once from HBM and written once.
+//
+// Specialisation: the method (order, transverse_waves, limiter, capacity,
+// f-waves) is a compile-time policy for the configurations that matter, so
+// a row of the march is straight-line code; Method2D<-1,...> reads every
+// choice at run time and covers all other configurations.  Solver traits
+// (wave_zero / trans_zero) remove arithmetic on structurally zero
+// components; the skipped terms are exact zeros, so results are unchanged.
 #pragma once
 #include "common.cuh"
 
 namespace clawb200 {
 
 constexpr int STRIP = 28;      // output columns per warp
-constexpr int RING = 12;       // rows in flight per warp
+constexpr int RING = 8;        // rows in flight per warp (power of two)
+constexpr int RING_LOG = 3;
 constexpr int WARPS2D = 4;     // warps per CTA
+static_assert((1 << RING_LOG) == RING, "RING must be 2^RING_LOG");
 
+// A TMA box must start at an x coordinate whose byte offset is a multiple of
+// 16: q boxes start XQ columns left of the strip (b is a multiple of 28, so
+// b - 2 is even and b - 4 a multiple of 4), aux boxes at padded column b.
 template <typename real>
-struct BoxW { static constexpr int value = 34; };
+struct BoxW { static constexpr int value = 34; static constexpr int XQ = 2; };
 template <>
-struct BoxW<float> { static constexpr int value = 36; };
+struct BoxW<float> { static constexpr int value = 36; static constexpr int XQ = 4; };
+static_assert(STRIP % 4 == 0, "strip width must keep b a multiple of 4");
+
+// Method policy: -1 = read from the kernel arguments at run time.
+template <int ORDER, int TRANS, int LIM, int CAPA, int FWAVE>
+struct Method2D {
+    static constexpr int order = ORDER, trans = TRANS, lim = LIM, capa = CAPA, fwave = FWAVE;
+};
+using MethodGeneric2D = Method2D<-1, -1, -1, -1, -1>;
+using MethodMC2D = Method2D<2, 2, 4, 0, 0>;  // order 2, transverse 2, MC, no capa
 
 template <class S>
 struct Step2Args {
@@ -61,7 +82,7 @@ struct Step2Args {
 __device__ __forceinline__ int bc_map(int x, int n, int blo, int bhi, bool& neg) {
     neg = false;
     if (x < 0) {
-        if (x < -2) x = -2;  // beyond the two ghost layers: only garbage lanes
+        if (x < -2) x = -2;  // beyond the two ghost layers: only halo lanes past the edge
         if (blo == BC_PERIODIC) return x + n;
         if (blo == BC_WALL) { neg = true; return -1 - x; }
         return 0;
@@ -87,14 +108,19 @@ struct Ring2D {
     static constexpr int SMEM = WARPS2D * WARP_BYTES + WARPS2D * RING * 8 + 64;
 };
 
-template <class S>
-__global__ void __launch_bounds__(32 * WARPS2D)
+#ifndef CLAW_STEP2_MINB
+#define CLAW_STEP2_MINB 4  // 128 registers: 16 warps per SM hide the FP64 latency
+#endif
+
+template <class S, class M>
+__global__ void __launch_bounds__(32 * WARPS2D, CLAW_STEP2_MINB)
 step2_kernel(const __grid_constant__ Step2Args<S> A) {
     using real = typename S::real;
     constexpr int ME = S::meqn, MW = S::mwaves, MA = S::maux;
     constexpr int MAX = MA > 0 ? MA : 1;
     using R = Ring2D<S>;
     constexpr int W = R::W;
+    constexpr unsigned FULL = 0xffffffffu;
 
     ClawCtl* ctl = A.ctl;
     __shared__ double red[WARPS2D];
@@ -107,6 +133,18 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
     real* __restrict__ qnew = A.q[cur ^ 1];
     const CUtensorMap* tmq = &A.tmq[cur];
 
+    // method: compile-time where the policy fixes it
+    const int order = M::order >= 0 ? M::order : A.order;
+    const int trans = M::trans >= 0 ? M::trans : A.trans;
+    const bool capa = M::capa >= 0 ? (M::capa != 0) : (A.capa > 0);
+    const bool fwave = M::fwave >= 0 ? (M::fwave != 0) : (A.fwave != 0);
+    const int ic = capa ? A.capa - 1 : 0;
+    bool limit = M::lim > 0;
+    if (M::lim < 0)
+        limit = (A.mthlim[0] | A.mthlim[1] | A.mthlim[2] | A.mthlim[3] | A.mthlim[4] |
+                 A.mthlim[5] | A.mthlim[6] | A.mthlim[7]) != 0;
+    auto lim_of = [&](int mw) -> int { return M::lim >= 0 ? M::lim : A.mthlim[mw]; };
+
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* ring = smem + warp * R::WARP_BYTES;
@@ -118,10 +156,6 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
     __syncwarp();
 
     const int mx = A.mx, my = A.my;
-    const bool limit = (A.mthlim[0] | A.mthlim[1] | A.mthlim[2] | A.mthlim[3] | A.mthlim[4] |
-                        A.mthlim[5] | A.mthlim[6] | A.mthlim[7]) != 0;
-    const bool capa = A.capa > 0;
-    const int ic = A.capa - 1;
     double cfl = 0.0;
     bool failed = false;
     uint32_t seq_base = 0;
@@ -137,7 +171,7 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
         u0 += nr;
         const int b = strip * STRIP;
         const int c = b - 1 + lane;
-        const int x0 = b - 2;  // first column held in the ring
+        const int x0 = b - BoxW<real>::XQ;  // first q column held in the ring
         const int rfirst = r0 - 2, rlast = r0 + nr + 1;  // rows streamed
         const int nrows = rlast - rfirst + 1;
 
@@ -147,20 +181,24 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
         const int sc = bc_map(c, mx, A.bc[0], A.bc[1], negc);
         const bool gm = (sm - x0) < 0 || (sm - x0) >= W;
         const bool gc = (sc - x0) < 0 || (sc - x0) >= W;
+        const bool any_global = __any_sync(FULL, gm || gc);
         const int im = gm ? 0 : sm - x0, icc = gc ? 0 : sc - x0;
+        // x-interface c counts toward the CFL for columns 0..mx, y-interface
+        // of column c for columns -1..mx (src/2d/flux2.f90:124-132 over the
+        // slices of src/2d/step2.f90:92,173)
+        const bool cx_ok = c >= 0 && c <= mx;
+        const bool cy_ok = c >= -1 && c <= mx;
 
-        auto slot_of = [&](int r) -> int { return (int)((seq_base + (uint32_t)(r - rfirst)) % RING); };
-        auto parity_of = [&](int r) -> uint32_t {
-            return ((seq_base + (uint32_t)(r - rfirst)) / RING) & 1u;
-        };
+        auto seq_of = [&](int r) -> uint32_t { return seq_base + (uint32_t)(r - rfirst); };
         auto issue = [&](int r) {
-            const int sl = slot_of(r);
+            const uint32_t sq = seq_of(r);
+            const int sl = (int)(sq & (RING - 1));
             unsigned char* dst = ring + sl * R::SLOT;
             bool nyneg;
             const int sr = bc_map(r, my, A.bc[2], A.bc[3], nyneg);
             mbar_arrive_expect_tx(&bars[sl], (uint32_t)(R::QB + R::AB));
             tma_load_3d(dst, tmq, x0, sr, 0, &bars[sl]);
-            if constexpr (MA > 0) tma_load_3d(dst + R::QBP, &A.tmaux, x0 + 2, r + 2, 0, &bars[sl]);
+            if constexpr (MA > 0) tma_load_3d(dst + R::QBP, &A.tmaux, b, r + 2, 0, &bars[sl]);
         };
         if (lane == 0) {
             const int npre = nrows < RING ? nrows : RING;
@@ -168,19 +206,27 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
         }
         __syncwarp();
 
-        // Wait for row r and load q(c-1, r), q(c, r).
         auto wait_row = [&](int r) -> bool {
-            return mbar_wait_bounded(&bars[slot_of(r)], parity_of(r));
+            const uint32_t sq = seq_of(r);
+            return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u);
         };
+        auto slot_ptr = [&](int r) -> const unsigned char* {
+            return ring + (int)(seq_of(r) & (RING - 1)) * R::SLOT;
+        };
+        // q(c-1, r), q(c, r) with the x and y boundary conditions applied.
         auto load_q = [&](int r, real* qm, real* qc) {
-            const real* sq = reinterpret_cast<const real*>(ring + slot_of(r) * R::SLOT);
+            const real* sq = reinterpret_cast<const real*>(slot_ptr(r));
             bool nyneg;
             const int sr = bc_map(r, my, A.bc[2], A.bc[3], nyneg);
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                real vm = gm ? qold[m * A.fstride + (long long)sr * A.ld + sm] : sq[m * W + im];
-                real vc = gc ? qold[m * A.fstride + (long long)sr * A.ld + sc] : sq[m * W + icc];
-                if (m == 1) { if (negm) vm = -vm; if (negc) vc = -vc; }
+                real vm = sq[m * W + im];
+                real vc = sq[m * W + icc];
+                if (any_global) {
+                    if (gm) vm = qold[m * A.fstride + (long long)sr * A.ld + sm];
+                    if (gc) vc = qold[m * A.fstride + (long long)sr * A.ld + sc];
+                }
+                if (m == 1) { vm = negm ? -vm : vm; vc = negc ? -vc : vc; }
                 if (m == 2 && nyneg) { vm = -vm; vc = -vc; }
                 qm[m] = vm;
                 qc[m] = vc;
@@ -189,7 +235,7 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
         // aux of column (c + dc) at row r (ring already resident).
         auto aux_at = [&](int r, int dc, real* a) {
             if constexpr (MA > 0) {
-                const real* sa = reinterpret_cast<const real*>(ring + slot_of(r) * R::SLOT + R::QBP);
+                const real* sa = reinterpret_cast<const real*>(slot_ptr(r) + R::QBP);
 #pragma unroll
                 for (int k = 0; k < MA; ++k) a[k] = sa[k * W + lane + 1 + dc];
             }
@@ -206,264 +252,315 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
         real P1[ME], P3[ME], P4[ME], Fy_prev[ME];
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-            Ax_prev[m] = q2_prev[m] = qc_p[m] = real(0);
+            Ax_prev[m] = q2_prev[m] = real(0);
             P1[m] = P3[m] = P4[m] = Fy_prev[m] = real(0);
-            amy[m] = apy[m] = real(0);
         }
 #pragma unroll
-        for (int mw = 0; mw < MW; ++mw) {
-            dotl_y[mw] = real(0);
-            sy[mw] = real(0);
-#pragma unroll
-            for (int m = 0; m < ME; ++m) wy[mw][m] = real(0);
-        }
+        for (int mw = 0; mw < MW; ++mw) dotl_y[mw] = real(0);
 
         int last_issued = rfirst + (nrows < RING ? nrows : RING) - 1;
         int fail_row = rlast + 1;
-        if (!wait_row(rfirst)) { failed = true; fail_row = rfirst; }
-        if (!failed) load_q(rfirst, qm_t, qc_t);
 
-        for (int t = rfirst; t <= r0 + nr && !failed; ++t) {
+        // ---- prologue: rows r0-2, r0-1 and the y-interface between them ----
+        if (!wait_row(rfirst)) { failed = true; fail_row = rfirst; }
+        if (!failed && !wait_row(rfirst + 1)) { failed = true; fail_row = rfirst + 1; }
+        if (!failed) {
+            load_q(rfirst, qm_t, qc_t);
+            load_q(rfirst + 1, qm_n, qc_n);
+            real a_c[MAX], a_cn[MAX];
+            aux_at(rfirst, 0, a_c);
+            aux_at(rfirst + 1, 0, a_cn);
+            A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wy, sy, amy, apy);
+            if (cy_ok && rfirst + 1 >= 0) {
+                const double dt0 = capa ? dtdy_d / (double)a_c[ic] : dtdy_d;
+                const double dt1 = capa ? dtdy_d / (double)a_cn[ic] : dtdy_d;
+                double em = 0.0;
+#pragma unroll
+                for (int mw = 0; mw < MW; ++mw)
+                    em = fmax(em, fmax(dt1 * (double)sy[mw], -dt0 * (double)sy[mw]));
+                cfl = fmax(cfl, em);
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                qc_p[m] = qc_t[m];
+                qm_t[m] = qm_n[m];
+                qc_t[m] = qc_n[m];
+            }
+        }
+
+        for (int t = r0 - 1; t <= r0 + nr && !failed; ++t) {
             // ---------------- read row t+1 ----------------
             if (!wait_row(t + 1)) { failed = true; fail_row = t + 1; break; }
             load_q(t + 1, qm_n, qc_n);
-            real a_m[MAX], a_c[MAX], a_cn[MAX];  // aux at (c-1,t), (c,t), (c,t+1)
-            aux_at(t, -1, a_m);
-            aux_at(t, 0, a_c);
-            aux_at(t + 1, 0, a_cn);
-            // raw y-interface t+1 (rows t, t+1) and its CFL
-            real wn[MW][ME], sn[MW], amn[ME], apn[ME];
-            A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wn, sn, amn, apn);
-            if (c >= -1 && c <= mx && t + 1 >= 0 && t + 1 <= my) {
-                const double dt0 = capa ? dtdy_d / (double)a_c[ic] : dtdy_d;
-                const double dt1 = capa ? dtdy_d / (double)a_cn[ic] : dtdy_d;
-#pragma unroll
-                for (int mw = 0; mw < MW; ++mw)
-                    cfl = fmax(fmax(cfl, dt1 * (double)sn[mw]), -dt0 * (double)sn[mw]);
-            }
+            real a_m[MAX], a_c[MAX], a_cn[MAX], a_p[MAX], a_cp[MAX], a_mp[MAX], a_pp[MAX], a_mn[MAX];
+            aux_at(t, -1, a_m);       // (c-1, t)
+            aux_at(t, 0, a_c);        // (c,   t)
+            aux_at(t, 1, a_p);        // (c+1, t)
+            aux_at(t + 1, 0, a_cn);   // (c,   t+1)
+            aux_at(t + 1, -1, a_mn);  // (c-1, t+1)
+            aux_at(t - 1, 0, a_cp);   // (c,   t-1)
+            aux_at(t - 1, -1, a_mp);  // (c-1, t-1)
+            aux_at(t - 1, 1, a_pp);   // (c+1, t-1)
 
-            if (t >= r0 - 1) {
-                // rows t-1 .. t+1 are resident from here on
-                real a_p[MAX], a_cp[MAX], a_mp[MAX], a_pp[MAX], a_mn[MAX];
-                aux_at(t, 1, a_p);        // (c+1, t)
-                aux_at(t - 1, 0, a_cp);   // (c,   t-1)
-                aux_at(t - 1, -1, a_mp);  // (c-1, t-1)
-                aux_at(t - 1, 1, a_pp);   // (c+1, t-1)
-                aux_at(t + 1, -1, a_mn);  // (c-1, t+1)
-
-                // ======== x-slice t: interface c (between columns c-1, c) ========
-                real q3[ME];
+            // ======== x-slice t: interface c (between columns c-1, c) ========
+            real q3[ME];
+            {
+                real w[MW][ME], s[MW], amdq[ME], apdq[ME];
+                A.solver.rpn(1, qm_t, qc_t, a_m, a_c, w, s, amdq, apdq);
+                const real dtm = capa ? dtdx / a_m[ic] : dtdx;  // dtdx1d(i-1)
+                const real dtc = capa ? dtdx / a_c[ic] : dtdx;  // dtdx1d(i)
                 {
-                    real w[MW][ME], s[MW], amdq[ME], apdq[ME];
-                    A.solver.rpn(1, qm_t, qc_t, a_m, a_c, w, s, amdq, apdq);
-                    const real dtm = capa ? dtdx / a_m[ic] : dtdx;  // dtdx1d(i-1)
-                    const real dtc = capa ? dtdx / a_c[ic] : dtdx;  // dtdx1d(i)
-                    if (c >= 0 && c <= mx && t >= -1 && t <= my) {
-                        const double dm = capa ? dtdx_d / (double)a_m[ic] : dtdx_d;
-                        const double dc = capa ? dtdx_d / (double)a_c[ic] : dtdx_d;
+                    const double dm = capa ? dtdx_d / (double)a_m[ic] : dtdx_d;
+                    const double dc = capa ? dtdx_d / (double)a_c[ic] : dtdx_d;
+                    double em = 0.0;
 #pragma unroll
-                        for (int mw = 0; mw < MW; ++mw)
-                            cfl = fmax(fmax(cfl, dc * (double)s[mw]), -dm * (double)s[mw]);
-                    }
-                    real send1[ME], qadd[ME], F[ME], cq[ME];
+                    for (int mw = 0; mw < MW; ++mw)
+                        em = fmax(em, fmax(dc * (double)s[mw], -dm * (double)s[mw]));
+                    cfl = (cx_ok && t >= -1 && t <= my) ? fmax(cfl, em) : cfl;
+                }
+                real send1[ME], qadd[ME], F[ME], cq[ME];
 #pragma unroll
-                    for (int m = 0; m < ME; ++m) {
-                        send1[m] = dtm * amdq[m];           // qadd of cell c-1 from this interface
-                        qadd[m] = real(0) - dtc * apdq[m];  // qadd of cell c, first term
-                        F[m] = real(0);
-                        cq[m] = real(0);
-                    }
-                    if (A.order != 1) {
-                        if (limit) {
-                            real dotr[MW], wn2[MW];
+                for (int m = 0; m < ME; ++m) {
+                    const bool z = S::wave_zero(1, m);
+                    send1[m] = z ? real(0) : dtm * amdq[m];   // qadd of cell c-1 from this interface
+                    qadd[m] = z ? real(0) : -(dtc * apdq[m]);  // qadd of cell c, first term
+                    F[m] = real(0);
+                    cq[m] = real(0);
+                }
+                if (order != 1) {
+                    if (limit) {
+                        real dotr[MW], wn2[MW];
 #pragma unroll
-                            for (int mw = 0; mw < MW; ++mw) {
-                                real dr = real(0), nn = real(0);
+                        for (int mw = 0; mw < MW; ++mw) {
+                            real dr = real(0), nn = real(0);
+                            bool first = true;
 #pragma unroll
-                                for (int m = 0; m < ME; ++m) {
-                                    const real wr = __shfl_down_sync(0xffffffffu, w[mw][m], 1);
+                            for (int m = 0; m < ME; ++m) {
+                                if (S::wave_zero(1, m)) continue;
+                                const real wr = __shfl_down_sync(FULL, w[mw][m], 1);
+                                if (first) {
+                                    nn = w[mw][m] * w[mw][m];
+                                    dr = w[mw][m] * wr;
+                                    first = false;
+                                } else {
                                     nn = nn + w[mw][m] * w[mw][m];
                                     dr = dr + w[mw][m] * wr;
                                 }
-                                dotr[mw] = dr;
-                                wn2[mw] = nn;
                             }
-#pragma unroll
-                            for (int mw = 0; mw < MW; ++mw) {
-                                const real dl = __shfl_up_sync(0xffffffffu, dotr[mw], 1);
-                                const int ml = A.mthlim[mw];
-                                if (ml != 0 && wn2[mw] != real(0)) {
-                                    const real r = (s[mw] > real(0) ? dl : dotr[mw]) / wn2[mw];
-                                    const real ph = phi_limiter<real>(ml, r);
-#pragma unroll
-                                    for (int m = 0; m < ME; ++m) w[mw][m] = ph * w[mw][m];
-                                }
-                            }
+                            dotr[mw] = dr;
+                            wn2[mw] = nn;
                         }
-                        const real ave = real(0.5) * (dtm + dtc);
 #pragma unroll
                         for (int mw = 0; mw < MW; ++mw) {
-                            const real as = fabs(s[mw]);
-                            const real coef = A.fwave ? copysign(real(1), s[mw]) * (real(1) - as * ave)
-                                                      : as * (real(1) - as * ave);
+                            const int ml = lim_of(mw);
+                            if (ml == 0) continue;
+                            const real dl = __shfl_up_sync(FULL, dotr[mw], 1);
+                            const real r = (s[mw] > real(0) ? dl : dotr[mw]) / wn2[mw];
+                            const real ph = wn2[mw] != real(0) ? phi_limiter<real>(ml, r) : real(1);
 #pragma unroll
-                            for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * w[mw][m];
-                        }
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) F[m] = real(0.5) * cq[m];
-                    }
-                    real s3[ME], s4[ME], g1b[ME], g2b[ME];
-                    if (A.trans > 0) {
-                        if (A.order != 1 && A.trans == 2) {
-#pragma unroll
-                            for (int m = 0; m < ME; ++m) {
-                                amdq[m] = amdq[m] + cq[m];
-                                apdq[m] = apdq[m] - cq[m];
-                            }
-                        }
-                        real bm[ME], bp[ME];
-                        A.solver.rpt(1, 1, qm_t, qc_t, a_mp, a_m, a_mn, amdq, bm, bp);
-                        const real hm = real(0.5) * dtm, hc = real(0.5) * dtc;
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) {
-                            s3[m] = -(hm * bm[m]);  // gadd(:,1,i-1) from this interface
-                            s4[m] = -(hm * bp[m]);  // gadd(:,2,i-1)
-                        }
-                        A.solver.rpt(1, 2, qm_t, qc_t, a_cp, a_c, a_cn, apdq, bm, bp);
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) {
-                            g1b[m] = hc * bm[m];
-                            g2b[m] = hc * bp[m];
-                        }
-                    } else {
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) s3[m] = s4[m] = g1b[m] = g2b[m] = real(0);
-                    }
-                    // interface c+1 (lane+1) finishes cell c
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) {
-                        const real r1 = __shfl_down_sync(0xffffffffu, send1[m], 1);
-                        const real r2 = __shfl_down_sync(0xffffffffu, F[m], 1);
-                        const real r3 = __shfl_down_sync(0xffffffffu, s3[m], 1);
-                        const real r4 = __shfl_down_sync(0xffffffffu, s4[m], 1);
-                        const real qa = qadd[m] - r1;
-                        const real G1 = r3 - g1b[m];
-                        const real G2 = r4 - g2b[m];
-                        const real dF = r2 - F[m];
-                        real q2, Ax, Bx;
-                        if (!capa) {
-                            q2 = (((qc_t[m] + Ax_prev[m]) + qa) - dtdx * dF) - dtdy * (G2 - G1);
-                            Ax = dtdy * G2;
-                            Bx = dtdy * G1;
-                        } else {
-                            q2 = ((qc_t[m] + Ax_prev[m]) + qa) -
-                                 (dtdx * dF + dtdy * (G2 - G1)) / a_c[ic];
-                            Ax = dtdy * G2 / a_cn[ic];
-                            Bx = dtdy * G1 / a_cp[ic];
-                        }
-                        q3[m] = q2_prev[m] - Bx;  // x-part of cell (c, t-1) complete
-                        q2_prev[m] = q2;
-                        Ax_prev[m] = Ax;
-                    }
-                }
-
-                // ======== y-interface t (rows t-1, t) limited; y-part of cell (c, t-1) ========
-                const real dty_p = capa ? dtdy / a_cp[ic] : dtdy;  // dtdy1d(t-1)
-                const real dty_t = capa ? dtdy / a_c[ic] : dtdy;   // dtdy1d(t)
-                real cqy[ME], Fy[ME], dotr_y[MW];
-#pragma unroll
-                for (int m = 0; m < ME; ++m) { cqy[m] = real(0); Fy[m] = real(0); }
-#pragma unroll
-                for (int mw = 0; mw < MW; ++mw) {
-                    real dr = real(0);
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) dr = dr + wy[mw][m] * wn[mw][m];
-                    dotr_y[mw] = dr;
-                }
-                if (A.order != 1) {
-                    if (limit) {
-#pragma unroll
-                        for (int mw = 0; mw < MW; ++mw) {
-                            real nn = real(0);
-#pragma unroll
-                            for (int m = 0; m < ME; ++m) nn = nn + wy[mw][m] * wy[mw][m];
-                            const int ml = A.mthlim[mw];
-                            if (ml != 0 && nn != real(0)) {
-                                const real r = (sy[mw] > real(0) ? dotl_y[mw] : dotr_y[mw]) / nn;
-                                const real ph = phi_limiter<real>(ml, r);
-#pragma unroll
-                                for (int m = 0; m < ME; ++m) wy[mw][m] = ph * wy[mw][m];
-                            }
+                            for (int m = 0; m < ME; ++m)
+                                if (!S::wave_zero(1, m)) w[mw][m] = ph * w[mw][m];
                         }
                     }
-                    const real ave = real(0.5) * (dty_p + dty_t);
+                    const real ave = real(0.5) * (dtm + dtc);
 #pragma unroll
                     for (int mw = 0; mw < MW; ++mw) {
-                        const real as = fabs(sy[mw]);
-                        const real coef = A.fwave ? copysign(real(1), sy[mw]) * (real(1) - as * ave)
-                                                  : as * (real(1) - as * ave);
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) cqy[m] = cqy[m] + coef * wy[mw][m];
-                    }
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) Fy[m] = real(0.5) * cqy[m];
-                }
-                real amo[ME], apo[ME];
-#pragma unroll
-                for (int m = 0; m < ME; ++m) { amo[m] = amy[m]; apo[m] = apy[m]; }
-                real bma[ME], bpa[ME], bmb[ME], bpb[ME];
-                if (A.trans > 0) {
-                    if (A.order != 1 && A.trans == 2) {
+                        const real as = fabs(s[mw]);
+                        const real coef = fwave ? copysign(real(1), s[mw]) * (real(1) - as * ave)
+                                                : as * (real(1) - as * ave);
 #pragma unroll
                         for (int m = 0; m < ME; ++m) {
-                            amy[m] = amy[m] + cqy[m];
-                            apy[m] = apy[m] - cqy[m];
+                            if (S::wave_zero(1, m)) continue;
+                            cq[m] = mw == 0 ? coef * w[mw][m] : cq[m] + coef * w[mw][m];
                         }
                     }
-                    A.solver.rpt(2, 1, qc_p, qc_t, a_mp, a_cp, a_pp, amy, bma, bpa);
-                    A.solver.rpt(2, 2, qc_p, qc_t, a_m, a_c, a_p, apy, bmb, bpb);
-                } else {
 #pragma unroll
-                    for (int m = 0; m < ME; ++m) bma[m] = bpa[m] = bmb[m] = bpb[m] = real(0);
+                    for (int m = 0; m < ME; ++m) F[m] = real(0.5) * cq[m];
                 }
-                const real hp = real(0.5) * dty_p, ht = real(0.5) * dty_t;
-                const bool out = (t - 1 >= r0) && (lane >= 1) && (lane <= STRIP) && (c < mx);
+                real s3[ME], s4[ME], g1b[ME], g2b[ME];
 #pragma unroll
-                for (int m = 0; m < ME; ++m) {
-                    const real qa = P1[m] - dty_p * amo[m];
-                    const real G1 = -(hp * bma[m]) - P3[m];
-                    const real G2 = -(hp * bpa[m]) - P4[m];
-                    const real dF = Fy[m] - Fy_prev[m];
-                    real Ay, By, q5pre;
-                    if (!capa) {
-                        Ay = dtdx * G2;
-                        By = dtdx * G1;
-                    } else {
-                        Ay = dtdx * G2 / a_pp[ic];
-                        By = dtdx * G1 / a_mp[ic];
+                for (int m = 0; m < ME; ++m) s3[m] = s4[m] = g1b[m] = g2b[m] = real(0);
+                if (trans > 0) {
+                    if (order != 1 && trans == 2) {
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) {
+                            if (S::wave_zero(1, m)) continue;
+                            amdq[m] = amdq[m] + cq[m];
+                            apdq[m] = apdq[m] - cq[m];
+                        }
                     }
-                    const real Al = __shfl_up_sync(0xffffffffu, Ay, 1);    // from column c-1
-                    const real Br = __shfl_down_sync(0xffffffffu, By, 1);  // from column c+1
-                    const real q4 = q3[m] + Al;
-                    if (!capa) q5pre = q4 + ((qa - dtdy * dF) - dtdx * (G2 - G1));
-                    else q5pre = (q4 + qa) - (dtdy * dF + dtdx * (G2 - G1)) / a_cp[ic];
-                    const real q6 = q5pre - Br;
-                    if (out) qnew[m * A.fstride + (long long)(t - 1) * A.ld + c] = q6;
+                    real bm[ME], bp[ME];
+                    A.solver.rpt(1, 1, qm_t, qc_t, a_mp, a_m, a_mn, amdq, bm, bp);
+                    const real hm = real(0.5) * dtm, hc = real(0.5) * dtc;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        if (S::trans_zero(1, m)) continue;
+                        s3[m] = -(hm * bm[m]);  // gadd(:,1,i-1) from this interface
+                        s4[m] = -(hm * bp[m]);  // gadd(:,2,i-1)
+                    }
+                    A.solver.rpt(1, 2, qm_t, qc_t, a_cp, a_c, a_cn, apdq, bm, bp);
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        if (S::trans_zero(1, m)) continue;
+                        g1b[m] = hc * bm[m];
+                        g2b[m] = hc * bp[m];
+                    }
                 }
-                // contributions of y-interface t to cell (c, t)
+                // interface c+1 (lane+1) finishes cell c
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
-                    P1[m] = real(0) - dty_t * apo[m];
-                    P3[m] = ht * bmb[m];
-                    P4[m] = ht * bpb[m];
-                    Fy_prev[m] = Fy[m];
+                    const bool wz = S::wave_zero(1, m), tz = S::trans_zero(1, m) || trans <= 0;
+                    real qa = real(0), dF = real(0), G1 = real(0), G2 = real(0);
+                    if (!wz) {
+                        const real r1 = __shfl_down_sync(FULL, send1[m], 1);
+                        const real r2 = __shfl_down_sync(FULL, F[m], 1);
+                        qa = qadd[m] - r1;
+                        dF = r2 - F[m];
+                    }
+                    if (!tz) {
+                        const real r3 = __shfl_down_sync(FULL, s3[m], 1);
+                        const real r4 = __shfl_down_sync(FULL, s4[m], 1);
+                        G1 = r3 - g1b[m];
+                        G2 = r4 - g2b[m];
+                    }
+                    real q2, Ax = real(0), Bx = real(0);
+                    if (!capa) {
+                        q2 = qc_t[m];
+                        if (!tz) q2 = q2 + Ax_prev[m];
+                        if (!wz) q2 = (q2 + qa) - dtdx * dF;
+                        if (!tz) {
+                            q2 = q2 - dtdy * (G2 - G1);
+                            Ax = dtdy * G2;
+                            Bx = dtdy * G1;
+                        }
+                    } else {
+                        q2 = ((qc_t[m] + Ax_prev[m]) + qa) - (dtdx * dF + dtdy * (G2 - G1)) / a_c[ic];
+                        Ax = dtdy * G2 / a_cn[ic];
+                        Bx = dtdy * G1 / a_cp[ic];
+                    }
+                    q3[m] = (!tz || capa) ? q2_prev[m] - Bx : q2_prev[m];  // x-part of (c, t-1)
+                    q2_prev[m] = q2;
+                    Ax_prev[m] = Ax;
+                }
+            }
+
+            // ======== y-interface t+1 raw; y-interface t limited; y-part of (c, t-1) ========
+            real wn[MW][ME], sn[MW], amn[ME], apn[ME];
+            A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wn, sn, amn, apn);
+            {
+                const double dt0 = capa ? dtdy_d / (double)a_c[ic] : dtdy_d;
+                const double dt1 = capa ? dtdy_d / (double)a_cn[ic] : dtdy_d;
+                double em = 0.0;
+#pragma unroll
+                for (int mw = 0; mw < MW; ++mw)
+                    em = fmax(em, fmax(dt1 * (double)sn[mw], -dt0 * (double)sn[mw]));
+                cfl = (cy_ok && t + 1 <= my) ? fmax(cfl, em) : cfl;
+            }
+            const real dty_p = capa ? dtdy / a_cp[ic] : dtdy;  // dtdy1d(t-1)
+            const real dty_t = capa ? dtdy / a_c[ic] : dtdy;   // dtdy1d(t)
+            real cqy[ME], Fy[ME], dotr_y[MW];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) { cqy[m] = real(0); Fy[m] = real(0); }
+#pragma unroll
+            for (int mw = 0; mw < MW; ++mw) {
+                real dr = real(0);
+                bool first = true;
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    if (S::wave_zero(2, m)) continue;
+                    dr = first ? wy[mw][m] * wn[mw][m] : dr + wy[mw][m] * wn[mw][m];
+                    first = false;
+                }
+                dotr_y[mw] = dr;
+            }
+            if (order != 1) {
+                if (limit) {
+#pragma unroll
+                    for (int mw = 0; mw < MW; ++mw) {
+                        const int ml = lim_of(mw);
+                        if (ml == 0) continue;
+                        real nn = real(0);
+                        bool first = true;
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) {
+                            if (S::wave_zero(2, m)) continue;
+                            nn = first ? wy[mw][m] * wy[mw][m] : nn + wy[mw][m] * wy[mw][m];
+                            first = false;
+                        }
+                        const real r = (sy[mw] > real(0) ? dotl_y[mw] : dotr_y[mw]) / nn;
+                        const real ph = nn != real(0) ? phi_limiter<real>(ml, r) : real(1);
+#pragma unroll
+                        for (int m = 0; m < ME; ++m)
+                            if (!S::wave_zero(2, m)) wy[mw][m] = ph * wy[mw][m];
+                    }
+                }
+                const real ave = real(0.5) * (dty_p + dty_t);
+#pragma unroll
+                for (int mw = 0; mw < MW; ++mw) {
+                    const real as = fabs(sy[mw]);
+                    const real coef = fwave ? copysign(real(1), sy[mw]) * (real(1) - as * ave)
+                                            : as * (real(1) - as * ave);
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        if (S::wave_zero(2, m)) continue;
+                        cqy[m] = mw == 0 ? coef * wy[mw][m] : cqy[m] + coef * wy[mw][m];
+                    }
                 }
 #pragma unroll
-                for (int mw = 0; mw < MW; ++mw) dotl_y[mw] = dotr_y[mw];
+                for (int m = 0; m < ME; ++m) Fy[m] = real(0.5) * cqy[m];
             }
-            // roll the y-interface window and the rows: t-1 <- t, t <- t+1
+            real amo[ME], apo[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) { amo[m] = amy[m]; apo[m] = apy[m]; }
+            real bma[ME], bpa[ME], bmb[ME], bpb[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) bma[m] = bpa[m] = bmb[m] = bpb[m] = real(0);
+            if (trans > 0) {
+                if (order != 1 && trans == 2) {
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        if (S::wave_zero(2, m)) continue;
+                        amy[m] = amy[m] + cqy[m];
+                        apy[m] = apy[m] - cqy[m];
+                    }
+                }
+                A.solver.rpt(2, 1, qc_p, qc_t, a_mp, a_cp, a_pp, amy, bma, bpa);
+                A.solver.rpt(2, 2, qc_p, qc_t, a_m, a_c, a_p, apy, bmb, bpb);
+            }
+            const real hp = real(0.5) * dty_p, ht = real(0.5) * dty_t;
+            const bool out = (t - 1 >= r0) && (lane >= 1) && (lane <= STRIP) && (c < mx);
+            real* __restrict__ dst = qnew + (long long)(t - 1) * A.ld + c;
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
+                const bool wz = S::wave_zero(2, m), tz = S::trans_zero(2, m) || trans <= 0;
+                const real qa = wz ? real(0) : P1[m] - dty_p * amo[m];
+                const real dF = wz ? real(0) : Fy[m] - Fy_prev[m];
+                const real G1 = tz ? real(0) : -(hp * bma[m]) - P3[m];
+                const real G2 = tz ? real(0) : -(hp * bpa[m]) - P4[m];
+                real q6;
+                if (!capa) {
+                    real q5 = q3[m];
+                    if (!tz) q5 = q5 + __shfl_up_sync(FULL, dtdx * G2, 1);  // from column c-1
+                    if (!wz && !tz) q5 = q5 + ((qa - dtdy * dF) - dtdx * (G2 - G1));
+                    else if (!wz) q5 = q5 + (qa - dtdy * dF);
+                    else if (!tz) q5 = q5 + (-(dtdx * (G2 - G1)));
+                    q6 = tz ? q5 : q5 - __shfl_down_sync(FULL, dtdx * G1, 1);  // from column c+1
+                } else {
+                    const real Al = __shfl_up_sync(FULL, dtdx * G2 / a_pp[ic], 1);
+                    const real Br = __shfl_down_sync(FULL, dtdx * G1 / a_mp[ic], 1);
+                    const real q4 = q3[m] + Al;
+                    const real q5 = (q4 + qa) - (dtdy * dF + dtdx * (G2 - G1)) / a_cp[ic];
+                    q6 = q5 - Br;
+                }
+                if (out) dst[m * A.fstride] = q6;
+            }
+            // contributions of y-interface t to cell (c, t); roll the window
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                P1[m] = S::wave_zero(2, m) ? real(0) : -(dty_t * apo[m]);
+                P3[m] = S::trans_zero(2, m) ? real(0) : ht * bmb[m];
+                P4[m] = S::trans_zero(2, m) ? real(0) : ht * bpb[m];
+                Fy_prev[m] = Fy[m];
                 amy[m] = amn[m];
                 apy[m] = apn[m];
                 qc_p[m] = qc_t[m];
@@ -472,13 +569,14 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
             }
 #pragma unroll
             for (int mw = 0; mw < MW; ++mw) {
+                dotl_y[mw] = dotr_y[mw];
                 sy[mw] = sn[mw];
 #pragma unroll
                 for (int m = 0; m < ME; ++m) wy[mw][m] = wn[mw][m];
             }
             // release row t-1 and prefetch row t-1+RING into its slot
             __syncwarp();
-            if (t - 1 >= rfirst && t - 1 + RING <= rlast) {
+            if (t - 1 + RING <= rlast) {
                 if (lane == 0) issue(t - 1 + RING);
                 last_issued = t - 1 + RING;
             }
