@@ -101,6 +101,8 @@ SIGNATURES = {
                                      ctypes.POINTER(ctypes.c_longlong),
                                      ctypes.POINTER(ctypes.c_longlong)]),
     "claw_launch_count": (ctypes.c_longlong, [_P]),
+    "claw_step2d_noalloc": (ctypes.c_int, [ctypes.POINTER(ClawConfig), _P, _P, ctypes.c_longlong,
+                                           _P, ctypes.c_longlong, ctypes.c_double, _D, _P]),
     "claw_last_error": (ctypes.c_char_p, []),
     "claw_build_info": (ctypes.c_char_p, []),
 }

@@ -41,7 +41,7 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         return LIB
     cmd = [_nvcc(), ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
            "-Xcompiler", "-fPIC", "-shared", "-o", LIB,
-           os.path.join(CSRC, "claw_b200.cu")]
+           os.path.join(CSRC, "claw_b200.cu"), os.path.join(CSRC, "noalloc.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)

@@ -255,6 +255,11 @@ __global__ void narrow_to_float(const double* src, float* dst, long long n) {
 
 }  // namespace
 
+namespace clawb200 {
+// Error message for claw_last_error() from other translation units.
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace clawb200
+
 struct claw_handle {
     claw_config cfg;
     Geometry g;

@@ -150,6 +150,25 @@ int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld,
 /* Number of step-kernel launches issued on this handle so far. */
 long long claw_launch_count(claw_handle* h);
 
+/* One 2D step (bc2 + step2, FP64) from caller-owned device buffers, with no
+ * device allocation.  No counterpart in the reference: it serves callers that
+ * cannot call cudaMalloc -- codes whose device memory all comes from their own
+ * pool or arena, memory-capped partitions, time loops that cannot take
+ * cudaMalloc's implicit device synchronisation.
+ *   q_in, q_out : device arrays [num_eqn][my][q_ld] (q_ld >= mx, even,
+ *                 16-byte aligned), distinct; q_out receives the new state
+ *   aux         : device array [num_aux][my+4][aux_ld] or NULL
+ *   stream      : a cudaStream_t (NULL = the default stream); the call waits
+ *                 for it and returns the Courant number in *cfl
+ * The step kernel's scratch (its 256-byte control block) is a static device
+ * array of the library: the first call on a device looks up its address (make
+ * that first call before any stream capture); calls that overlap on the GPU
+ * race on it; each call resets it.  Requests whose scratch would exceed the
+ * 256-byte maximum are rejected with CLAW_E_INVALID. */
+int claw_step2d_noalloc(const claw_config* cfg, const double* q_in, double* q_out,
+                        long long q_ld, const double* aux, long long aux_ld, double dt,
+                        double* cfl, void* stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* claw_last_error(void);
 
