@@ -15,13 +15,14 @@
 
 #include "../../include/claw_b200.h"
 #include "common.cuh"
+#include "host.h"
 #include "riemann.cuh"
 #include "step1d.cuh"
 #include "step2d.cuh"
 
 using namespace clawb200;
 
-namespace {
+namespace clawb200 {
 
 thread_local std::string g_err;
 
@@ -35,14 +36,9 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define CUDA_TRY(x)                                                                     \
-    do {                                                                                \
-        cudaError_t e_ = (x);                                                           \
-        if (e_ != cudaSuccess)                                                          \
-            return fail(CLAW_E_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));      \
-    } while (0)
+void set_last_error(const char* msg) { g_err = msg; }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
         cudaDriverEntryPointQueryResult qr;
@@ -55,7 +51,6 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// 3D tiled map over an SoA array: dims (n0, n1, n2) with pitches p1, p2 (elements).
 int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, long long n2,
               long long p1, long long p2, int box0, int box1, int box2) {
     auto fn = encode_fn();
@@ -72,24 +67,13 @@ int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, 
     return 0;
 }
 
+}  // namespace clawb200
+
+namespace {
+
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
-struct Geometry {
-    int dim, mx, my, mz, meqn, maux, es;
-    long long ld, fstride, ald, afstride;  // pitches in elements
-    void* q[2];
-    void* aux;
-    ClawCtl* ctl;
-    double dx, dy, dz;
-};
-
 // ------------------------------------------------------------------ runners ---
-struct Runner {
-    virtual ~Runner() {}
-    virtual int prepare(const claw_config& cfg, const Geometry& g) = 0;
-    virtual cudaError_t launch(cudaStream_t s) = 0;
-};
-
 template <class S, class M>
 struct Runner2D : Runner {
     Step2Args<S> args;
@@ -213,6 +197,12 @@ std::unique_ptr<Runner> runner2d(const claw_config& cfg, const S& s) {
 template <typename real>
 std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
     const int id = cfg.solver_id;
+    if (cfg.precision != CLAW_FP64) {
+        // fused / FP32 arithmetic: constant-coefficient acoustics runs in
+        // characteristic variables when the method allows it
+        auto r = make_char_runner(cfg);
+        if (r) return r;
+    }
     if (id == CLAW_SOLVER_ACOUSTICS_2D || id == CLAW_SOLVER_ACOUSTICS_1D) {
         const double rho = cfg.solver_params[0], bulk = cfg.solver_params[1];
         const double cc = std::sqrt(bulk / rho), zz = rho * cc, hz = 0.5 / zz;
@@ -254,11 +244,6 @@ __global__ void narrow_to_float(const double* src, float* dst, long long n) {
 }
 
 }  // namespace
-
-namespace clawb200 {
-// Error message for claw_last_error() from other translation units.
-void set_last_error(const char* msg) { g_err = msg; }
-}  // namespace clawb200
 
 struct claw_handle {
     claw_config cfg;
@@ -311,7 +296,6 @@ static int validate(const claw_config* c, SolverShape* sh) {
     for (int k = 0; k < c->num_waves; ++k)
         if (c->limiter[k] < 0 || c->limiter[k] > 5) return fail(CLAW_E_INVALID, "invalid limiter %d", c->limiter[k]);
     if (c->precision < CLAW_FP64 || c->precision > CLAW_FP32) return fail(CLAW_E_INVALID, "bad precision");
-    if (c->precision == CLAW_FP64_FMA) return fail(CLAW_E_UNSUPPORTED, "FMA variant is not built");
     return 0;
 }
 

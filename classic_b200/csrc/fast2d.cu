@@ -1,0 +1,87 @@
+// Characteristic-variable 2D acoustics runner (char2d.cuh).  This
+// translation unit is compiled with fused multiply-add contraction; it
+// serves CLAW_FP64_FMA and CLAW_FP32.
+#include <cstring>
+#include <memory>
+
+#include "char2d.cuh"
+#include "host.h"
+
+namespace clawb200 {
+
+namespace {
+
+template <typename real, int LIM>
+struct CharRunner : Runner {
+    CharArgs<real> args;
+    int grid = 1, smem = 0;
+
+    int prepare(const claw_config& cfg, const Geometry& g) override {
+        using R = CharRing<real>;
+        std::memset(&args, 0, sizeof(args));
+        const double rho = cfg.solver_params[0], bulk = cfg.solver_params[1];
+        const double cc = std::sqrt(bulk / rho), zz = rho * cc;
+        args.s = CharAcoustics2D<real>{(real)cc, (real)zz, (real)(0.5 / zz)};
+        args.q[0] = static_cast<real*>(g.q[0]);
+        args.q[1] = static_cast<real*>(g.q[1]);
+        args.ld = g.ld;
+        args.fstride = g.fstride;
+        args.mx = g.mx;
+        args.my = g.my;
+        args.nstrips = (g.mx + STRIP - 1) / STRIP;
+        args.bc[0] = cfg.bc_lower[0];
+        args.bc[1] = cfg.bc_upper[0];
+        args.bc[2] = cfg.bc_lower[1];
+        args.bc[3] = cfg.bc_upper[1];
+        args.lim = cfg.limiter[0];
+        args.dx = g.dx;
+        args.dy = g.dy;
+        args.ctl = g.ctl;
+        for (int k = 0; k < 2; ++k) {
+            const int rc = make_map3(&args.tmq[k], g.q[k], g.es, g.mx, g.my, 3, g.ld, g.fstride, R::W, 1, 3);
+            if (rc) return rc;
+        }
+        smem = R::SMEM;
+        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int dev = 0, nsm = 0, per_sm = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM>,
+                                                               32 * WARPS2D, smem));
+        if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
+        args.units = (long long)args.nstrips * g.my;
+        const long long want = args.units / 48 > 0 ? args.units / 48 : 1;
+        const long long full = (long long)nsm * per_sm * WARPS2D;
+        const long long nw = want < full ? want : full;
+        grid = (int)((nw + WARPS2D - 1) / WARPS2D);
+        args.nwarps = (int)nw;
+        return 0;
+    }
+
+    cudaError_t launch(cudaStream_t s) override {
+        step2_char_kernel<real, LIM><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        return cudaGetLastError();
+    }
+};
+
+template <typename real>
+std::unique_ptr<Runner> pick(int lim) {
+    if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4>());
+    return std::unique_ptr<Runner>(new CharRunner<real, -1>());
+}
+
+}  // namespace
+
+std::unique_ptr<Runner> make_char_runner(const claw_config& cfg) {
+    if (cfg.solver_id != CLAW_SOLVER_ACOUSTICS_2D || cfg.num_dim != 2) return nullptr;
+    if (cfg.order != 2 || cfg.transverse_waves != 2 || cfg.capa_index != 0 || cfg.use_fwaves)
+        return nullptr;
+    for (int k = 1; k < cfg.num_waves; ++k)
+        if (cfg.limiter[k] != cfg.limiter[0]) return nullptr;
+    if (cfg.precision == CLAW_FP32) return pick<float>(cfg.limiter[0]);
+    if (cfg.precision == CLAW_FP64_FMA) return pick<double>(cfg.limiter[0]);
+    return nullptr;
+}
+
+}  // namespace clawb200

@@ -1,0 +1,51 @@
+// Host-side pieces shared by the translation units of libclawb200.so:
+// the geometry of one grid on the device, the kernel-runner interface, error
+// reporting for claw_last_error() and TMA descriptor creation.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <memory>
+
+#include "../../include/claw_b200.h"
+#include "common.cuh"
+
+namespace clawb200 {
+
+struct Geometry {
+    int dim, mx, my, mz, meqn, maux, es;
+    long long ld, fstride, ald, afstride;  // pitches in elements
+    void* q[2];
+    void* aux;
+    ClawCtl* ctl;
+    double dx, dy, dz;
+};
+
+// One compiled step kernel bound to one grid.
+struct Runner {
+    virtual ~Runner() {}
+    virtual int prepare(const claw_config& cfg, const Geometry& g) = 0;
+    virtual cudaError_t launch(cudaStream_t s) = 0;
+};
+
+// Record an error message (claw_last_error) and return code.
+int fail(int code, const char* fmt, ...);
+void set_last_error(const char* msg);
+
+// 3D tiled TMA map over an SoA array: dims (n0, n1, n2), pitches p1, p2 in
+// elements, element size es (4 or 8), box (box0, box1, box2).
+int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, long long n2,
+              long long p1, long long p2, int box0, int box1, int box2);
+
+// Characteristic-variable kernel for constant-coefficient 2D acoustics
+// (char2d.cuh, built with fused multiply-add); nullptr if cfg is not served.
+std::unique_ptr<Runner> make_char_runner(const claw_config& cfg);
+
+}  // namespace clawb200
+
+#define CUDA_TRY(x)                                                                      \
+    do {                                                                                 \
+        cudaError_t e_ = (x);                                                            \
+        if (e_ != cudaSuccess)                                                           \
+            return ::clawb200::fail(CLAW_E_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)

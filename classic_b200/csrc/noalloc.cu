@@ -29,7 +29,7 @@
 using namespace clawb200;
 
 namespace clawb200 {
-void set_last_error(const char* msg);  // claw_b200.cu: message for claw_last_error()
+void set_last_error(const char* msg);  // message for claw_last_error()
 }
 
 namespace {

@@ -160,3 +160,49 @@ def test_fp32_variant_tracks_fp64():
     assert ig == io == 0 and sg["steps_taken"] == so["steps_taken"]
     assert np.all(rel_diff(g.get_q(), o.get_q()) < 2e-5)
     g.close()
+
+
+# ---------------------------------------------------------------------------
+# Characteristic-variable path (CLAW_FP64_FMA): same algorithm with fused
+# multiply-adds and strength ratios; same dt sequence, q within 1e-12.
+@pytest.mark.parametrize("bc", BCS)
+def test_fast_fp64_matches_oracle(bc):
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(61, 45, seed=11, bc=bc)
+    g, o = _pair(rd, solver, params, q0, precision="fp64_fma")
+    for _ in range(20):
+        assert g.step(0.004) == o.step(0.004)  # Courant number bit-identical
+    assert np.all(rel_diff(g.get_q(), o.get_q()) < 1e-12)
+    g.close()
+
+
+def test_fast_fp64_full_run_4096_within_1e12():
+    """The benchmark workload end to end: 2D radial acoustics, 4096^2, MC,
+    t = 0 -> 0.6 (~2700 steps).  The fast path against the reference-order
+    path (itself bit-identical to the oracle): identical dt sequence, max
+    relative difference per field <= 1e-12."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
+    out = {}
+    for prec in ("fp64", "fp64_fma"):
+        s = Solver(rd.clawdata, solver, params, precision=prec)
+        s.set_q(q0)
+        info, st = s.advance(0.0, 0.6, 0.01)
+        assert info == 0
+        out[prec] = (s.get_q(), st)
+        s.close()
+    (qa, sa), (qb, sb) = out["fp64"], out["fp64_fma"]
+    for key in ("t_reached", "steps_taken", "dt_next", "cfl_max_seen", "steps_rejected"):
+        assert sa[key] == sb[key], key
+    assert sa["steps_taken"] > 2000
+    d = rel_diff(qb, qa)
+    assert np.all(d <= 1e-12), d
+
+
+def test_fast_fp32_tracks_fp64_all_bcs():
+    for bc in BCS:
+        rd, solver, params, q0, _ = problems.random_acoustics_2d(70, 33, seed=2, bc=bc)
+        g, o = _pair(rd, solver, params, q0, precision="fp32")
+        for _ in range(10):
+            cg, co = g.step(0.004), o.step(0.004)
+            assert abs(cg - co) <= 1e-7 * co
+        assert np.all(rel_diff(g.get_q(), o.get_q()) < 1e-5)
+        g.close()
