@@ -48,15 +48,38 @@ __device__ __forceinline__ float rcp_newton(float a) {
     return fmaf(y, e, y);
 }
 
-// phi(r) of inlinelimiter.f90:71-97 for a strength ratio r = num/den;
-// den == 0 (no wave) gives a zero limited strength, as the reference skips it.
+// x with the sign of s flipped in (x * sign(s)), and copysign, by bit operations.
+__device__ __forceinline__ double sign_times(double x, double s) {
+    return __longlong_as_double(__double_as_longlong(x) ^
+                                (__double_as_longlong(s) & (long long)0x8000000000000000ull));
+}
+__device__ __forceinline__ float sign_times(float x, float s) {
+    return __int_as_float(__float_as_int(x) ^ (__float_as_int(s) & (int)0x80000000u));
+}
+
+// phi(r) * a of inlinelimiter.f90:71-97 for the strength ratio r = n / a
+// (n = upwind neighbour's strength).  For minmod, superbee and MC the product
+// has an exact division-free form: with A = |a| and N = n sign(a),
+//   minmod   phi a = sign(a) max(0, min(A, N))
+//   superbee phi a = sign(a) max(0, min(A, 2N), min(2A, N))
+//   MC       phi a = sign(a) max(0, min(2A, 2N, (A+N)/2))
+// (multiply phi's arguments by a, reversing min/max when a < 0).  a == 0 gives
+// 0, as the reference skips a zero wave.  Other limiters use the ratio.
 template <typename real, int LIM>
-__device__ __forceinline__ real limited_strength(real a, real anb, int lim_rt) {
-    const real inv = rcp_newton(a != real(0) ? a : real(1));
-    const real r = anb * inv;
+__device__ __forceinline__ real limited_strength(real a, real n, int lim_rt) {
     const int lim = LIM >= 0 ? LIM : lim_rt;
-    const real ph = lim == 0 ? real(1) : phi_limiter<real>(lim, r);
-    return ph * a;
+    if (LIM == 1 || LIM == 2 || LIM == 4) {
+        const real A = fabs(a), N = sign_times(n, a);
+        real m;
+        if (LIM == 1) m = fmin(A, N);
+        else if (LIM == 2) m = fmax(fmin(A, real(2) * N), fmin(real(2) * A, N));
+        else m = real(2) * fmin(fmin(A, N), real(0.25) * (A + N));
+        return sign_times(fmax(real(0), m), a);
+    }
+    if (lim == 0) return a;
+    const real inv = rcp_newton(a != real(0) ? a : real(1));
+    const real r = n * inv;
+    return phi_limiter<real>(lim, r) * a;
 }
 
 template <typename real>
@@ -74,17 +97,39 @@ struct CharArgs {
     CharAcoustics2D<real> s;
 };
 
+// Two columns per lane: a warp covers 64 columns and writes STRIP2 = 60.
+constexpr int STRIP2 = 60;
+static_assert(STRIP2 % 4 == 0, "strip start must stay a multiple of 4 for TMA");
+
 template <typename real>
 struct CharRing {
-    static constexpr int W = BoxW<real>::value;
+    // columns b-4 .. b+61 (b-4 keeps the box start 16-byte aligned)
+    static constexpr int XQ = 4;
+    static constexpr int W = sizeof(real) == 8 ? 66 : 68;
     static constexpr int QB = 3 * W * (int)sizeof(real);
     static constexpr int SLOT = ((QB + 127) / 128) * 128;
     static constexpr int WARP_BYTES = RING * SLOT;
     static constexpr int SMEM = WARPS2D * WARP_BYTES + WARPS2D * RING * 8 + 64;
 };
 
-template <typename real, int LIM>
-__global__ void __launch_bounds__(32 * WARPS2D, sizeof(real) == 8 ? 5 : 6)
+// One column's q source in the ring (or, for a periodic ghost outside the
+// box, in global memory) and its wall sign flip.
+struct ColSrc {
+    int idx;   // ring index
+    int src;   // interior column (global fallback)
+    bool neg;  // wall: negate the normal velocity
+    bool glob; // periodic ghost outside the ring box
+};
+
+#ifndef CLAW_CHAR_MINB
+#define CLAW_CHAR_MINB 3  // 168 registers, 12 warps per SM: no spills in FP64
+#endif
+
+// PX: x-boundaries are periodic, so halo lanes of the edge strips may need
+// a column from the far side of the grid that is not in the ring box; those
+// come from global memory.  Without PX that path is compiled out.
+template <typename real, int LIM, bool PX>
+__global__ void __launch_bounds__(32 * WARPS2D, CLAW_CHAR_MINB)
 step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     using R = CharRing<real>;
     constexpr int W = R::W;
@@ -101,15 +146,15 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     const CUtensorMap* tmq = &A.tmq[cur];
     const real c = A.s.cc, Z = A.s.zz, h = A.s.hz;
     const real cZ = c * Z;
-    // per-direction constants: kappa = c(1 - c dt/dx) (second-order
-    // coefficient of flux2.f90:156-157), fadd = kappa/2 (...), transverse
-    // gamma = dt/dx c/4 and delta = dt/dx c/(4Z) scaled by the other dt/d.
+    // kappa = c(1 - c dt/dx): second-order coefficient (flux2.f90:156-157);
+    // fadd = kappa/2 (Z(b2-b1), b1+b2); transverse gamma = (dt/dx) c/4,
+    // delta = (dt/dx) c/(4Z), each scaled by the other direction's dt/d.
     const real kx = c * (real(1) - c * dtdx), ky = c * (real(1) - c * dtdy);
-    const real fxp = real(0.5) * kx * Z, fxu = real(0.5) * kx;  // x: F = (fxp(a2-a1), fxu(a1+a2))
+    const real fxp = real(0.5) * kx * Z, fxu = real(0.5) * kx;
     const real fyp = real(0.5) * ky * Z, fyv = real(0.5) * ky;
     const real gx = dtdy * (dtdx * c * real(0.25)), dx4 = dtdy * (dtdx * c * real(0.25) / Z);
     const real gy = dtdx * (dtdy * c * real(0.25)), dy4 = dtdx * (dtdy * c * real(0.25) / Z);
-    const real qpx = dtdx * cZ, qux = dtdx * c;  // Godunov: qadd from a1, a2 (x)
+    const real qpx = dtdx * cZ, qux = dtdx * c;
     const real qpy = dtdy * cZ, qvy = dtdy * c;
 
     extern __shared__ __align__(128) unsigned char smem[];
@@ -136,18 +181,22 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
         const int r0 = (int)(u0 % my);
         const int nr = (int)min((long long)(my - r0), u1 - u0);
         u0 += nr;
-        const int b = strip * STRIP;
-        const int col = b - 1 + lane;
-        const int x0 = b - BoxW<real>::XQ;
+        const int b = strip * STRIP2;
+        const int c0 = b - 2 + 2 * lane, c1 = c0 + 1;  // this lane's two columns
+        const int x0 = b - R::XQ;
         const int rfirst = r0 - 2, rlast = r0 + nr + 1;
         const int nrows = rlast - rfirst + 1;
-        bool negm, negc;
-        const int sm = bc_map(col - 1, mx, A.bc[0], A.bc[1], negm);
-        const int sc = bc_map(col, mx, A.bc[0], A.bc[1], negc);
-        const bool gm = (sm - x0) < 0 || (sm - x0) >= W;
-        const bool gc = (sc - x0) < 0 || (sc - x0) >= W;
-        const bool any_global = __any_sync(FULL, gm || gc);
-        const int im = gm ? 0 : sm - x0, icc = gc ? 0 : sc - x0;
+        auto colsrc = [&](int col) -> ColSrc {
+            ColSrc cs;
+            cs.src = bc_map(col, mx, A.bc[0], A.bc[1], cs.neg);
+            cs.glob = (cs.src - x0) < 0 || (cs.src - x0) >= W;
+            cs.idx = cs.glob ? 0 : cs.src - x0;
+            return cs;
+        };
+        const ColSrc sM = colsrc(c0 - 1), s0 = colsrc(c0), s1 = colsrc(c1);
+        const bool any_global = PX && __any_sync(FULL, sM.glob || s0.glob || s1.glob);
+        const bool out_lane = lane >= 1 && lane <= 30;
+        const bool out0 = out_lane && c0 < mx, out1 = out_lane && c1 < mx;
 
         auto seq_of = [&](int r) -> uint32_t { return seq_base + (uint32_t)(r - rfirst); };
         auto issue = [&](int r) {
@@ -167,108 +216,146 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
             const uint32_t sq = seq_of(r);
             return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u);
         };
-        auto load_q = [&](int r, real* qm, real* qc) {
-            const real* sq = reinterpret_cast<const real*>(ring + (int)(seq_of(r) & (RING - 1)) * R::SLOT);
-            bool nyneg;
-            const int sr = bc_map(r, my, A.bc[2], A.bc[3], nyneg);
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                real vm = sq[m * W + im];
-                real vc = sq[m * W + icc];
-                if (any_global) {
-                    if (gm) vm = qold[m * A.fstride + (long long)sr * A.ld + sm];
-                    if (gc) vc = qold[m * A.fstride + (long long)sr * A.ld + sc];
-                }
-                if (m == 1) { vm = negm ? -vm : vm; vc = negc ? -vc : vc; }
-                if (m == 2 && nyneg) { vm = -vm; vc = -vc; }
-                qm[m] = vm;
-                qc[m] = vc;
+        // field m of column cs at row r (boundary conditions applied)
+        auto fetch = [&](const real* sq, int sr, bool nyneg, const ColSrc& cs, int m) -> real {
+            real v = sq[m * W + cs.idx];
+            if constexpr (PX) {
+                if (any_global && cs.glob) v = qold[m * A.fstride + (long long)sr * A.ld + cs.src];
             }
+            if (m == 1 && cs.neg) v = -v;
+            if (m == 2 && nyneg) v = -v;
+            return v;
+        };
+        auto row_ptr = [&](int r) -> const real* {
+            return reinterpret_cast<const real*>(ring + (int)(seq_of(r) & (RING - 1)) * R::SLOT);
         };
 
-        real qm_t[3], qc_t[3], qm_n[3], qc_n[3];
-        real q2p[3] = {real(0), real(0), real(0)};  // x-part of (c, t) before row t+1
-        real axp = real(0), axv = real(0);         // x-slice t-1 -> row t (p, v)
-        real a1y = real(0), a2y = real(0);         // y-interface t strengths
-        real a2y_lo = real(0);                     // a2 of y-interface t-1
-        real A2y_lo = real(0), Fpy_lo = real(0), Fvy_lo = real(0);  // of y-interface t-1
+        // carried per column k = 0, 1
+        real q2p[2][3] = {};          // x-part of (c_k, t) awaiting row t+1's transfer
+        real axp[2] = {}, axv[2] = {};  // x-slice t-1 -> row t (p, v)
+        real a1y[2] = {}, a2y[2] = {};  // y-interface t strengths
+        real a2y_lo[2] = {}, A2y_lo[2] = {}, Fpy_lo[2] = {}, Fvy_lo[2] = {};  // y-interface t-1
         int last_issued = rfirst + (nrows < RING ? nrows : RING) - 1;
         int fail_row = rlast + 1;
 
         if (!wait_row(rfirst) || !wait_row(rfirst + 1)) { failed = true; fail_row = rfirst; }
         if (!failed) {
-            load_q(rfirst, qm_t, qc_t);
-            load_q(rfirst + 1, qm_n, qc_n);
-            const real dp = qc_n[0] - qc_t[0], dv = qc_n[2] - qc_t[2];
-            a1y = (Z * dv - dp) * h;
-            a2y = (Z * dv + dp) * h;
+            bool ng0, ng1;
+            const int sr0 = bc_map(rfirst, my, A.bc[2], A.bc[3], ng0);
+            const int sr1 = bc_map(rfirst + 1, my, A.bc[2], A.bc[3], ng1);
+            const real* q0p = row_ptr(rfirst);
+            const real* q1p = row_ptr(rfirst + 1);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) { qm_t[m] = qm_n[m]; qc_t[m] = qc_n[m]; }
+            for (int k = 0; k < 2; ++k) {
+                const ColSrc& cs = k ? s1 : s0;
+                const real dp = fetch(q1p, sr1, ng1, cs, 0) - fetch(q0p, sr0, ng0, cs, 0);
+                const real dv = fetch(q1p, sr1, ng1, cs, 2) - fetch(q0p, sr0, ng0, cs, 2);
+                a1y[k] = (Z * dv - dp) * h;
+                a2y[k] = (Z * dv + dp) * h;
+            }
         }
 
+        // two rows per trip: the carried state rotates by renaming, not copies
+#pragma unroll 2
         for (int t = r0 - 1; t <= r0 + nr && !failed; ++t) {
             if (!wait_row(t + 1)) { failed = true; fail_row = t + 1; break; }
-            load_q(t + 1, qm_n, qc_n);
-
-            // ---- x-slice t: interface at column col ----
-            const real dpx = qc_t[0] - qm_t[0], dux = qc_t[1] - qm_t[1];
-            const real a1 = (Z * dux - dpx) * h;
-            const real a2 = (Z * dux + dpx) * h;
-            const real a1r = __shfl_down_sync(FULL, a1, 1);  // interface col+1
-            const real a2l = __shfl_up_sync(FULL, a2, 1);    // interface col-1
-            const real al1 = limited_strength<real, LIM>(a1, a1r, A.lim);  // s<0: upwind is col+1
-            const real al2 = limited_strength<real, LIM>(a2, a2l, A.lim);  // s>0: upwind is col-1
-            const real Fp = fxp * (al2 - al1), Fu = fxu * (al1 + al2);
-            const real A1 = fma(cZ, a1, real(2) * Fp);   // pressure of amdq + cqxx
-            const real A2 = fma(cZ, a2, real(-2) * Fp);  // pressure of apdq - cqxx
-            const real Fpr = __shfl_down_sync(FULL, Fp, 1);
-            const real Fur = __shfl_down_sync(FULL, Fu, 1);
-            const real A1r = __shfl_down_sync(FULL, A1, 1);
-            const real S = A1r + A2;
-            const real gS = gx * S, dS = dx4 * S;
-            // x-part of cell (col, t): q + (row t-1's transfer) + qadd - dt/dx dF - dt/dy dG
-            const real nq0 = (qc_t[0] + axp) - qpx * (a2 + a1r) - dtdx * (Fpr - Fp) + real(2) * gS;
-            const real nq1 = qc_t[1] + qux * (a1r - a2) - dtdx * (Fur - Fu);
-            const real nq2 = qc_t[2] + axv;
-            // row t completes the x-part of (col, t-1)
-            const real q3p = q2p[0] - gS, q3u = q2p[1], q3v = q2p[2] + dS;
-            q2p[0] = nq0;
-            q2p[1] = nq1;
-            q2p[2] = nq2;
-            axp = -gS;
-            axv = -dS;
-
-            // ---- y-interface t+1 raw; y-interface t limited; y-part of (col, t-1) ----
-            const real dpy = qc_n[0] - qc_t[0], dvy = qc_n[2] - qc_t[2];
-            const real a1n = (Z * dvy - dpy) * h;
-            const real a2n = (Z * dvy + dpy) * h;
-            const real bl1 = limited_strength<real, LIM>(a1y, a1n, A.lim);    // upwind t+1
-            const real bl2 = limited_strength<real, LIM>(a2y, a2y_lo, A.lim); // upwind t-1
-            const real Fpy = fyp * (bl2 - bl1), Fvy = fyv * (bl1 + bl2);
-            const real A1y = fma(cZ, a1y, real(2) * Fpy);   // into cell t-1
-            const real A2y = fma(cZ, a2y, real(-2) * Fpy);  // into cell t
-            const real Sy = A1y + A2y_lo;
-            const real hS = gy * Sy, kS = dy4 * Sy;
-            const real hSl = __shfl_up_sync(FULL, hS, 1), kSl = __shfl_up_sync(FULL, kS, 1);
-            const real hSr = __shfl_down_sync(FULL, hS, 1), kSr = __shfl_down_sync(FULL, kS, 1);
-            const real o0 = q3p - qpy * (a2y_lo + a1y) - dtdy * (Fpy - Fpy_lo) + real(2) * hS - hSl - hSr;
-            const real o1 = q3u - kSl + kSr;
-            const real o2 = q3v + qvy * (a1y - a2y_lo) - dtdy * (Fvy - Fvy_lo);
-            if ((t - 1 >= r0) && (lane >= 1) && (lane <= STRIP) && (col < mx)) {
-                real* dst = qnew + (long long)(t - 1) * A.ld + col;
-                dst[0] = o0;
-                dst[A.fstride] = o1;
-                dst[2 * A.fstride] = o2;
-            }
-            a2y_lo = a2y;
-            A2y_lo = A2y;
-            Fpy_lo = Fpy;
-            Fvy_lo = Fvy;
-            a1y = a1n;
-            a2y = a2n;
+            bool ngt, ngn;
+            const int srt = bc_map(t, my, A.bc[2], A.bc[3], ngt);
+            const int srn = bc_map(t + 1, my, A.bc[2], A.bc[3], ngn);
+            const real* qt = row_ptr(t);
+            const real* qn = row_ptr(t + 1);
+            // row t: p, u at columns c0-1, c0, c1; v at c0, c1.  row t+1: p, v.
+            const real pM = fetch(qt, srt, ngt, sM, 0), uM = fetch(qt, srt, ngt, sM, 1);
+            real p[2], u[2], v[2], pn[2], vn[2];
 #pragma unroll
-            for (int m = 0; m < 3; ++m) { qm_t[m] = qm_n[m]; qc_t[m] = qc_n[m]; }
+            for (int k = 0; k < 2; ++k) {
+                const ColSrc& cs = k ? s1 : s0;
+                p[k] = fetch(qt, srt, ngt, cs, 0);
+                u[k] = fetch(qt, srt, ngt, cs, 1);
+                v[k] = fetch(qt, srt, ngt, cs, 2);
+                pn[k] = fetch(qn, srn, ngn, cs, 0);
+                vn[k] = fetch(qn, srn, ngn, cs, 2);
+            }
 
+            // ---- x-slice t: interfaces I0 = (c0-1 | c0) and I1 = (c0 | c1) ----
+            const real a1_0 = (Z * (u[0] - uM) - (p[0] - pM)) * h;
+            const real a2_0 = (Z * (u[0] - uM) + (p[0] - pM)) * h;
+            const real a1_1 = (Z * (u[1] - u[0]) - (p[1] - p[0])) * h;
+            const real a2_1 = (Z * (u[1] - u[0]) + (p[1] - p[0])) * h;
+            const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
+            const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
+            // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
+            const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
+            const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim);
+            const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
+            const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim);
+            const real Fp0 = fxp * (l2_0 - l1_0), Fu0 = fxu * (l1_0 + l2_0);
+            const real Fp1 = fxp * (l2_1 - l1_1), Fu1 = fxu * (l1_1 + l2_1);
+            const real A1_0 = fma(cZ, a1_0, real(2) * Fp0), A2_0 = fma(cZ, a2_0, real(-2) * Fp0);
+            const real A1_1 = fma(cZ, a1_1, real(2) * Fp1), A2_1 = fma(cZ, a2_1, real(-2) * Fp1);
+            const real FpR = __shfl_down_sync(FULL, Fp0, 1), FuR = __shfl_down_sync(FULL, Fu0, 1);
+            const real A1R = __shfl_down_sync(FULL, A1_0, 1);
+            // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0
+            real q3[2][3];
+            {
+                const real S0 = A1_1 + A2_0, S1 = A1R + A2_1;
+                const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
+                const real n00 = (p[0] + axp[0]) - qpx * (a2_0 + a1_1) - dtdx * (Fp1 - Fp0) + real(2) * gS0;
+                const real n01 = u[0] + qux * (a1_1 - a2_0) - dtdx * (Fu1 - Fu0);
+                const real n02 = v[0] + axv[0];
+                const real n10 = (p[1] + axp[1]) - qpx * (a2_1 + a1_R) - dtdx * (FpR - Fp1) + real(2) * gS1;
+                const real n11 = u[1] + qux * (a1_R - a2_1) - dtdx * (FuR - Fu1);
+                const real n12 = v[1] + axv[1];
+                q3[0][0] = q2p[0][0] - gS0; q3[0][1] = q2p[0][1]; q3[0][2] = q2p[0][2] + dS0;
+                q3[1][0] = q2p[1][0] - gS1; q3[1][1] = q2p[1][1]; q3[1][2] = q2p[1][2] + dS1;
+                q2p[0][0] = n00; q2p[0][1] = n01; q2p[0][2] = n02;
+                q2p[1][0] = n10; q2p[1][1] = n11; q2p[1][2] = n12;
+                axp[0] = -gS0; axv[0] = -dS0;
+                axp[1] = -gS1; axv[1] = -dS1;
+            }
+
+            // ---- y: interface t+1 raw, interface t limited, y-part of (c_k, t-1) ----
+            real hS[2], kS[2], o[2][3], Fpy[2], Fvy[2], A2y[2], a1n[2], a2n[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const real dp = pn[k] - p[k], dv = vn[k] - v[k];
+                a1n[k] = (Z * dv - dp) * h;
+                a2n[k] = (Z * dv + dp) * h;
+                const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
+                const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim); // upwind t-1
+                Fpy[k] = fyp * (b2 - b1);
+                Fvy[k] = fyv * (b1 + b2);
+                const real A1y = fma(cZ, a1y[k], real(2) * Fpy[k]);  // into cell t-1
+                A2y[k] = fma(cZ, a2y[k], real(-2) * Fpy[k]);         // into cell t
+                const real Sy = A1y + A2y_lo[k];
+                hS[k] = gy * Sy;
+                kS[k] = dy4 * Sy;
+                o[k][0] = q3[k][0] - qpy * (a2y_lo[k] + a1y[k]) - dtdy * (Fpy[k] - Fpy_lo[k]) + real(2) * hS[k];
+                o[k][1] = q3[k][1];
+                o[k][2] = q3[k][2] + qvy * (a1y[k] - a2y_lo[k]) - dtdy * (Fvy[k] - Fvy_lo[k]);
+            }
+            // transverse transfers: column c0 from c0-1 (lane-1's c1) and c1;
+            // column c1 from c0 and c1+1 (lane+1's c0)
+            const real hL = __shfl_up_sync(FULL, hS[1], 1), kL = __shfl_up_sync(FULL, kS[1], 1);
+            const real hR = __shfl_down_sync(FULL, hS[0], 1), kR = __shfl_down_sync(FULL, kS[0], 1);
+            o[0][0] = o[0][0] - hL - hS[1];
+            o[0][1] = o[0][1] - kL + kS[1];
+            o[1][0] = o[1][0] - hS[0] - hR;
+            o[1][1] = o[1][1] - kS[0] + kR;
+            if (t - 1 >= r0) {
+                real* dst = qnew + (long long)(t - 1) * A.ld + c0;
+                if (out0) { dst[0] = o[0][0]; dst[A.fstride] = o[0][1]; dst[2 * A.fstride] = o[0][2]; }
+                if (out1) { dst[1] = o[1][0]; dst[A.fstride + 1] = o[1][1]; dst[2 * A.fstride + 1] = o[1][2]; }
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                a2y_lo[k] = a2y[k];
+                A2y_lo[k] = A2y[k];
+                Fpy_lo[k] = Fpy[k];
+                Fvy_lo[k] = Fvy[k];
+                a1y[k] = a1n[k];
+                a2y[k] = a2n[k];
+            }
             __syncwarp();
             if (t - 1 + RING <= rlast) {
                 if (lane == 0) issue(t - 1 + RING);
@@ -282,10 +369,9 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
         }
         seq_base += (uint32_t)nrows;
     }
-    // Courant number as flux2 forms it (dt/dx * c over the x-interfaces,
-    // dt/dy * c over the y-interfaces; constant speeds)
-    double cfl = any_work ? fmax(dtdx_d * (double)c, dtdy_d * (double)c) : 0.0;
-    if (!any_work) cfl = 0.0;
+    // Courant number as flux2 forms it (dt/dx * c over x-interfaces, dt/dy * c
+    // over y-interfaces; the speeds are constant)
+    const double cfl = any_work ? fmax(dtdx_d * (double)c, dtdy_d * (double)c) : 0.0;
     cta_cfl_and_control(ctl, cfl, red);
 }
 

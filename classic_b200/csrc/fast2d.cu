@@ -11,7 +11,7 @@ namespace clawb200 {
 
 namespace {
 
-template <typename real, int LIM>
+template <typename real, int LIM, bool PX>
 struct CharRunner : Runner {
     CharArgs<real> args;
     int grid = 1, smem = 0;
@@ -28,7 +28,7 @@ struct CharRunner : Runner {
         args.fstride = g.fstride;
         args.mx = g.mx;
         args.my = g.my;
-        args.nstrips = (g.mx + STRIP - 1) / STRIP;
+        args.nstrips = (g.mx + STRIP2 - 1) / STRIP2;
         args.bc[0] = cfg.bc_lower[0];
         args.bc[1] = cfg.bc_upper[0];
         args.bc[2] = cfg.bc_lower[1];
@@ -42,12 +42,12 @@ struct CharRunner : Runner {
             if (rc) return rc;
         }
         smem = R::SMEM;
-        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM>,
+        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, PX>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM>,
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, PX>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
         args.units = (long long)args.nstrips * g.my;
@@ -60,15 +60,21 @@ struct CharRunner : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_char_kernel<real, LIM><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        step2_char_kernel<real, LIM, PX><<<grid, 32 * WARPS2D, smem, s>>>(args);
         return cudaGetLastError();
     }
 };
 
+template <typename real, bool PX>
+std::unique_ptr<Runner> pick_lim(int lim) {
+    if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, PX>());
+    return std::unique_ptr<Runner>(new CharRunner<real, -1, PX>());
+}
+
 template <typename real>
-std::unique_ptr<Runner> pick(int lim) {
-    if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4>());
-    return std::unique_ptr<Runner>(new CharRunner<real, -1>());
+std::unique_ptr<Runner> pick(const claw_config& cfg) {
+    const bool px = cfg.bc_lower[0] == BC_PERIODIC || cfg.bc_upper[0] == BC_PERIODIC;
+    return px ? pick_lim<real, true>(cfg.limiter[0]) : pick_lim<real, false>(cfg.limiter[0]);
 }
 
 }  // namespace
@@ -79,8 +85,8 @@ std::unique_ptr<Runner> make_char_runner(const claw_config& cfg) {
         return nullptr;
     for (int k = 1; k < cfg.num_waves; ++k)
         if (cfg.limiter[k] != cfg.limiter[0]) return nullptr;
-    if (cfg.precision == CLAW_FP32) return pick<float>(cfg.limiter[0]);
-    if (cfg.precision == CLAW_FP64_FMA) return pick<double>(cfg.limiter[0]);
+    if (cfg.precision == CLAW_FP32) return pick<float>(cfg);
+    if (cfg.precision == CLAW_FP64_FMA) return pick<double>(cfg);
     return nullptr;
 }
 
