@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""Benchmark: 2D radial acoustics, plain FP64, 4096^2 cells, t_final = 0.6.
+"""Benchmark: 2D radial acoustics, FP64, 4096^2 cells, t_final = 0.6.
 
 One "step" is one claw2 call over one output interval (dtout = t_final/20,
 the unit in which claw2ez hands the state back to the host), i.e. ~137
@@ -15,8 +15,14 @@ cells / device time.
   roofline : the step kernel's algorithmic bytes (read q + write q,
              48 B per cell-update) / its average launch time, CUDA events on
              the library's stream over the timed region
+  variants : the same frames on the reference-order FP64 kernel (bit-identical
+             to the CPU restatement) and on the FP32 path
   cpu_baseline : the CPU restatement of step2/flux2 (the oracle) timed on
              this host on a bounded sample (whole 4096^2 steps)
+
+The headline arithmetic is FP64 with fused multiply-adds in characteristic
+variables (precision "fp64_fma"): the same algorithm and dt sequence as the
+reference-order path, within 1e-12 relative of it over the full run.
 
 --impl reference times that CPU restatement alone on the same metric.
 Under torchrun with N > 1 each rank runs an independent replica (the
@@ -42,6 +48,20 @@ N_CELLS = 4096
 NOUT = 20
 TFINAL = 0.6
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def traffic_per_launch(precision, cells):
+    """DRAM bytes (read + write) per launch of the step kernel, scaled from
+    the ncu capture summarised in profiles/ (bytes per cell-update at a size
+    larger than L2); None when no capture is recorded."""
+    p = os.path.join(ROOT, "profiles", "dram_bytes_per_cell.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and not line.startswith("#") and parts[0] == precision:
+            return float(parts[1]) * cells
+    return None
 
 
 def load_peaks():
@@ -167,9 +187,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_CELLS)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64_fma", choices=["fp64_fma", "fp64", "fp32"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -274,23 +295,42 @@ def main():
                "ms_per_step": ems / args.steps}
 
     # ---- roofline of the step kernel (algorithmic bytes per launch)
-    es = 8 if args.precision == "fp64" else 4
+    es = 4 if args.precision == "fp32" else 8
     bytes_per_launch = 2 * 3 * es * cells
     per_launch_ms = kms / max(launches, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peaks = load_peaks()
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "step2_traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get(f"{args.precision}_{n}")
-        except Exception:
-            traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                "peak_source": peaks["source"], "kernel": "step2_kernel",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic_per_launch(args.precision, cells),
+                "peak_source": peaks["source"],
+                "kernel": "step2_char_kernel" if args.precision != "fp64" else "step2_kernel",
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "avg_launch_ms": per_launch_ms}
+
+    # ---- the other arithmetic variants on the same frames (kernel-level rate)
+    variants = {}
+    if not args.no_variants:
+        for prec in ("fp64", "fp64_fma", "fp32"):
+            if prec == args.precision:
+                continue
+            v = Solver(cd, solver, params, precision=prec)
+            v.set_q(q0)
+            t, dt, vsteps, vms, vl = 0.0, float(cd.dt_initial), 0, 0.0, 0
+            for _ in range(2):
+                info, st = v.advance(t, t + dtout, dt)
+                t, dt = st["t_reached"], st["dt_next"]
+                vsteps += st["steps_taken"]
+                vms += st["device_ms"]
+                vl += st["launches"]
+            v.close()
+            ves = 4 if prec == "fp32" else 8
+            vpl = vms / max(vl, 1)
+            variants[prec] = {"cell_updates_per_s": cells * vsteps / (vms * 1e-3),
+                              "avg_launch_ms": vpl,
+                              "hbm_frac": 2 * 3 * ves * cells / (vpl * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                              "parity": {"fp64": "bit-identical to the CPU restatement",
+                                         "fp64_fma": "within 1e-12 relative of fp64, same dt sequence",
+                                         "fp32": "within 1e-5 relative of fp64"}[prec]}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_steps > 0:
@@ -304,10 +344,13 @@ def main():
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic",
-            "config": {"workload": f"2D radial acoustics {args.precision.upper()} {n}^2, "
-                                   "MC limiter, transverse 2, extrap BCs, t_final 0.6",
+            "config": {"workload": f"2D radial acoustics {n}^2, MC limiter, transverse 2, "
+                                   "extrap BCs, t_final 0.6",
+                       "arithmetic": {"fp64_fma": "FP64, fused multiply-add, characteristic variables",
+                                      "fp64": "FP64, reference operation order",
+                                      "fp32": "FP32 update, FP64 CFL/dt/time"}[args.precision],
                        "step": f"one claw2 call over dtout = {dtout:g} (~{steps / args.steps:.0f} "
                                "time steps)",
                        "time_steps_timed": steps, "cells": cells,
@@ -318,6 +361,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "variants": variants,
         }
         print(json.dumps(line), flush=True)
     s.close()
