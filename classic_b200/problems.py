@@ -196,3 +196,97 @@ def random_acoustics_2d(mx, my, seed=0, bc=("extrap", "extrap", "extrap", "extra
     q0[1] = 0.2 * rng.standard_normal((my, mx))
     q0[2] = 0.2 * rng.standard_normal((my, mx))
     return rd, solver, params, q0, None
+
+
+# ------------------------------------------------------------------- 3D ---
+def _two_layer_aux(mx, my, mz, zlower, dz, below, above):
+    """aux[maux=2][mz+4][my+4][mx+4] = (Z, c) by the sign of the cell-centre z,
+    ghost cells included (examples/acoustics_3d_heterogeneous/setaux.f)."""
+    k = np.arange(-1, mz + 3, dtype=np.float64)
+    zcell = zlower + (k - 0.5) * dz
+    lower = zcell < 0.0
+    aux = np.empty((2, mz + 4, my + 4, mx + 4))
+    for m in range(2):
+        aux[m] = np.where(lower, below[m], above[m])[:, None, None]
+    return aux
+
+
+def acoustics_3d_heterogeneous(n=20, nout=2, tfinal=1.0):
+    """examples/acoustics_3d_heterogeneous (setrun.py, setprob.f, setaux.f,
+    qinit.f, bc3.f) with the regression test's overrides
+    (test_acoustics_3d_heterogeneous.py:17-19): (Z, c) = (2, 2) below z=0 and
+    (1, 1) above, q0 = 0, van Leer, transverse_waves 22, and the piston wall
+    ('user' BC) at z-upper driving the flow."""
+    rd = ClawRunData("classic", 3)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    for k, v in (("z1", 2.0), ("c1", 2.0), ("z2", 1.0), ("c2", 1.0)):
+        pd.add_param(k, v)
+    cd = rd.clawdata
+    cd.lower, cd.upper, cd.num_cells = [-1.0] * 3, [1.0] * 3, [n, n, n]
+    cd.num_eqn, cd.num_aux, cd.capa_index = 4, 2, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 0.01, 1e9
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.transverse_waves, cd.dimensional_split = 2, 22, "unsplit"
+    cd.num_waves, cd.limiter = 2, [3, 3]
+    cd.bc_lower = ["extrap", "extrap", "extrap"]
+    cd.bc_upper = ["extrap", "extrap", "user"]
+    dz = 2.0 / float(np.float32(n))
+    aux = _two_layer_aux(n, n, n, -1.0, dz, (2.0, 2.0), (1.0, 1.0))
+    q0 = np.zeros((4, n, n, n))
+    return rd, "vc_acoustics_3d", {}, q0, aux
+
+
+def heterogeneous_acoustics_3d(n=256, nout=8, tfinal=0.8, limiter="mc", dt_initial=0.01,
+                               shape=None):
+    """3D heterogeneous acoustics workload: two layers split at z=0 (rho=1,
+    K=1 below; rho=4, K=2 above; Z = sqrt(rho K), c = sqrt(K/rho) per cell),
+    [-1,1]^3 with n^3 cells (or `shape` = (mx, my, mz)), Gaussian pulse
+    p0 = exp(-80 |x - x0|^2) at x0 = (0, 0, -0.4), zero velocity; order 2,
+    transverse_waves 22, MC, cfl 0.9, wall at z-lower, extrapolation
+    elsewhere, t_final 0.8."""
+    mx, my, mz = shape if shape is not None else (n, n, n)
+    rd = ClawRunData("classic", 3)
+    cd = rd.clawdata
+    cd.lower, cd.upper, cd.num_cells = [-1.0] * 3, [1.0] * 3, [mx, my, mz]
+    cd.num_eqn, cd.num_aux, cd.capa_index = 4, 2, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, dt_initial, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.transverse_waves, cd.dimensional_split = 2, 22, "unsplit"
+    cd.num_waves, cd.limiter = 2, [limiter, limiter]
+    cd.bc_lower = ["extrap", "extrap", "wall"]
+    cd.bc_upper = ["extrap", "extrap", "extrap"]
+    x, _ = _centres(-1.0, 1.0, mx)
+    y, _ = _centres(-1.0, 1.0, my)
+    z, dz = _centres(-1.0, 1.0, mz)
+    below = (np.sqrt(1.0 * 1.0), np.sqrt(1.0 / 1.0))
+    above = (np.sqrt(4.0 * 2.0), np.sqrt(2.0 / 4.0))
+    aux = _two_layer_aux(mx, my, mz, -1.0, dz, below, above)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    q0 = np.zeros((4, mz, my, mx))
+    q0[0] = np.exp(-80.0 * (X * X + Y * Y + (Z + 0.4) ** 2))
+    return rd, "vc_acoustics_3d", {}, q0, aux
+
+
+def random_acoustics_3d(mx, my, mz, seed=0, bc=("extrap",) * 6, limiter="mc", trans=22,
+                        order=2, nout=1, tfinal=0.02):
+    """Seeded random 3D heterogeneous acoustics state (random per-cell (Z, c)
+    and random q) for parity tests on ragged sizes and every BC kind."""
+    rng = np.random.default_rng(seed)
+    rd, solver, params, _, _ = heterogeneous_acoustics_3d(shape=(mx, my, mz), nout=nout,
+                                                          tfinal=tfinal, limiter=limiter)
+    cd = rd.clawdata
+    cd.bc_lower = [bc[0], bc[2], bc[4]]
+    cd.bc_upper = [bc[1], bc[3], bc[5]]
+    cd.transverse_waves = trans
+    cd.order = order
+    aux = np.empty((2, mz + 4, my + 4, mx + 4))
+    aux[0] = rng.uniform(0.5, 2.0, aux[0].shape)
+    aux[1] = rng.uniform(0.5, 1.5, aux[1].shape)
+    q0 = np.empty((4, mz, my, mx))
+    q0[0] = 1.0 + 0.3 * rng.standard_normal((mz, my, mx))
+    q0[1:] = 0.2 * rng.standard_normal((3, mz, my, mx))
+    return rd, solver, params, q0, aux

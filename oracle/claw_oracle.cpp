@@ -629,6 +629,502 @@ done:
     return info;
 }
 
+// ================================================================ 3D path ===
+// step3 (src/3d/step3.f90:3-873) in its serial execution order, flux3
+// (src/3d/flux3.f90:4-612), bc3 (src/3d/bc3.f), claw3 (src/3d/claw3.f:738-928).
+// Solver: variable-coefficient acoustics, q = (p, u, v, w), aux = (Z, c), with
+// transverse (rpt3) and double-transverse (rptt3) splits written from the
+// eigen-decomposition (the solver lives in the un-vendored clawpack/riemann).
+// The 3D example links src/3d/limiter.f90 + philim.f90 instead of the inlined
+// limiter; both form r = (w_i . w_upwind)/|w_i|^2 from unlimited waves with
+// the same sums and the same phi(r), so `limiter` above serves here too.
+}  // extern "C"
+
+namespace {
+
+// Normal velocity index (1-based) of a sweep, and of its y-like / z-like
+// transverse directions: (x: y, z), (y: z, x), (z: x, y).
+inline int vel_index(int dir) { return 1 + dir; }  // dir 1,2,3 -> 2,3,4
+inline int trans_dir(int ixyz, int icoor) {       // icoor 2 = y-like, 3 = z-like
+    return ((ixyz - 1 + (icoor - 1)) % 3) + 1;
+}
+
+struct Aux3 {  // aux slice arrays (maux, 1-mbc:maxm+mbc, 3)
+    const double* a;
+    int maux, n0lo, nlen;
+    double at(int ma, int i, int l) const {  // l = 1..3
+        return a[(ma - 1) + maux * ((i - n0lo) + nlen * (l - 1))];
+    }
+};
+
+void rpn3_vc_acoustics(int ixyz, int meqn, int mbc, int mx, const double* q, const Aux3& a2,
+                       double* wave, double* s, double* amdq, double* apdq) {
+    const int mu = vel_index(ixyz);
+    const Slice Q{meqn, 1 - mbc}, W{meqn * 2, 1 - mbc}, S{2, 1 - mbc};
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const double zl = a2.at(1, i - 1, 2), cl = a2.at(2, i - 1, 2);
+        const double zr = a2.at(1, i, 2), cr = a2.at(2, i, 2);
+        const double dp = q[Q.at(1, i)] - q[Q.at(1, i - 1)];
+        const double du = q[Q.at(mu, i)] - q[Q.at(mu, i - 1)];
+        const double a1 = (zr * du - dp) / (zl + zr);
+        const double a2v = (zl * du + dp) / (zl + zr);
+        double* w1 = &wave[W.at(1, i)];
+        double* w2 = w1 + meqn;
+        for (int m = 0; m < meqn; ++m) { w1[m] = 0.0; w2[m] = 0.0; amdq[Q.at(m + 1, i)] = 0.0; apdq[Q.at(m + 1, i)] = 0.0; }
+        w1[0] = -(a1 * zl); w1[mu - 1] = a1;
+        w2[0] = a2v * zr;   w2[mu - 1] = a2v;
+        s[S.at(1, i)] = -cl;
+        s[S.at(2, i)] = cr;
+        amdq[Q.at(1, i)] = cl * (a1 * zl);
+        amdq[Q.at(mu, i)] = -(cl * a1);
+        apdq[Q.at(1, i)] = cr * (a2v * zr);
+        apdq[Q.at(mu, i)] = cr * a2v;
+    }
+}
+
+// Split a fluctuation living in cell (i1, mid) into the parts transmitted
+// down (speed -c below) and up (speed +c above), given (Z, c) below, mid,
+// above: b1 = (-asdq_p + Z_mid asdq_t)/(Z_below + Z_mid), down part
+// c_below (b1 Z_below, -b1); b2 = (asdq_p + Z_mid asdq_t)/(Z_mid + Z_above),
+// up part c_above (b2 Z_above, b2); the reflected remainder is dropped.
+inline void vc_split(int meqn, int mt, const double* asdq, double zb, double cb, double zm,
+                     double za, double ca, double* bm, double* bp) {
+    const double b1 = (zm * asdq[mt - 1] - asdq[0]) / (zb + zm);
+    const double b2 = (zm * asdq[mt - 1] + asdq[0]) / (zm + za);
+    for (int m = 0; m < meqn; ++m) { bm[m] = 0.0; bp[m] = 0.0; }
+    bm[0] = (cb * b1) * zb;
+    bm[mt - 1] = -(cb * b1);
+    bp[0] = (ca * b2) * za;
+    bp[mt - 1] = ca * b2;
+}
+
+// rpt3(ixyz, icoor, imp): transverse split in the y-like (icoor 2) or z-like
+// (icoor 3) direction of a fluctuation in cell i1 = i-2+imp (imp 0: the cell
+// is irrelevant for constant coefficients; here aux is always present).
+void rpt3_vc_acoustics(int ixyz, int icoor, int imp, int meqn, int mbc, int mx,
+                       const Aux3& a1, const Aux3& a2, const Aux3& a3, const double* asdq,
+                       double* bm, double* bp) {
+    const int mt = vel_index(trans_dir(ixyz, icoor));
+    const Slice Q{meqn, 1 - mbc};
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int i1 = i - 2 + (imp == 0 ? 2 : imp);
+        double zb, cb, zm, za, ca;
+        if (icoor == 2) {
+            zb = a1.at(1, i1, 2); cb = a1.at(2, i1, 2);
+            zm = a2.at(1, i1, 2);
+            za = a3.at(1, i1, 2); ca = a3.at(2, i1, 2);
+        } else {
+            zb = a2.at(1, i1, 1); cb = a2.at(2, i1, 1);
+            zm = a2.at(1, i1, 2);
+            za = a2.at(1, i1, 3); ca = a2.at(2, i1, 3);
+        }
+        vc_split(meqn, mt, &asdq[Q.at(1, i)], zb, cb, zm, za, ca, &bm[Q.at(1, i)], &bp[Q.at(1, i)]);
+    }
+}
+
+// rptt3(ixyz, icoor, imp, impt): split, in direction icoor, a fluctuation
+// already moved one cell in the other transverse direction (impt 1: down,
+// 2: up), i.e. living at that neighbour of cell i1.
+void rptt3_vc_acoustics(int ixyz, int icoor, int imp, int impt, int meqn, int mbc, int mx,
+                        const Aux3& a1, const Aux3& a2, const Aux3& a3, const double* asdq,
+                        double* bm, double* bp) {
+    const int mt = vel_index(trans_dir(ixyz, icoor));
+    const Slice Q{meqn, 1 - mbc};
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int i1 = i - 2 + imp;
+        double zb, cb, zm, za, ca;
+        if (icoor == 2) {  // moved in z-like: level l = 1 (below) or 3 (above)
+            const int l = impt == 1 ? 1 : 3;
+            zb = a1.at(1, i1, l); cb = a1.at(2, i1, l);
+            zm = a2.at(1, i1, l);
+            za = a3.at(1, i1, l); ca = a3.at(2, i1, l);
+        } else {  // moved in y-like: row aux1 (below) or aux3 (above)
+            const Aux3& r = impt == 1 ? a1 : a3;
+            zb = r.at(1, i1, 1); cb = r.at(2, i1, 1);
+            zm = r.at(1, i1, 2);
+            za = r.at(1, i1, 3); ca = r.at(2, i1, 3);
+        }
+        vc_split(meqn, mt, &asdq[Q.at(1, i)], zb, cb, zm, za, ca, &bm[Q.at(1, i)], &bp[Q.at(1, i)]);
+    }
+}
+
+// flux3 for one slice; gadd/hadd laid out (m, k=1:2, l=-1:1, i).
+void flux3(int ixyz, int meqn, int mwaves, int mbc, int mx, const double* q1d,
+           const double* dtdx1d, double dtdy, double dtdz, const Aux3& a1, const Aux3& a2,
+           const Aux3& a3, const int* method, const int* mthlim, double* qadd, double* fadd,
+           double* gadd, double* hadd, double* cfl1d, bool use_fwave) {
+    const int n = mx + 2 * mbc + 1;
+    const Slice Q{meqn, 1 - mbc}, S{mwaves, 1 - mbc}, W{meqn * mwaves, 1 - mbc};
+    auto D = [&](int i) { return dtdx1d[i - (1 - mbc)]; };
+    auto G = [&](double* g, int m, int k, int l, int i) -> double& {
+        return g[(m - 1) + meqn * ((k - 1) + 2 * ((l + 1) + 3 * (i - (1 - mbc))))];
+    };
+    std::vector<double> wave(meqn * mwaves * n), s(mwaves * n), amdq(meqn * n), apdq(meqn * n),
+        cqxx(meqn * n, 0.0);
+    std::vector<double> bmamdq(meqn * n), bmapdq(meqn * n), bpamdq(meqn * n), bpapdq(meqn * n),
+        cmamdq(meqn * n), cmapdq(meqn * n), cpamdq(meqn * n), cpapdq(meqn * n),
+        cmamdq2(meqn * n), cmapdq2(meqn * n), cpamdq2(meqn * n), cpapdq2(meqn * n),
+        bmcqxxp(meqn * n), bpcqxxp(meqn * n), bmcqxxm(meqn * n), bpcqxxm(meqn * n),
+        cmcqxxp(meqn * n), cpcqxxp(meqn * n), cmcqxxm(meqn * n), cpcqxxm(meqn * n),
+        bmcmamdq(meqn * n), bmcmapdq(meqn * n), bpcmamdq(meqn * n), bpcmapdq(meqn * n),
+        bmcpamdq(meqn * n), bmcpapdq(meqn * n), bpcpamdq(meqn * n), bpcpapdq(meqn * n);
+    bool limit = false;
+    for (int mw = 0; mw < mwaves; ++mw)
+        if (mthlim[mw] > 0) limit = true;
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+        for (int m = 1; m <= meqn; ++m) {
+            qadd[Q.at(m, i)] = 0.0;
+            fadd[Q.at(m, i)] = 0.0;
+            for (int k = 1; k <= 2; ++k)
+                for (int l = -1; l <= 1; ++l) { G(gadd, m, k, l, i) = 0.0; G(hadd, m, k, l, i) = 0.0; }
+        }
+    int m3, m4;
+    if (method[2] < 0) { m3 = -1; m4 = 0; }
+    else { m3 = method[2] / 10; m4 = method[2] - 10 * m3; }
+
+    rpn3_vc_acoustics(ixyz, meqn, mbc, mx, q1d, a2, wave.data(), s.data(), amdq.data(), apdq.data());
+    // forall: the first statement for every i, then the second
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 1; m <= meqn; ++m) qadd[Q.at(m, i)] = qadd[Q.at(m, i)] - D(i) * apdq[Q.at(m, i)];
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 1; m <= meqn; ++m)
+            qadd[Q.at(m, i - 1)] = qadd[Q.at(m, i - 1)] - D(i - 1) * amdq[Q.at(m, i)];
+    double c1 = 0.0;
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int mw = 1; mw <= mwaves; ++mw) {
+            const double sm = s[S.at(mw, i)];
+            c1 = std::fmax(std::fmax(c1, D(i) * sm), -D(i - 1) * sm);
+        }
+    *cfl1d = c1;
+    if (method[1] != 1) {
+        if (limit) limiter(mx, meqn, mwaves, mbc, mx, wave.data(), s.data(), mthlim);
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            const double dtdxave = 0.5 * (D(i - 1) + D(i));
+            for (int m = 1; m <= meqn; ++m) cqxx[Q.at(m, i)] = 0.0;
+            for (int mw = 1; mw <= mwaves; ++mw) {
+                const double sm = s[S.at(mw, i)];
+                const double coef = use_fwave ? 0.5 * std::copysign(1.0, sm) * (1.0 - std::fabs(sm) * dtdxave)
+                                              : 0.5 * std::fabs(sm) * (1.0 - std::fabs(sm) * dtdxave);
+                const double* wv = &wave[W.at(1, i)] + (mw - 1) * meqn;
+                for (int m = 1; m <= meqn; ++m) cqxx[Q.at(m, i)] = cqxx[Q.at(m, i)] + coef * wv[m - 1];
+            }
+            for (int m = 1; m <= meqn; ++m) fadd[Q.at(m, i)] = fadd[Q.at(m, i)] + cqxx[Q.at(m, i)];
+        }
+    }
+    if (m3 <= 0) return;
+    rpt3_vc_acoustics(ixyz, 2, 1, meqn, mbc, mx, a1, a2, a3, amdq.data(), bmamdq.data(), bpamdq.data());
+    rpt3_vc_acoustics(ixyz, 2, 2, meqn, mbc, mx, a1, a2, a3, apdq.data(), bmapdq.data(), bpapdq.data());
+    rpt3_vc_acoustics(ixyz, 3, 1, meqn, mbc, mx, a1, a2, a3, amdq.data(), cmamdq.data(), cpamdq.data());
+    rpt3_vc_acoustics(ixyz, 3, 2, meqn, mbc, mx, a1, a2, a3, apdq.data(), cmapdq.data(), cpapdq.data());
+    if (m3 == 2) {
+        // maux > 0: split cqxx with imp = 1 and 2 in each transverse direction.
+        // (src/3d/flux3.f90:331 passes an undefined scalar as aux3 for the
+        // z-like imp=1 split; the z-like split reads only aux2, so aux3 is
+        // passed here.)
+        rpt3_vc_acoustics(ixyz, 2, 1, meqn, mbc, mx, a1, a2, a3, cqxx.data(), bmcqxxm.data(), bpcqxxm.data());
+        rpt3_vc_acoustics(ixyz, 2, 2, meqn, mbc, mx, a1, a2, a3, cqxx.data(), bmcqxxp.data(), bpcqxxp.data());
+        rpt3_vc_acoustics(ixyz, 3, 1, meqn, mbc, mx, a1, a2, a3, cqxx.data(), cmcqxxm.data(), cpcqxxm.data());
+        rpt3_vc_acoustics(ixyz, 3, 2, meqn, mbc, mx, a1, a2, a3, cqxx.data(), cmcqxxp.data(), cpcqxxp.data());
+    }
+    for (int i = 0; i <= mx + 2; ++i)
+        for (int m = 1; m <= meqn; ++m) {
+            const int x = Q.at(m, i);
+            if (m4 == 1) {
+                cpapdq2[x] = cpapdq[x]; cpamdq2[x] = cpamdq[x];
+                cmapdq2[x] = cmapdq[x]; cmamdq2[x] = cmamdq[x];
+            } else if (m4 == 2) {
+                cpapdq2[x] = cpapdq[x] - 3.0 * cpcqxxp[x];
+                cpamdq2[x] = cpamdq[x] + 3.0 * cpcqxxm[x];
+                cmapdq2[x] = cmapdq[x] - 3.0 * cmcqxxp[x];
+                cmamdq2[x] = cmamdq[x] + 3.0 * cmcqxxm[x];
+            }
+        }
+    if (m4 > 0) {
+        rptt3_vc_acoustics(ixyz, 2, 2, 2, meqn, mbc, mx, a1, a2, a3, cpapdq2.data(), bmcpapdq.data(), bpcpapdq.data());
+        rptt3_vc_acoustics(ixyz, 2, 1, 2, meqn, mbc, mx, a1, a2, a3, cpamdq2.data(), bmcpamdq.data(), bpcpamdq.data());
+        rptt3_vc_acoustics(ixyz, 2, 2, 1, meqn, mbc, mx, a1, a2, a3, cmapdq2.data(), bmcmapdq.data(), bpcmapdq.data());
+        rptt3_vc_acoustics(ixyz, 2, 1, 1, meqn, mbc, mx, a1, a2, a3, cmamdq2.data(), bmcmamdq.data(), bpcmamdq.data());
+    }
+    const double sixth = 1.0 / 6.0;
+    auto trans_updates = [&](double* g, double dtt, const std::vector<double>& mam,
+                             const std::vector<double>& pam, const std::vector<double>& map,
+                             const std::vector<double>& pap, const std::vector<double>& pmcqm,
+                             const std::vector<double>& ppcqm, const std::vector<double>& pmcqp,
+                             const std::vector<double>& ppcqp) {
+        for (int i = 1; i <= mx + 1; ++i)
+            for (int m = 1; m <= meqn; ++m) {
+                const int x = Q.at(m, i);
+                G(g, m, 1, 0, i - 1) = G(g, m, 1, 0, i - 1) - 0.5 * D(i - 1) * mam[x];
+                G(g, m, 2, 0, i - 1) = G(g, m, 2, 0, i - 1) - 0.5 * D(i - 1) * pam[x];
+                G(g, m, 1, 0, i) = G(g, m, 1, 0, i) - 0.5 * D(i) * map[x];
+                G(g, m, 2, 0, i) = G(g, m, 2, 0, i) - 0.5 * D(i) * pap[x];
+                if (m4 > 0) {
+                    G(g, m, 2, 0, i) = G(g, m, 2, 0, i) + sixth * D(i) * dtt * (bpcpapdq[x] - bpcmapdq[x]);
+                    G(g, m, 1, 0, i) = G(g, m, 1, 0, i) + sixth * D(i) * dtt * (bmcpapdq[x] - bmcmapdq[x]);
+                    G(g, m, 2, 1, i) = G(g, m, 2, 1, i) - sixth * D(i) * dtt * bpcpapdq[x];
+                    G(g, m, 1, 1, i) = G(g, m, 1, 1, i) - sixth * D(i) * dtt * bmcpapdq[x];
+                    G(g, m, 2, -1, i) = G(g, m, 2, -1, i) + sixth * D(i) * dtt * bpcmapdq[x];
+                    G(g, m, 1, -1, i) = G(g, m, 1, -1, i) + sixth * D(i) * dtt * bmcmapdq[x];
+                    G(g, m, 2, 0, i - 1) = G(g, m, 2, 0, i - 1) + sixth * D(i - 1) * dtt * (bpcpamdq[x] - bpcmamdq[x]);
+                    G(g, m, 1, 0, i - 1) = G(g, m, 1, 0, i - 1) + sixth * D(i - 1) * dtt * (bmcpamdq[x] - bmcmamdq[x]);
+                    G(g, m, 2, 1, i - 1) = G(g, m, 2, 1, i - 1) - sixth * D(i - 1) * dtt * bpcpamdq[x];
+                    G(g, m, 1, 1, i - 1) = G(g, m, 1, 1, i - 1) - sixth * D(i - 1) * dtt * bmcpamdq[x];
+                    G(g, m, 2, -1, i - 1) = G(g, m, 2, -1, i - 1) + sixth * D(i - 1) * dtt * bpcmamdq[x];
+                    G(g, m, 1, -1, i - 1) = G(g, m, 1, -1, i - 1) + sixth * D(i - 1) * dtt * bmcmamdq[x];
+                }
+                if (m3 < 2) continue;
+                G(g, m, 2, 0, i) = G(g, m, 2, 0, i) + D(i) * ppcqp[x];
+                G(g, m, 1, 0, i) = G(g, m, 1, 0, i) + D(i) * pmcqp[x];
+                G(g, m, 2, 0, i - 1) = G(g, m, 2, 0, i - 1) - D(i - 1) * ppcqm[x];
+                G(g, m, 1, 0, i - 1) = G(g, m, 1, 0, i - 1) - D(i - 1) * pmcqm[x];
+            }
+    };
+    // G fluxes (y-like), src/3d/flux3.f90:381-447
+    trans_updates(gadd, dtdz, bmamdq, bpamdq, bmapdq, bpapdq, bmcqxxm, bpcqxxm, bmcqxxp, bpcqxxp);
+    if (m4 == 2)
+        for (int i = 0; i <= mx + 2; ++i)
+            for (int m = 1; m <= meqn; ++m) {
+                const int x = Q.at(m, i);
+                bpapdq[x] = bpapdq[x] - 3.0 * bpcqxxp[x];
+                bpamdq[x] = bpamdq[x] + 3.0 * bpcqxxm[x];
+                bmapdq[x] = bmapdq[x] - 3.0 * bmcqxxp[x];
+                bmamdq[x] = bmamdq[x] + 3.0 * bmcqxxm[x];
+            }
+    if (m4 > 0) {
+        rptt3_vc_acoustics(ixyz, 3, 2, 2, meqn, mbc, mx, a1, a2, a3, bpapdq.data(), bmcpapdq.data(), bpcpapdq.data());
+        rptt3_vc_acoustics(ixyz, 3, 1, 2, meqn, mbc, mx, a1, a2, a3, bpamdq.data(), bmcpamdq.data(), bpcpamdq.data());
+        rptt3_vc_acoustics(ixyz, 3, 2, 1, meqn, mbc, mx, a1, a2, a3, bmapdq.data(), bmcmapdq.data(), bpcmapdq.data());
+        rptt3_vc_acoustics(ixyz, 3, 1, 1, meqn, mbc, mx, a1, a2, a3, bmamdq.data(), bmcmamdq.data(), bpcmamdq.data());
+    }
+    // H fluxes (z-like), src/3d/flux3.f90:513-609
+    trans_updates(hadd, dtdy, cmamdq, cpamdq, cmapdq, cpapdq, cmcqxxm, cpcqxxm, cmcqxxp, cpcqxxp);
+}
+
+}  // namespace
+
+extern "C" {
+
+// bc3 (src/3d/bc3.f): x, then y, then z, each over all other indices
+// including ghosts; mthbc 1 extrap, 2 periodic, 3 wall (negate q(2|3|4)).
+// bc code 10 at z-upper is the piston wall of
+// examples/acoustics_3d_heterogeneous/bc3.f:596-606 (reflect, then
+// q(4) = 2 s - q(4) with s = -exp(-500 r^2) exp(-500 t^2) for t < 0.1).
+int orc_bc3(int meqn, int mbc, int mx, int my, int mz, double* q, const int* mthbc, double t,
+            double xlower, double ylower, double dx, double dy) {
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    auto Q = [&](int m, int i, int j, int k) -> double& {
+        return q[(m - 1) + meqn * ((i - (1 - mbc)) + nx * ((j - (1 - mbc)) + ny * (k - (1 - mbc))))];
+    };
+    const int n[3] = {mx, my, mz};
+    for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+            const int code = mthbc[2 * d + side];
+            if (!(code >= 1 && code <= 3) && !(code == 10 && d == 2 && side == 1)) return -1;
+        }
+    for (int d = 0; d < 3; ++d) {
+        for (int side = 0; side < 2; ++side) {
+            const int code = mthbc[2 * d + side];
+            for (int g = 1; g <= mbc; ++g) {
+                const int dst = side == 0 ? 1 - g : n[d] + g;
+                int src;
+                if (code == 1) src = side == 0 ? 1 : n[d];
+                else if (code == 2) src = side == 0 ? n[d] + 1 - g : g;
+                else src = side == 0 ? g : n[d] + 1 - g;  // wall / piston: reflect
+                for (int k = 1 - mbc; k <= mz + mbc; ++k)
+                    for (int j = 1 - mbc; j <= my + mbc; ++j)
+                        for (int i = 1 - mbc; i <= mx + mbc; ++i) {
+                            int I[3] = {i, j, k};
+                            if (I[d] != dst) continue;
+                            int S[3] = {i, j, k};
+                            S[d] = src;
+                            for (int m = 1; m <= meqn; ++m) Q(m, i, j, k) = Q(m, S[0], S[1], S[2]);
+                            if (code == 3) Q(2 + d, i, j, k) = -Q(2 + d, S[0], S[1], S[2]);
+                            if (code == 10) {
+                                double sp = 0.0;
+                                if (t < 0.1) {
+                                    const double xi = xlower + (i - 0.5) * dx;
+                                    const double yj = ylower + (j - 0.5) * dy;
+                                    const double r2 = (xi * xi + yj * yj);
+                                    sp = -std::exp(-500.0 * r2) * std::exp(-(500.0 * (t * t)));
+                                    if (std::fabs(sp) < 1e-6) sp = 0.0;
+                                }
+                                Q(4, i, j, k) = 2.0 * sp - Q(4, S[0], S[1], S[2]);
+                            }
+                        }
+            }
+        }
+    }
+    return 0;
+}
+
+// step3: x-, y-, z-sweeps, each over 2x2 blocks of slices in the colour
+// order of the reference's OpenMP loops (koffset, joffset / ioffset), which
+// fixes every cell's order of accumulation.
+int orc_step3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, const double* qold,
+              double* qnew, const double* aux, double dx, double dy, double dz, double dt,
+              const int* method, const int* mthlim, int use_fwave, double* cfl_out) {
+    if (g_solver != ORC_VC_ACOUSTICS_3D || maux < 2) return -1;
+    if (method[5] != 0) return -3;  // capacity not restated for 3D
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    const int maxm = std::max(mx, std::max(my, mz));
+    const int n1 = maxm + 2 * mbc;
+    auto QO = [&](int m, int i, int j, int k) {
+        return qold[(m - 1) + meqn * ((i - (1 - mbc)) + nx * ((j - (1 - mbc)) + ny * (k - (1 - mbc))))];
+    };
+    auto QN = [&](int m, int i, int j, int k) -> double& {
+        return qnew[(m - 1) + meqn * ((i - (1 - mbc)) + nx * ((j - (1 - mbc)) + ny * (k - (1 - mbc))))];
+    };
+    auto AX = [&](int ma, int i, int j, int k) {
+        return aux[(ma - 1) + maux * ((i - (1 - mbc)) + nx * ((j - (1 - mbc)) + ny * (k - (1 - mbc))))];
+    };
+    std::vector<double> q1d(meqn * n1), dtd1d(n1), qadd(meqn * n1), fadd(meqn * n1),
+        gadd(meqn * 6 * n1), hadd(meqn * 6 * n1), x1(maux * n1 * 3), x2(maux * n1 * 3),
+        x3(maux * n1 * 3);
+    const Slice Q{meqn, 1 - mbc};
+    const double dtdx = dt / dx, dtdy = dt / dy, dtdz = dt / dz;
+    double cfl = 0.0;
+    const int dims[3] = {mx, my, mz};
+    const double dtd[3] = {dtdx, dtdy, dtdz};
+    auto Gv = [&](const std::vector<double>& g, int m, int k, int l, int i) {
+        return g[(m - 1) + meqn * ((k - 1) + 2 * ((l + 1) + 3 * (i - (1 - mbc))))];
+    };
+    for (int ixyz = 1; ixyz <= 3; ++ixyz) {
+        // directions: n = normal, e1 = y-like, e2 = z-like
+        const int dn = ixyz - 1, d1 = trans_dir(ixyz, 2) - 1, d2 = trans_dir(ixyz, 3) - 1;
+        const int len = dims[dn];
+        for (int i = 0; i < n1; ++i) dtd1d[i] = dtd[dn];
+        // colour, block and slice loops run over the two slice indices in
+        // the order of step3.f90: x: (k, j), y: (k, i), z: (j, i), i.e. the
+        // higher-numbered axis outermost
+        const int outer = std::max(d1, d2);  // slowest slice index
+        const int inner = std::min(d1, d2);
+        const int nblk_o = (dims[outer] + 2 + 1) / 2, nblk_i = (dims[inner] + 2 + 1) / 2;
+        for (int oo = 0; oo <= 1; ++oo)
+            for (int io = 0; io <= 1; ++io)
+                for (int ob = oo; ob <= nblk_o - 1; ob += 2)
+                    for (int ib = io; ib <= nblk_i - 1; ib += 2)
+                        for (int so = ob * 2; so <= std::min(ob * 2 + 1, dims[outer] + 1); ++so)
+                            for (int si = ib * 2; si <= std::min(ib * 2 + 1, dims[inner] + 1); ++si) {
+                                int P[3];
+                                P[outer] = so;
+                                P[inner] = si;
+                                auto cell = [&](int a, int de1, int de2, int* c) {
+                                    c[dn] = a;
+                                    c[d1] = P[d1] + de1;
+                                    c[d2] = P[d2] + de2;
+                                };
+                                for (int a = 1 - mbc; a <= len + mbc; ++a) {
+                                    int c[3];
+                                    cell(a, 0, 0, c);
+                                    for (int m = 1; m <= meqn; ++m) q1d[Q.at(m, a)] = QO(m, c[0], c[1], c[2]);
+                                }
+                                // aux1/aux2/aux3 = e1 offset -1/0/+1; third index = e2 offset -1..1
+                                for (int a = 1 - mbc; a <= len + mbc; ++a)
+                                    for (int l = -1; l <= 1; ++l)
+                                        for (int ma = 1; ma <= maux; ++ma) {
+                                            const int o = (ma - 1) + maux * ((a - (1 - mbc)) + n1 * (l + 1));
+                                            int c[3];
+                                            cell(a, -1, l, c); x1[o] = AX(ma, c[0], c[1], c[2]);
+                                            cell(a, 0, l, c); x2[o] = AX(ma, c[0], c[1], c[2]);
+                                            cell(a, 1, l, c); x3[o] = AX(ma, c[0], c[1], c[2]);
+                                        }
+                                const Aux3 A1{x1.data(), maux, 1 - mbc, n1}, A2{x2.data(), maux, 1 - mbc, n1},
+                                    A3{x3.data(), maux, 1 - mbc, n1};
+                                double cfl1d;
+                                flux3(ixyz, meqn, mwaves, mbc, len, q1d.data(), dtd1d.data(), dtd[d1],
+                                      dtd[d2], A1, A2, A3, method, mthlim, qadd.data(), fadd.data(),
+                                      gadd.data(), hadd.data(), &cfl1d, use_fwave != 0);
+                                cfl = std::fmax(cfl, cfl1d);
+                                const double te1 = dtd[d1], te2 = dtd[d2], tn = dtd[dn];
+                                for (int a = 1; a <= len; ++a)
+                                    for (int de2 = -1; de2 <= 1; ++de2)
+                                        for (int de1 = -1; de1 <= 1; ++de1)
+                                            for (int m = 1; m <= meqn; ++m) {
+                                                int c[3];
+                                                cell(a, de1, de2, c);
+                                                double& v = QN(m, c[0], c[1], c[2]);
+                                                if (de1 == 0 && de2 == 0) {
+                                                    v = v + qadd[Q.at(m, a)] -
+                                                        tn * (fadd[Q.at(m, a + 1)] - fadd[Q.at(m, a)]) -
+                                                        te1 * (Gv(gadd, m, 2, 0, a) - Gv(gadd, m, 1, 0, a)) -
+                                                        te2 * (Gv(hadd, m, 2, 0, a) - Gv(hadd, m, 1, 0, a));
+                                                    continue;
+                                                }
+                                                // e1 (G) term, then e2 (H) term
+                                                if (de1 == -1) v = v - te1 * Gv(gadd, m, 1, de2, a);
+                                                else if (de1 == 0) v = v - te1 * (Gv(gadd, m, 2, de2, a) - Gv(gadd, m, 1, de2, a));
+                                                else v = v + te1 * Gv(gadd, m, 2, de2, a);
+                                                if (de2 == -1) v = v - te2 * Gv(hadd, m, 1, de1, a);
+                                                else if (de2 == 0) v = v - te2 * (Gv(hadd, m, 2, de1, a) - Gv(hadd, m, 1, de1, a));
+                                                else v = v + te2 * Gv(hadd, m, 2, de1, a);
+                                            }
+                            }
+    }
+    *cfl_out = cfl;
+    return 0;
+}
+
+// claw3 (src/3d/claw3.f:738-928): the control flow of claw2 around bc3/step3.
+int orc_claw3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, double* q,
+              const double* aux, double xlower, double ylower, double dx, double dy, double dz,
+              double tstart, double* tend_io, double* dtv, double* cflv, int* nv,
+              const int* method, const int* mthlim, const int* mthbc, int use_fwaves) {
+    const double tend = *tend_io;
+    int info = 0;
+    double t = tstart;
+    int maxn = nv[0];
+    double dt = dtv[0];
+    double cflmax = 0.0, dtmin = dt, dtmax = dt, cfl = 0.0;
+    nv[1] = 0;
+    const size_t nq = (size_t)meqn * (mx + 2 * mbc) * (my + 2 * mbc) * (mz + 2 * mbc);
+    std::vector<double> qwork(nq);
+    if (method[0] == 0) {
+        if (tend < tstart) maxn = 1;
+        else {
+            maxn = (int)std::lround((tend - tstart) / dt);
+            if (std::fabs(maxn * dt - (tend - tstart)) > 1e-5 * (tend - tstart)) { info = 2; goto done; }
+        }
+    }
+    if (method[0] == 1 && cflv[1] > cflv[0]) { info = 3; goto done; }
+    if (maxn == 0) goto done;
+    for (int n = 1; n <= maxn; ++n) {
+        const double told = t;
+        if (told + dt > tend && tstart < tend) dt = tend - told;
+        for (;;) {
+            if (orc_bc3(meqn, mbc, mx, my, mz, q, mthbc, told, xlower, ylower, dx, dy) != 0) { info = -2; goto done; }
+            std::memcpy(qwork.data(), q, nq * sizeof(double));
+            const int rc = orc_step3(meqn, mwaves, maux, mbc, mx, my, mz, qwork.data(), q, aux, dx, dy,
+                                     dz, dt, method, mthlim, use_fwaves, &cfl);
+            if (rc != 0) { info = rc; goto done; }
+            t = told + dt;
+            if (cfl <= cflv[0]) { cflmax = std::fmax(cfl, cflmax); break; }
+            t = told;
+            std::memcpy(q, qwork.data(), nq * sizeof(double));
+            if (method[0] == 1) { dt = std::fmin(dtv[1], dt * cflv[1] / cfl); continue; }
+            cflmax = std::fmax(cfl, cflmax);
+            goto done;
+        }
+        if (method[0] == 1) {
+            if (cfl == 0.0) dt = dtv[1];
+            else dt = std::fmin(dtv[1], dt * cflv[1] / cfl);
+            dtmin = std::fmin(dt, dtmin);
+            dtmax = std::fmax(dt, dtmax);
+        }
+        nv[1] = nv[1] + 1;
+        if (t >= tend) break;
+    }
+done:
+    if (method[0] == 1 && t < tend && nv[1] == maxn) info = 11;
+    if (method[0] == 0 && cflmax > cflv[0]) info = 12;
+    *tend_io = t;
+    cflv[2] = cflmax;
+    cflv[3] = cfl;
+    dtv[2] = dtmin;
+    dtv[3] = dtmax;
+    dtv[4] = dt;
+    return info;
+}
+
 // ================================================================ 1D path ===
 // -------------------------------------------------------------------- bc1 ---
 int orc_bc1(int meqn, int mbc, int mx, double* q, const int* mthbc) {

@@ -1,13 +1,13 @@
 """ORACLE — test infrastructure only.
 
 ctypes wrapper of the CPU restatement in claw_oracle.cpp, plus the
-claw{1,2}ez frame loop (src/2d/claw2ez.f:265-324, src/1d/claw1ez.f) around
-it.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs
+claw{1,2,3}ez frame loop (src/2d/claw2ez.f:265-324, src/1d/claw1ez.f,
+src/3d/claw3ez.f) around it.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs
 use this module, always as the checker or the timed CPU reference.
 
-Arrays cross in the product's SoA layout (q: [meqn][my][mx] interior cells;
-aux: [maux][my+4][mx+4]) and are converted here to the reference's Fortran
-layout q(meqn, 1-mbc:mx+mbc, 1-mbc:my+mbc).
+Arrays cross in the product's SoA layout (q: [meqn]([mz])[my][mx] interior
+cells; aux: [maux]([mz+4])[my+4][mx+4]) and are converted here to the
+reference's Fortran layout q(meqn, 1-mbc:mx+mbc, 1-mbc:my+mbc(, 1-mbc:mz+mbc)).
 """
 from __future__ import annotations
 
@@ -33,6 +33,9 @@ SOLVER_PARAMS = {
     "acoustics_1d": ("rho", "bulk"),
     "euler_roe_2d": ("gamma",),
 }
+
+# bc code of the restated user BC (examples/acoustics_3d_heterogeneous/bc3.f:282-312)
+PISTON_BC = 10
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -69,6 +72,14 @@ def _load(variant: str):
     lib.orc_step1.restype = ctypes.c_int
     lib.orc_bc1.argtypes = [ctypes.c_int] * 3 + [_D, _I]
     lib.orc_bc1.restype = ctypes.c_int
+    lib.orc_claw3.argtypes = [ctypes.c_int] * 7 + [_D, _D] + [ctypes.c_double] * 6 + [
+        _D, _D, _D, _I, _I, _I, _I, ctypes.c_int]
+    lib.orc_claw3.restype = ctypes.c_int
+    lib.orc_step3.argtypes = [ctypes.c_int] * 7 + [_D, _D, _D] + [ctypes.c_double] * 4 + [
+        _I, _I, ctypes.c_int, _D]
+    lib.orc_step3.restype = ctypes.c_int
+    lib.orc_bc3.argtypes = [ctypes.c_int] * 5 + [_D, _I] + [ctypes.c_double] * 5
+    lib.orc_bc3.restype = ctypes.c_int
     return lib
 
 
@@ -98,6 +109,9 @@ def _codes(cd):
         mthbc = np.array([lo[0], hi[0], lo[1], hi[1]], dtype=np.int32)
     else:
         mthbc = np.array([lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]], dtype=np.int32)
+        if mthbc[5] == 0:
+            # 'user' at z-upper: the piston wall of examples/acoustics_3d_heterogeneous
+            mthbc[5] = PISTON_BC
     return method, mthlim, mthbc
 
 
@@ -167,13 +181,19 @@ class OracleGrid:
                                       _p(self.method, _I), _p(self.mthlim, _I),
                                       _p(self.mthbc, _I), self.use_fwaves)
         else:
-            raise NotImplementedError("3D oracle lives in claw_oracle_ext.cpp")
+            mx, my, mz = self.cells
+            info = self.lib.orc_claw3(self.meqn, self.mwaves, self.maux, self.mbc, mx, my, mz,
+                                      _p(self.qf), _p(self.af), float(self.cd.lower[0]),
+                                      float(self.cd.lower[1]), self.dxs[0], self.dxs[1],
+                                      self.dxs[2], float(tstart), ctypes.byref(te), _p(dtv),
+                                      _p(cflv), _p(nv, _I), _p(self.method, _I),
+                                      _p(self.mthlim, _I), _p(self.mthbc, _I), self.use_fwaves)
         stats = dict(t_reached=te.value, dt_min=dtv[2], dt_max_taken=dtv[3], dt_next=dtv[4],
                      cfl_max_seen=cflv[2], cfl_last=cflv[3], steps_taken=int(nv[1]), info=info)
         return info, stats
 
-    def step(self, dt):
-        """bc + copy + one step2/step1 of length dt; returns cfl."""
+    def step(self, dt, t=0.0):
+        """bc + copy + one step1/2/3 of length dt (t: the bc time); returns cfl."""
         self._set_solver()
         cfl = ctypes.c_double(0.0)
         if self.nd == 2:
@@ -184,6 +204,16 @@ class OracleGrid:
                                     _p(qold), _p(self.qf), _p(self.af), self.dxs[0], self.dxs[1],
                                     float(dt), _p(self.method, _I), _p(self.mthlim, _I),
                                     self.use_fwaves, ctypes.byref(cfl))
+        elif self.nd == 3:
+            mx, my, mz = self.cells
+            self.lib.orc_bc3(self.meqn, self.mbc, mx, my, mz, _p(self.qf), _p(self.mthbc, _I),
+                             float(t), float(self.cd.lower[0]), float(self.cd.lower[1]),
+                             self.dxs[0], self.dxs[1])
+            qold = self.qf.copy()
+            rc = self.lib.orc_step3(self.meqn, self.mwaves, self.maux, self.mbc, mx, my, mz,
+                                    _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                    self.dxs[1], self.dxs[2], float(dt), _p(self.method, _I),
+                                    _p(self.mthlim, _I), self.use_fwaves, ctypes.byref(cfl))
         else:
             (mx,) = self.cells
             self.lib.orc_bc1(self.meqn, self.mbc, mx, _p(self.qf), _p(self.mthbc, _I))

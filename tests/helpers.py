@@ -8,6 +8,15 @@ def e26(q):
     return f(np.asarray(q, dtype=np.float64))
 
 
+def frame_sum(field):
+    """Sum of one field as the reference's regression check forms it: pyclaw
+    stores a frame as q[m, i, j(, k)] (x index slowest in C order), so numpy
+    sums the interior with the last axis fastest.  `field` is the SoA
+    [(mz,)(my,)mx] layout used here."""
+    a = e26(field)
+    return float(np.ascontiguousarray(a.transpose(tuple(range(a.ndim))[::-1])).sum())
+
+
 def rel_diff(a, b):
     """Normwise relative difference per field: max|a-b| / max|b|."""
     a = np.asarray(a)
