@@ -40,7 +40,7 @@ def up_to_date() -> bool:
 # rounds every multiply and add separately; the characteristic-variable path
 # (fast2d.cu) contracts to fused multiply-adds.
 UNITS = [("claw_b200.cu", "--fmad=false"), ("noalloc.cu", "--fmad=false"),
-         ("fast2d.cu", "--fmad=true")]
+         ("fast2d.cu", "--fmad=true"), ("claw3d.cu", "--fmad=false")]
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:

@@ -197,6 +197,7 @@ std::unique_ptr<Runner> runner2d(const claw_config& cfg, const S& s) {
 template <typename real>
 std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
     const int id = cfg.solver_id;
+    if (cfg.num_dim == 3) return make_runner3d(cfg);
     if (cfg.precision != CLAW_FP64) {
         // fused / FP32 arithmetic: constant-coefficient acoustics runs in
         // characteristic variables when the method allows it
@@ -228,6 +229,7 @@ bool solver_shape(int id, SolverShape* sh) {
         case CLAW_SOLVER_VC_ADVECTION_2D: *sh = {2, 1, 1, 3}; return true;
         case CLAW_SOLVER_ACOUSTICS_1D: *sh = {1, 2, 2, 0}; return true;
         case CLAW_SOLVER_VC_ACOUSTICS_1D: *sh = {1, 2, 2, 2}; return true;
+        case CLAW_SOLVER_VC_ACOUSTICS_3D: *sh = {3, 4, 2, 2}; return true;
         default: return false;
     }
 }
@@ -258,6 +260,7 @@ struct claw_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
     int device = 0;
+    double t_now = 0.0;  // time of the current q (time-dependent boundary conditions)
 };
 
 extern "C" {
@@ -281,7 +284,10 @@ static int validate(const claw_config* c, SolverShape* sh) {
         if (!(c->upper[d] > c->lower[d])) return fail(CLAW_E_INVALID, "upper[%d] <= lower[%d]", d, d);
         for (int side = 0; side < 2; ++side) {
             const int b = side ? c->bc_upper[d] : c->bc_lower[d];
-            if (b == 0) return fail(CLAW_E_UNSUPPORTED, "user boundary conditions are not built");
+            if (b == CLAW_BC_PISTON && d == 2 && side == 1 && c->solver_id == CLAW_SOLVER_VC_ACOUSTICS_3D)
+                continue;
+            if (b == 0 || b == CLAW_BC_PISTON)
+                return fail(CLAW_E_UNSUPPORTED, "user boundary conditions are not built");
             if (b < 1 || b > 3) return fail(CLAW_E_INVALID, "bad boundary condition %d", b);
             if (b == 3 && c->num_eqn < d + 2)
                 return fail(CLAW_E_INVALID, "wall BC needs a velocity component %d", d + 2);
@@ -296,6 +302,11 @@ static int validate(const claw_config* c, SolverShape* sh) {
     for (int k = 0; k < c->num_waves; ++k)
         if (c->limiter[k] < 0 || c->limiter[k] > 5) return fail(CLAW_E_INVALID, "invalid limiter %d", c->limiter[k]);
     if (c->precision < CLAW_FP64 || c->precision > CLAW_FP32) return fail(CLAW_E_INVALID, "bad precision");
+    if (c->num_dim == 3) {
+        if (c->capa_index != 0) return fail(CLAW_E_UNSUPPORTED, "3D capacity is not built");
+        if (c->use_fwaves) return fail(CLAW_E_UNSUPPORTED, "3D f-waves are not built");
+        if (c->precision != CLAW_FP64) return fail(CLAW_E_UNSUPPORTED, "3D runs in FP64 only");
+    }
     return 0;
 }
 
@@ -475,13 +486,15 @@ int claw_step(claw_handle* h, double dt, double* cfl) {
     c->dt = dt;
     c->cur = h->cur;
     c->maxn = 1;
+    c->t = c->told = h->t_now;
     int rc = push_ctl(h);
     if (rc) return rc;
     CUDA_TRY(h->runner->launch(h->stream));
-    h->launches++;
+    h->launches += h->runner->launches_per_step();
     rc = pull_ctl(h);
     if (rc) return rc;
     h->cur = c->cur;
+    h->t_now += dt;
     if (cfl) *cfl = c->cfl_last;
     if (c->err & CTL_ERR_TMA_TIMEOUT) return fail(CLAW_E_DEVICE, "device wait timed out");
     return 0;
@@ -540,6 +553,13 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
     if (!info && cfg.dt_variable && cfg.cfl_desired > cfg.cfl_max) info = 3;
     if (!info && cfg.capa_index > cfg.num_aux) info = 5;
     if (!info && cfg.order < cfg.transverse_waves && cfg.num_dim == 2) info = 6;
+    if (!info && cfg.num_dim == 3) {
+        // src/3d/chkmth.f: the unsplit transverse codes allowed per order
+        const int t3 = cfg.transverse_waves;
+        const bool ok = t3 == 0 || t3 == 10 || t3 == 11 ||
+                        (cfg.order == 2 && (t3 == 20 || t3 == 21 || t3 == 22));
+        if (!ok) info = 6;
+    }
     c->maxn = maxn;
     c->done = (info != 0 || maxn == 0) ? 1 : 0;
     if (!c->done && c->told + c->dt > tend && tstart < tend) c->dt = tend - c->told;
@@ -562,7 +582,7 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
             if (rc) return rc;
             for (;;) {
                 CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
-                h->launches += chunk;
+                h->launches += (long long)chunk * h->runner->launches_per_step();
                 rc = pull_ctl(h);
                 if (rc) return rc;
                 if (c->done) break;
@@ -574,6 +594,7 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
     float ms = 0.f;
     CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->cur = c->cur;
+    h->t_now = c->t;
     if (!info && cfg.dt_variable && c->t < tend && c->n == maxn) info = 11;
     if (!info && !cfg.dt_variable && c->cflmax_seen > cfg.cfl_max) info = 12;
     if (c->err & CTL_ERR_TMA_TIMEOUT) info = CLAW_E_DEVICE;

@@ -25,7 +25,8 @@ struct Geometry {
 struct Runner {
     virtual ~Runner() {}
     virtual int prepare(const claw_config& cfg, const Geometry& g) = 0;
-    virtual cudaError_t launch(cudaStream_t s) = 0;
+    virtual cudaError_t launch(cudaStream_t s) = 0;  // one time step
+    virtual int launches_per_step() const { return 1; }
 };
 
 // Record an error message (claw_last_error) and return code.
@@ -40,6 +41,9 @@ int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, 
 // Characteristic-variable kernel for constant-coefficient 2D acoustics
 // (char2d.cuh, built with fused multiply-add); nullptr if cfg is not served.
 std::unique_ptr<Runner> make_char_runner(const claw_config& cfg);
+
+// 3D step (step3d.cuh: one launch per sweep); nullptr if cfg is not served.
+std::unique_ptr<Runner> make_runner3d(const claw_config& cfg);
 
 }  // namespace clawb200
 

@@ -151,4 +151,49 @@ struct VCAcoustics1D {
     }
 };
 
+
+// Variable-coefficient 3D acoustics, q = (p, u, v, w), aux = (Z, c) per cell:
+// the rpn3 / rpt3 / rptt3 plugins of examples/acoustics_3d_heterogeneous
+// (clawpack/riemann rp{n,t,tt}3_vc_acoustics) in pointwise, compact form.
+// Every fluctuation of this system has two non-zero components: the pressure
+// and the velocity along the direction of its last split, so the solver
+// works on (p, velocity) pairs and the step kernel places them.
+template <typename real_>
+struct VCAcoustics3D {
+    using real = real_;
+    static constexpr int meqn = 4, mwaves = 2, maux = 2;
+
+    // Normal solve at one interface: jump (dp, dun) between cells with
+    // impedance / sound speed (zl, cl) | (zr, cr).  w[k] = (p, un) of wave k.
+    __device__ __forceinline__ static void rpn(real pL, real uL, real pR, real uR, real zl,
+                                               real cl, real zr, real cr, real w[2][2],
+                                               real s[2], real am[2], real ap[2]) {
+        const real dp = pR - pL;
+        const real du = uR - uL;
+        const real a1 = (zr * du - dp) / (zl + zr);
+        const real a2 = (zl * du + dp) / (zl + zr);
+        w[0][0] = -(a1 * zl); w[0][1] = a1;
+        w[1][0] = a2 * zr;    w[1][1] = a2;
+        s[0] = -cl;
+        s[1] = cr;
+        am[0] = cl * (a1 * zl); am[1] = -(cl * a1);
+        ap[0] = cr * (a2 * zr); ap[1] = cr * a2;
+    }
+
+    // Transverse split of a fluctuation whose pressure part is xp (its
+    // velocity along the split direction is structurally zero) living in a
+    // cell of impedance zm, between the neighbours below (zb, cb) and above
+    // (za, ca): down = c_b (b1 Z_b, -b1), up = c_a (b2 Z_a, b2) with
+    // b1 = -xp / (Z_b + Z_m), b2 = xp / (Z_m + Z_a).  rpt3 and rptt3 differ
+    // only in which cells' coefficients they pass.
+    struct Split { real dp, dt, up, ut; };
+    __device__ __forceinline__ static Split split(real xp, real zb, real cb, real zm, real za,
+                                                  real ca) {
+        const real b1 = -xp / (zb + zm);
+        const real b2 = xp / (zm + za);
+        const real c1 = cb * b1, c2 = ca * b2;
+        return Split{c1 * zb, -c1, c2 * za, c2};
+    }
+};
+
 }  // namespace clawb200

@@ -30,9 +30,15 @@ SOLVER_PARAMS = {
 }
 
 
+# Built-in user boundary conditions ('user' in bc_lower / bc_upper), by name.
+USER_BCS = {"piston": 10}  # examples/acoustics_3d_heterogeneous/bc3.f:282-312, z-upper
+
+
 def make_config(cd: ClawInputData, solver: str, params: dict | None = None,
-                precision: str = "fp64") -> ClawConfig:
-    """Map clawdata + solver choice onto the C ``claw_config``."""
+                precision: str = "fp64", user_bc: str | None = None) -> ClawConfig:
+    """Map clawdata + solver choice onto the C ``claw_config``.  ``user_bc``
+    names the built-in routine that stands for the example's own bc code
+    wherever clawdata says 'user'."""
     if solver not in SOLVER_IDS:
         raise ValueError(f"unknown solver {solver!r}; built: {sorted(SOLVER_IDS)}")
     params = params or {}
@@ -61,6 +67,11 @@ def make_config(cd: ClawInputData, solver: str, params: dict | None = None,
         c.limiter[k] = v
     c.num_ghost = int(cd.num_ghost)
     lo, hi = cd.bc_codes()
+    if user_bc is not None:
+        if user_bc not in USER_BCS:
+            raise ValueError(f"unknown user_bc {user_bc!r}; built: {sorted(USER_BCS)}")
+        lo = [USER_BCS[user_bc] if v == 0 else v for v in lo]
+        hi = [USER_BCS[user_bc] if v == 0 else v for v in hi]
     for d in range(3):
         c.bc_lower[d] = lo[d] if d < nd else 1
         c.bc_upper[d] = hi[d] if d < nd else 1
@@ -88,14 +99,14 @@ class Solver:
     """Device state of one grid and the step / advance entry points."""
 
     def __init__(self, clawdata, solver: str, params: dict | None = None,
-                 precision: str = "fp64"):
+                 precision: str = "fp64", user_bc: str | None = None):
         if isinstance(clawdata, ClawRunData):
             clawdata = clawdata.clawdata
         self.lib = _lib.load()
         self.clawdata = clawdata
         self.solver = solver
         self.precision = precision
-        self.cfg = make_config(clawdata, solver, params, precision)
+        self.cfg = make_config(clawdata, solver, params, precision, user_bc)
         self.ndim = self.cfg.num_dim
         self.meqn = self.cfg.num_eqn
         self.maux = self.cfg.num_aux
@@ -127,7 +138,7 @@ class Solver:
 
     # -- stepping -----------------------------------------------------------
     def step(self, dt: float) -> float:
-        """One step of length dt (bc2 + step2); returns the Courant number."""
+        """One step of length dt (bc + step2/step3); returns the Courant number."""
         cfl = ctypes.c_double(0.0)
         check(self.lib.claw_step(self._h, float(dt), ctypes.byref(cfl)), "claw_step")
         return cfl.value
@@ -193,11 +204,11 @@ def frame_times(cd: ClawInputData):
 def run(rundata, solver: str, params: dict | None, q0: np.ndarray,
         aux: np.ndarray | None = None, precision: str = "fp64",
         on_frame: Callable[[Frame], None] | None = None, keep_frames: bool = True,
-        flush_tiny: bool = True, solver_obj: Solver | None = None):
+        flush_tiny: bool = True, solver_obj: Solver | None = None, user_bc: str | None = None):
     """claw{1,2}ez's frame loop on the GPU.  Returns the list of frames
     (frame 0 included when output_t0); raises on a nonzero info."""
     cd = rundata.clawdata if isinstance(rundata, ClawRunData) else rundata
-    s = solver_obj or Solver(cd, solver, params, precision)
+    s = solver_obj or Solver(cd, solver, params, precision, user_bc)
     q = np.array(q0, dtype=np.float64, copy=True)
     if flush_tiny:
         q[np.abs(q) < 1e-99] = 0.0

@@ -44,6 +44,13 @@ enum claw_solver_id {
     CLAW_SOLVER_VC_ACOUSTICS_3D = 21 /* q=(p,u,v,w); aux=(Z,c)                  */
 };
 
+/* Boundary-condition codes beyond claw.data's 0..3: the built-in user BC of
+ * examples/acoustics_3d_heterogeneous (bc3.f:282-312) -- a solid wall at
+ * z-upper whose centre moves as a piston, w_ghost = 2 s(x,y,t) - w_interior
+ * with s = -exp(-500 (x^2+y^2)) exp(-500 t^2) for t < 0.1.  Valid only at
+ * bc_upper[2] with CLAW_SOLVER_VC_ACOUSTICS_3D; t is the step's start time. */
+enum claw_bc { CLAW_BC_PISTON = 10 };
+
 /* Arithmetic of the Riemann/limiter/update path. */
 enum claw_precision {
     CLAW_FP64 = 0,      /* every multiply and add rounded separately: same
@@ -81,7 +88,8 @@ typedef struct claw_config {
     int use_fwaves;
     int limiter[CLAW_MAX_WAVES]; /* mthlim: 0 none,1 minmod,2 superbee,3 vanleer,4 MC,5 BW */
     int num_ghost;            /* mbc, must be 2                                    */
-    int bc_lower[3];          /* mthbc: 0 user, 1 extrap, 2 periodic, 3 wall       */
+    int bc_lower[3];          /* mthbc: 0 user, 1 extrap, 2 periodic, 3 wall,
+                                 CLAW_BC_PISTON                                    */
     int bc_upper[3];
     double dt_initial;        /* dtv(1)                                            */
     double dt_max;            /* dtv(2)                                            */
@@ -127,13 +135,16 @@ int claw_set_aux(claw_handle* h, const double* aux);
 
 /* One step of length dt from the current q, ghost cells from the boundary
  * conditions: bc2 + copyq2 + step2 (src/2d/claw2.f:622-668,
- * src/2d/step2.f90:2-251).  Writes the Courant number to *cfl and makes the
- * new q current; no accept/reject. */
+ * src/2d/step2.f90:2-251; bc3 + step3 in 3D, src/3d/step3.f90:3-873).
+ * Writes the Courant number to *cfl and makes the new q current; no
+ * accept/reject.  The step starts at the time the last advance reached
+ * (0 after claw_create), advanced by dt per claw_step. */
 int claw_step(claw_handle* h, double dt, double* cfl);
 
 /* Advance from tstart to tend with claw2's variable/fixed dt control,
  * rejection and retry (src/2d/claw2.f:494-784; src/1d/claw1.f:394-583 in
- * 1D).  dt_initial plays dtv(1); the returned stats carry dtv/cflv/nv. */
+ * 1D; src/3d/claw3.f:620-928 in 3D, with chkmth's method check returning
+ * info 6).  dt_initial plays dtv(1); the returned stats carry dtv/cflv/nv. */
 int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial,
                  claw_stats* stats);
 
