@@ -1,8 +1,10 @@
-"""Run a few steps of the 2D radial acoustics workload (for profiler captures).
+"""Run a few steps of the 2D radial or 3D heterogeneous acoustics workload
+(for profiler captures).
 
     python -m classic_b200.profile_step --n 3072 --steps 4 --precision fp64_fma
+    python -m classic_b200.profile_step --dim 3 --n 128 --steps 2
 
-Each step is one claw_step (bc2 + step2) of fixed dt = 0.9 dx / c.
+Each step is one claw_step (bc + step2 / step3) of fixed dt = 0.9 dx / c_max.
 """
 import argparse
 
@@ -12,17 +14,27 @@ from .solver import Solver
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--dim", type=int, default=2, choices=[2, 3])
     ap.add_argument("--n", type=int, default=3072)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", default="fp64_fma", choices=["fp64", "fp64_fma", "fp32"])
     args = ap.parse_args()
-    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=args.n)
-    s = Solver(rd.clawdata, solver, params, precision=args.precision)
+    if args.dim == 2:
+        rd, solver, params, q0, aux = problems.radial_acoustics_2d(n=args.n)
+        cmax = 2.0
+        prec = args.precision
+    else:
+        rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=args.n)
+        cmax = 1.0
+        prec = "fp64"
+    s = Solver(rd.clawdata, solver, params, precision=prec)
     s.set_q(q0)
-    dt = 0.9 * (2.0 / args.n) / 2.0
+    if aux is not None:
+        s.set_aux(aux)
+    dt = 0.9 * (2.0 / args.n) / cmax
     for _ in range(args.steps):
         s.step(dt)
-    print(f"{args.steps} steps of {args.n}^2 ({args.precision}), sum p = {s.get_q()[0].sum():.12e}")
+    print(f"{args.steps} steps of {args.n}^{args.dim} ({prec}), sum p = {s.get_q()[0].sum():.12e}")
     s.close()
 
 
