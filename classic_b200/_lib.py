@@ -103,6 +103,13 @@ SIGNATURES = {
     "claw_launch_count": (ctypes.c_longlong, [_P]),
     "claw_step2d_noalloc": (ctypes.c_int, [ctypes.POINTER(ClawConfig), _P, _P, ctypes.c_longlong,
                                            _P, ctypes.c_longlong, ctypes.c_double, _D, _P]),
+    "claw_batch_create": (ctypes.c_int, [ctypes.POINTER(ClawConfig), ctypes.c_int,
+                                         ctypes.POINTER(_P)]),
+    "claw_batch_destroy": (ctypes.c_int, [_P]),
+    "claw_batch_set_q": (ctypes.c_int, [_P, ctypes.c_int, _D]),
+    "claw_batch_get_q": (ctypes.c_int, [_P, ctypes.c_int, _D]),
+    "claw_batch_advance": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _D,
+                                          ctypes.POINTER(ClawStats)]),
     "claw_last_error": (ctypes.c_char_p, []),
     "claw_build_info": (ctypes.c_char_p, []),
 }

@@ -214,6 +214,11 @@ std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
         Acoustics1D<real> s{(real)cc, (real)zz, (real)hz};
         return std::unique_ptr<Runner>(new Runner1D<Acoustics1D<real>>(s));
     }
+    if (id == CLAW_SOLVER_EULER_ROE_2D) {
+        const double gamma = cfg.solver_params[0];
+        EulerRoe2D<real> s{(real)gamma, (real)(gamma - 1.0)};
+        return runner2d(cfg, s);
+    }
     if (id == CLAW_SOLVER_VC_ADVECTION_2D)
         return std::unique_ptr<Runner>(new Runner2D<VCAdvection2D<real>, MethodGeneric2D>(VCAdvection2D<real>{}));
     if (id == CLAW_SOLVER_VC_ACOUSTICS_1D)
@@ -227,6 +232,7 @@ bool solver_shape(int id, SolverShape* sh) {
     switch (id) {
         case CLAW_SOLVER_ACOUSTICS_2D: *sh = {2, 3, 2, 0}; return true;
         case CLAW_SOLVER_VC_ADVECTION_2D: *sh = {2, 1, 1, 3}; return true;
+        case CLAW_SOLVER_EULER_ROE_2D: *sh = {2, 4, 3, 0}; return true;
         case CLAW_SOLVER_ACOUSTICS_1D: *sh = {1, 2, 2, 0}; return true;
         case CLAW_SOLVER_VC_ACOUSTICS_1D: *sh = {1, 2, 2, 2}; return true;
         case CLAW_SOLVER_VC_ACOUSTICS_3D: *sh = {3, 4, 2, 2}; return true;

@@ -22,6 +22,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#ifndef EULER_MINB
+#define EULER_MINB 2
+#endif
+
 namespace clawb200 {
 
 // ------------------------------------------------------------------------
@@ -65,6 +69,140 @@ struct Acoustics2D {
         const real b2 = (zz * asdq[mv] + asdq[0]) * hz;
         bmasdq[0] = cc * (b1 * zz); bmasdq[mu] = real(0); bmasdq[mv] = -(cc * b1);
         bpasdq[0] = cc * (b2 * zz); bpasdq[mu] = real(0); bpasdq[mv] = cc * b2;
+    }
+};
+
+// ------------------------------------------------------------------------
+// 2D Euler equations, q = (rho, rho u, rho v, E), gamma-law gas.  Roe solver
+// with three waves (u-a; the entropy and shear wave at u; u+a) and the
+// Harten-Hyman entropy fix on transonic rarefactions in A^- dq (A^+ dq = the
+// total flux difference minus A^- dq); the transverse split uses the
+// eigenvectors of the transverse Jacobian at the same interface's Roe average.
+// (LeVeque, Finite Volume Methods for Hyperbolic Problems, 15.3 and 18.8;
+// Harten & Hyman, J. Comput. Phys. 50, 1983.)
+template <typename real_>
+struct EulerRoe2D {
+    using real = real_;
+    static constexpr int meqn = 4, mwaves = 3, maux = 0;
+    static constexpr int min_blocks = EULER_MINB;  // registers for the Roe state
+    real gamma, gamma1;
+    __host__ __device__ static constexpr bool wave_zero(int, int) { return false; }
+    __host__ __device__ static constexpr bool trans_zero(int, int) { return false; }
+
+    struct Roe { real u, v, enth, a, g1a2, euv, hu; };
+
+    __device__ __forceinline__ Roe average(const real* qL, const real* qR, int mu, int mv) const {
+        const real rhsqrtl = sqrt(qL[0]);
+        const real rhsqrtr = sqrt(qR[0]);
+        const real pl = gamma1 * (qL[3] - real(0.5) * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / qL[0]);
+        const real pr = gamma1 * (qR[3] - real(0.5) * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / qR[0]);
+        const real rhsq2 = rhsqrtl + rhsqrtr;
+        Roe r;
+        r.u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
+        r.v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
+        r.enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+        const real u2v2 = r.u * r.u + r.v * r.v;
+        const real a2 = gamma1 * (r.enth - real(0.5) * u2v2);
+        r.a = sqrt(a2);
+        r.g1a2 = gamma1 / a2;
+        r.euv = r.enth - u2v2;
+        r.hu = real(0.5) * u2v2;
+        return r;
+    }
+
+    // normal velocity and sound speed of a conserved state
+    __device__ __forceinline__ void state(const real* q, int mu, int mv, real& un, real& c) const {
+        const real p = gamma1 * (q[3] - real(0.5) * (q[mu] * q[mu] + q[mv] * q[mv]) / q[0]);
+        c = sqrt(gamma * p / q[0]);
+        un = q[mu] / q[0];
+    }
+
+    __device__ __forceinline__ void rpn(int ixy, const real* qL, const real* qR, const real*,
+                                        const real*, real w[mwaves][meqn], real s[mwaves],
+                                        real amdq[meqn], real apdq[meqn]) const {
+        const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
+        const Roe r = average(qL, qR, mu, mv);
+        real d[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) d[m] = qR[m] - qL[m];
+        const real a3 = r.g1a2 * (r.euv * d[0] + r.u * d[mu] + r.v * d[mv] - d[3]);
+        const real a2 = d[mv] - r.v * d[0];
+        const real a4 = (d[mu] + (r.a - r.u) * d[0] - r.a * a3) / (real(2) * r.a);
+        const real a1 = d[0] - a3 - a4;
+        w[0][0] = a1; w[0][mu] = a1 * (r.u - r.a); w[0][mv] = a1 * r.v; w[0][3] = a1 * (r.enth - r.u * r.a);
+        s[0] = r.u - r.a;
+        w[1][0] = a3; w[1][mu] = a3 * r.u; w[1][mv] = a3 * r.v + a2; w[1][3] = a3 * r.hu + a2 * r.v;
+        s[1] = r.u;
+        w[2][0] = a4; w[2][mu] = a4 * (r.u + r.a); w[2][mv] = a4 * r.v; w[2][3] = a4 * (r.enth + r.u * r.a);
+        s[2] = r.u + r.a;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) amdq[m] = real(0);
+        real ul, cl;
+        state(qL, mu, mv, ul, cl);
+        const real s0 = ul - cl;
+        real q1[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) q1[m] = qL[m] + w[0][m];
+        real u1, c1;
+        state(q1, mu, mv, u1, c1);
+        const real s1 = u1 - c1;
+        if (!(s0 >= real(0) && s[0] > real(0))) {
+            real sfract;
+            if (s0 < real(0) && s1 > real(0)) sfract = s0 * (s1 - s[0]) / (s1 - s0);
+            else if (s[0] < real(0)) sfract = s[0];
+            else sfract = real(0);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) amdq[m] = sfract * w[0][m];
+            if (s[1] < real(0)) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+                real ur, cr;
+                state(qR, mu, mv, ur, cr);
+                const real s3 = ur + cr;
+                real q2[4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) q2[m] = qR[m] - w[2][m];
+                real u2, c2;
+                state(q2, mu, mv, u2, c2);
+                const real s2 = u2 + c2;
+                real sf3;
+                if (s2 < real(0) && s3 > real(0)) sf3 = s2 * (s3 - s[2]) / (s3 - s2);
+                else if (s[2] < real(0)) sf3 = s[2];
+                else sf3 = real(0);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) amdq[m] = amdq[m] + sf3 * w[2][m];
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const real df = (s[0] * w[0][m] + s[1] * w[1][m]) + s[2] * w[2][m];
+            apdq[m] = df - amdq[m];
+        }
+    }
+
+    __device__ __forceinline__ void rpt(int ixy, int, const real* qL, const real* qR, const real*,
+                                        const real*, const real*, const real* asdq,
+                                        real bm[meqn], real bp[meqn]) const {
+        const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
+        const Roe r = average(qL, qR, mu, mv);
+        const real a3 = r.g1a2 * (r.euv * asdq[0] + r.u * asdq[mu] + r.v * asdq[mv] - asdq[3]);
+        const real a2 = asdq[mu] - r.u * asdq[0];
+        const real a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) / (real(2) * r.a);
+        const real a1 = asdq[0] - a3 - a4;
+        real w[3][4], sb[3];
+        w[0][0] = a1; w[0][mu] = a1 * r.u; w[0][mv] = a1 * (r.v - r.a); w[0][3] = a1 * (r.enth - r.v * r.a);
+        sb[0] = r.v - r.a;
+        w[1][0] = a3; w[1][mu] = a3 * r.u + a2; w[1][mv] = a3 * r.v; w[1][3] = a3 * r.hu + a2 * r.u;
+        sb[1] = r.v;
+        w[2][0] = a4; w[2][mu] = a4 * r.u; w[2][mv] = a4 * (r.v + r.a); w[2][3] = a4 * (r.enth + r.v * r.a);
+        sb[2] = r.v + r.a;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            bm[m] = (fmin(sb[0], real(0)) * w[0][m] + fmin(sb[1], real(0)) * w[1][m]) +
+                    fmin(sb[2], real(0)) * w[2][m];
+            bp[m] = (fmax(sb[0], real(0)) * w[0][m] + fmax(sb[1], real(0)) * w[1][m]) +
+                    fmax(sb[2], real(0)) * w[2][m];
+        }
     }
 };
 

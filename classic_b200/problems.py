@@ -290,3 +290,62 @@ def random_acoustics_3d(mx, my, mz, seed=0, bc=("extrap",) * 6, limiter="mc", tr
     q0[0] = 1.0 + 0.3 * rng.standard_normal((mz, my, mx))
     q0[1:] = 0.2 * rng.standard_normal((3, mz, my, mx))
     return rd, solver, params, q0, aux
+
+
+# ------------------------------------------------------------- 2D Euler ---
+def euler_quadrant_state(seed):
+    """Seeded four-quadrant Riemann data: per quadrant rho ~ U[0.5, 2],
+    p ~ U[0.1, 1.5], u, v ~ U[-0.75, 0.75]; split point ~ U[0.3, 0.7]^2.
+    Returns (x_split, y_split, prim[4 quadrants][rho, u, v, p]) with the
+    quadrants ordered (x < xs, y < ys), (x >= xs, y < ys), (x < xs, y >= ys),
+    (x >= xs, y >= ys)."""
+    rng = np.random.default_rng(seed)
+    prim = np.empty((4, 4))
+    for k in range(4):
+        prim[k, 0] = rng.uniform(0.5, 2.0)
+        prim[k, 3] = rng.uniform(0.1, 1.5)
+        prim[k, 1] = rng.uniform(-0.75, 0.75)
+        prim[k, 2] = rng.uniform(-0.75, 0.75)
+    xs, ys = rng.uniform(0.3, 0.7, size=2)
+    return float(xs), float(ys), prim
+
+
+def euler_quadrants(n=256, seed=0, gamma=1.4, tfinal=0.25, nout=1, dt_initial=1e-3,
+                    limiter="mc", order=2, trans=2, bc=("extrap",) * 4, shape=None):
+    """One instance of the batched Euler workload: gamma = 1.4, Roe solver with
+    the Harten-Hyman entropy fix, four-quadrant Riemann data on [0,1]^2 from
+    `seed` (euler_quadrant_state), n^2 cells (or shape = (mx, my)); order 2,
+    MC, transverse 2, extrapolation BCs, t_final 0.25."""
+    mx, my = shape if shape is not None else (n, n)
+    rd = ClawRunData("classic", 2)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("gamma", gamma)
+    cd = rd.clawdata
+    cd.lower, cd.upper, cd.num_cells = [0.0, 0.0], [1.0, 1.0], [mx, my]
+    cd.num_eqn, cd.num_aux, cd.capa_index = 4, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, dt_initial, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.transverse_waves, cd.dimensional_split = order, trans, "unsplit"
+    cd.num_waves, cd.limiter = 3, [limiter] * 3
+    cd.bc_lower, cd.bc_upper = [bc[0], bc[2]], [bc[1], bc[3]]
+    xs, ys, prim = euler_quadrant_state(seed)
+    x, _ = _centres(0.0, 1.0, mx)
+    y, _ = _centres(0.0, 1.0, my)
+    X, Y = np.meshgrid(x, y, indexing="xy")
+    quad = (X >= xs).astype(int) + 2 * (Y >= ys).astype(int)
+    rho, u, v, p = (prim[quad, k] for k in range(4))
+    q0 = np.empty((4, my, mx))
+    q0[0] = rho
+    q0[1] = rho * u
+    q0[2] = rho * v
+    q0[3] = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)
+    return rd, "euler_roe_2d", {"gamma": gamma}, q0, None
+
+
+def euler_ensemble_sizes(count=256, seed=0, nmin=128, nmax=1024):
+    """Grid sides of the batched workload: N = round(exp(U[ln nmin, ln nmax]))
+    per instance (log-uniform), from one seeded generator."""
+    rng = np.random.default_rng(seed)
+    return [int(round(float(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))) for _ in range(count)]

@@ -258,3 +258,59 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray,
     if solver_obj is None:
         s.close()
     return frames
+
+
+class BatchSolver:
+    """Many independent 2D grids of one solver and method (uneven sizes), each
+    with its own claw2 dt control, advanced together (claw_batch_* of the C
+    ABI): one persistent launch per step over the rows of every instance
+    still running."""
+
+    def __init__(self, clawdatas, solver: str, params: dict | None = None):
+        self.lib = _lib.load()
+        cds = [c.clawdata if isinstance(c, ClawRunData) else c for c in clawdatas]
+        self.count = len(cds)
+        arr = (ClawConfig * self.count)()
+        self.q_shapes = []
+        for k, cd in enumerate(cds):
+            arr[k] = make_config(cd, solver, params, "fp64")
+            cells = [arr[k].num_cells[d] for d in range(2)]
+            self.q_shapes.append((arr[k].num_eqn, cells[1], cells[0]))
+        self._cfgs = arr
+        h = ctypes.c_void_p()
+        check(self.lib.claw_batch_create(arr, self.count, ctypes.byref(h)), "claw_batch_create")
+        self._h = h
+
+    def set_q(self, k: int, q: np.ndarray):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        if q.shape != self.q_shapes[k]:
+            raise ValueError(f"q shape {q.shape} != {self.q_shapes[k]}")
+        check(self.lib.claw_batch_set_q(self._h, k, _dptr(q)), "claw_batch_set_q")
+
+    def get_q(self, k: int) -> np.ndarray:
+        out = np.empty(self.q_shapes[k], dtype=np.float64)
+        check(self.lib.claw_batch_get_q(self._h, k, _dptr(out)), "claw_batch_get_q")
+        return out
+
+    def advance(self, tstart: float, tend: float, dt_initial=None):
+        """Advance every instance; returns (first nonzero info or 0, [stats])."""
+        st = (ClawStats * self.count)()
+        dts = None
+        if dt_initial is not None:
+            dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt_initial, dtype=np.float64),
+                                                       (self.count,)))
+        info = check(self.lib.claw_batch_advance(self._h, float(tstart), float(tend),
+                                                 _dptr(dts) if dts is not None else None, st),
+                     "claw_batch_advance")
+        return info, [st[k].as_dict() for k in range(self.count)]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.claw_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

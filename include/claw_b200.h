@@ -180,6 +180,27 @@ int claw_step2d_noalloc(const claw_config* cfg, const double* q_in, double* q_ou
                         long long q_ld, const double* aux, long long aux_ld, double dt,
                         double* cfl, void* stream);
 
+/* ---- Batches: many independent 2D grids advanced together -------------
+ * Instances share the solver, its parameters, the method and the boundary
+ * conditions; their num_cells, lower/upper and dt limits may differ.  Each
+ * instance runs claw2's own dt control from its own Courant number
+ * (src/2d/claw2.f:494-784, per instance); one persistent launch per step
+ * covers the rows of every instance still advancing.  No counterpart in the
+ * reference, whose claw2 advances one grid per call. */
+typedef struct claw_batch claw_batch;
+
+/* count instances (1..1024), cfgs[k] for instance k; FP64, 2D. */
+int claw_batch_create(const claw_config* cfgs, int count, claw_batch** out);
+int claw_batch_destroy(claw_batch* b);
+/* q of instance k, [num_eqn][my][mx] as for claw_set_q / claw_get_q */
+int claw_batch_set_q(claw_batch* b, int k, const double* q);
+int claw_batch_get_q(claw_batch* b, int k, double* q);
+/* Advance every instance from tstart to tend.  dt_initial[k] seeds instance
+ * k (NULL: cfgs[k].dt_initial); stats[count] receives each instance's claw2
+ * returns and info.  Returns 0, or the first nonzero per-instance info. */
+int claw_batch_advance(claw_batch* b, double tstart, double tend, const double* dt_initial,
+                       claw_stats* stats);
+
 /* Last error message of the calling thread ("" if none). */
 const char* claw_last_error(void);
 

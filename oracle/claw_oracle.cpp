@@ -168,6 +168,162 @@ void rpt2_vc_advection(int ixy, int imp, int, int meqn, int, int maux, int mbc, 
     }
 }
 
+
+// ---- 2D Euler equations, Roe solver with the Harten-Hyman entropy fix -------
+// q = (rho, rho u, rho v, E), p = (gamma-1)(E - (rho u^2 + rho v^2)/2 / rho).
+// Roe averages of u, v and the enthalpy H = (E + p)/rho between the left and
+// right states; three waves: acoustic u-a, the entropy + shear wave u, and
+// acoustic u+a (LeVeque, Finite Volume Methods for Hyperbolic Problems,
+// sections 15.3 and 18.8).  The entropy fix splits a transonic rarefaction
+// in the 1- or 3-wave by Harten and Hyman's linear interpolation of the
+// characteristic speed across the wave (Harten & Hyman, J. Comput. Phys. 50,
+// 1983).  This is the pointwise arithmetic, identical to the device functor.
+struct RoeAvg {
+    double u, v, enth, a, g1a2, euv, hu;
+};
+
+inline RoeAvg roe_average(const double* qL, const double* qR, int mu, int mv) {
+    const double g1 = g_gamma - 1.0;
+    const double rhsqrtl = std::sqrt(qL[0]);
+    const double rhsqrtr = std::sqrt(qR[0]);
+    const double pl = g1 * (qL[3] - 0.5 * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / qL[0]);
+    const double pr = g1 * (qR[3] - 0.5 * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / qR[0]);
+    const double rhsq2 = rhsqrtl + rhsqrtr;
+    RoeAvg r;
+    r.u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
+    r.v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
+    r.enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+    const double u2v2 = r.u * r.u + r.v * r.v;
+    const double a2 = g1 * (r.enth - 0.5 * u2v2);
+    r.a = std::sqrt(a2);
+    r.g1a2 = g1 / a2;
+    r.euv = r.enth - u2v2;
+    r.hu = 0.5 * u2v2;
+    return r;
+}
+
+// sound speed and normal velocity of a conserved state
+inline void euler_state(const double* q, int mu, int mv, double* un, double* c) {
+    const double g1 = g_gamma - 1.0;
+    const double p = g1 * (q[3] - 0.5 * (q[mu] * q[mu] + q[mv] * q[mv]) / q[0]);
+    *c = std::sqrt(g_gamma * p / q[0]);
+    *un = q[mu] / q[0];
+}
+
+// pointwise normal solve: qL = q(i-1), qR = q(i); mu/mv 0-based
+void euler_rpn(const double* qL, const double* qR, int mu, int mv, double w[3][4],
+               double s[3], double* amdq, double* apdq) {
+    const RoeAvg r = roe_average(qL, qR, mu, mv);
+    double d[4];
+    for (int m = 0; m < 4; ++m) d[m] = qR[m] - qL[m];
+    const double a3 = r.g1a2 * (r.euv * d[0] + r.u * d[mu] + r.v * d[mv] - d[3]);
+    const double a2 = d[mv] - r.v * d[0];
+    const double a4 = (d[mu] + (r.a - r.u) * d[0] - r.a * a3) / (2.0 * r.a);
+    const double a1 = d[0] - a3 - a4;
+    w[0][0] = a1;
+    w[0][mu] = a1 * (r.u - r.a);
+    w[0][mv] = a1 * r.v;
+    w[0][3] = a1 * (r.enth - r.u * r.a);
+    s[0] = r.u - r.a;
+    w[1][0] = a3;
+    w[1][mu] = a3 * r.u;
+    w[1][mv] = a3 * r.v + a2;
+    w[1][3] = a3 * r.hu + a2 * r.v;
+    s[1] = r.u;
+    w[2][0] = a4;
+    w[2][mu] = a4 * (r.u + r.a);
+    w[2][mv] = a4 * r.v;
+    w[2][3] = a4 * (r.enth + r.u * r.a);
+    s[2] = r.u + r.a;
+    // A^- dq with the entropy fix; A^+ dq = sum s w - A^- dq
+    for (int m = 0; m < 4; ++m) amdq[m] = 0.0;
+    double ul, cl;
+    euler_state(qL, mu, mv, &ul, &cl);
+    const double s0 = ul - cl;  // u - c left of the 1-wave
+    double q1[4];
+    for (int m = 0; m < 4; ++m) q1[m] = qL[m] + w[0][m];
+    double u1, c1;
+    euler_state(q1, mu, mv, &u1, &c1);
+    const double s1 = u1 - c1;  // u - c right of the 1-wave
+    if (!(s0 >= 0.0 && s[0] > 0.0)) {
+        double sfract;
+        if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) / (s1 - s0);
+        else if (s[0] < 0.0) sfract = s[0];
+        else sfract = 0.0;
+        for (int m = 0; m < 4; ++m) amdq[m] = sfract * w[0][m];
+        if (s[1] < 0.0) {
+            for (int m = 0; m < 4; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+            double ur, cr;
+            euler_state(qR, mu, mv, &ur, &cr);
+            const double s3 = ur + cr;  // u + c right of the 3-wave
+            double q2[4];
+            for (int m = 0; m < 4; ++m) q2[m] = qR[m] - w[2][m];
+            double u2, c2;
+            euler_state(q2, mu, mv, &u2, &c2);
+            const double s2 = u2 + c2;  // u + c left of the 3-wave
+            double sf3;
+            if (s2 < 0.0 && s3 > 0.0) sf3 = s2 * (s3 - s[2]) / (s3 - s2);
+            else if (s[2] < 0.0) sf3 = s[2];
+            else sf3 = 0.0;
+            for (int m = 0; m < 4; ++m) amdq[m] = amdq[m] + sf3 * w[2][m];
+        }
+    }
+    for (int m = 0; m < 4; ++m) {
+        const double df = (s[0] * w[0][m] + s[1] * w[1][m]) + s[2] * w[2][m];
+        apdq[m] = df - amdq[m];
+    }
+}
+
+// pointwise transverse split of asdq on the eigenvectors of the transverse
+// flux Jacobian at the Roe average of the interface's two states
+void euler_rpt(const double* qL, const double* qR, int mu, int mv, const double* asdq,
+               double* bm, double* bp) {
+    const RoeAvg r = roe_average(qL, qR, mu, mv);
+    const double a3 = r.g1a2 * (r.euv * asdq[0] + r.u * asdq[mu] + r.v * asdq[mv] - asdq[3]);
+    const double a2 = asdq[mu] - r.u * asdq[0];
+    const double a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) / (2.0 * r.a);
+    const double a1 = asdq[0] - a3 - a4;
+    double w[3][4], sb[3];
+    w[0][0] = a1; w[0][mu] = a1 * r.u; w[0][mv] = a1 * (r.v - r.a); w[0][3] = a1 * (r.enth - r.v * r.a);
+    sb[0] = r.v - r.a;
+    w[1][0] = a3; w[1][mu] = a3 * r.u + a2; w[1][mv] = a3 * r.v; w[1][3] = a3 * r.hu + a2 * r.u;
+    sb[1] = r.v;
+    w[2][0] = a4; w[2][mu] = a4 * r.u; w[2][mv] = a4 * (r.v + r.a); w[2][3] = a4 * (r.enth + r.v * r.a);
+    sb[2] = r.v + r.a;
+    for (int m = 0; m < 4; ++m) {
+        bm[m] = (std::fmin(sb[0], 0.0) * w[0][m] + std::fmin(sb[1], 0.0) * w[1][m]) +
+                std::fmin(sb[2], 0.0) * w[2][m];
+        bp[m] = (std::fmax(sb[0], 0.0) * w[0][m] + std::fmax(sb[1], 0.0) * w[1][m]) +
+                std::fmax(sb[2], 0.0) * w[2][m];
+    }
+}
+
+void rpn2_euler_roe(int ixy, int, int meqn, int mwaves, int, int mbc, int mx, const double* ql,
+                    const double* qr, const double*, const double*, double* wave, double* s,
+                    double* amdq, double* apdq) {
+    const Slice q{meqn, 1 - mbc}, w{meqn * mwaves, 1 - mbc}, sv{mwaves, 1 - mbc};
+    const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double wl[3][4], sl[3];
+        euler_rpn(&qr[q.at(1, i - 1)], &ql[q.at(1, i)], mu, mv, wl, sl, &amdq[q.at(1, i)],
+                  &apdq[q.at(1, i)]);
+        for (int k = 0; k < 3; ++k) {
+            for (int m = 0; m < 4; ++m) wave[w.at(1, i) + k * meqn + m] = wl[k][m];
+            s[sv.at(k + 1, i)] = sl[k];
+        }
+    }
+}
+
+void rpt2_euler_roe(int ixy, int, int, int meqn, int, int, int mbc, int mx, const double* ql,
+                    const double* qr, const double*, const double*, const double*,
+                    const double* asdq, double* bmasdq, double* bpasdq) {
+    const Slice q{meqn, 1 - mbc};
+    const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i)
+        euler_rpt(&qr[q.at(1, i - 1)], &ql[q.at(1, i)], mu, mv, &asdq[q.at(1, i)],
+                  &bmasdq[q.at(1, i)], &bpasdq[q.at(1, i)]);
+}
+
 // ---- 1D acoustics --------------------------------------------------------------
 typedef void (*rp1_t)(int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
                       const double* ql, const double* qr, const double* auxl,
@@ -366,16 +522,12 @@ bool pick2(int solver, rpn2_t* rpn, rpt2_t* rpt) {
     switch (solver) {
         case ORC_ACOUSTICS_2D: *rpn = rpn2_acoustics; *rpt = rpt2_acoustics; return true;
         case ORC_VC_ADVECTION_2D: *rpn = rpn2_vc_advection; *rpt = rpt2_vc_advection; return true;
+        case ORC_EULER_ROE_2D: *rpn = rpn2_euler_roe; *rpt = rpt2_euler_roe; return true;
         default: return false;
     }
 }
 
 }  // namespace
-
-// Euler / 3D solvers and step3 live in claw_oracle_ext.cpp.
-namespace orc_ext {
-bool pick2_ext(int solver, rpn2_t* rpn, rpt2_t* rpt);
-}
 
 extern "C" {
 
@@ -387,7 +539,7 @@ int orc_step2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const dou
               const int* method, const int* mthlim, int use_fwave, double* cfl_out) {
     rpn2_t rpn2;
     rpt2_t rpt2;
-    if (!pick2(g_solver, &rpn2, &rpt2) && !orc_ext::pick2_ext(g_solver, &rpn2, &rpt2)) return -1;
+    if (!pick2(g_solver, &rpn2, &rpt2)) return -1;
     const int maxm = std::max(mx, my);
     const int n = maxm + 2 * mbc;
     const int nx = mx + 2 * mbc;

@@ -1,0 +1,120 @@
+"""2D Euler (Roe + Harten-Hyman entropy fix) on the GPU against the CPU
+oracle: single grids and the batched ensemble, bit for bit (value equality,
++0 == -0) in q, the Courant numbers and every instance's dt sequence."""
+import numpy as np
+import pytest
+
+from classic_b200 import problems
+from classic_b200.solver import BatchSolver, Solver
+from helpers import same
+from pyoracle import OracleGrid
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(7, 5), (29, 31), (64, 40), (3, 57)]
+BCS = [("extrap",) * 4, ("wall",) * 4, ("periodic",) * 4, ("wall", "extrap", "periodic", "periodic")]
+
+
+def _pair(rd, solver, params, q0):
+    g = Solver(rd.clawdata, solver, params)
+    o = OracleGrid(rd.clawdata, solver, params)
+    g.set_q(q0)
+    o.set_q(q0)
+    return g, o
+
+
+@pytest.mark.parametrize("shape", SIZES)
+@pytest.mark.parametrize("bc", BCS)
+def test_single_step_bitwise(shape, bc):
+    rd, solver, params, q0, _ = problems.euler_quadrants(shape=shape, seed=shape[0] + 7 * shape[1],
+                                                         bc=bc)
+    g, o = _pair(rd, solver, params, q0)
+    for dt in (0.002, 0.003):
+        assert g.step(dt) == o.step(dt)
+        assert same(g.get_q(), o.get_q())
+    g.close()
+
+
+@pytest.mark.parametrize("lim", ["none", "minmod", "superbee", "vanleer", "mc", 5])
+@pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 0), (2, 1), (2, 2)])
+def test_methods_bitwise(lim, order, trans):
+    rd, solver, params, q0, _ = problems.euler_quadrants(shape=(37, 30), seed=5, limiter=lim,
+                                                         order=order, trans=trans,
+                                                         bc=("wall", "extrap", "extrap", "wall"))
+    g, o = _pair(rd, solver, params, q0)
+    for _ in range(3):
+        assert g.step(0.004) == o.step(0.004)
+    assert same(g.get_q(), o.get_q())
+    g.close()
+
+
+def test_advance_reject_and_dt_sequence():
+    rd, solver, params, q0, _ = problems.euler_quadrants(n=96, seed=11, dt_initial=0.05)
+    g, o = _pair(rd, solver, params, q0)
+    ig, sg = g.advance(0.0, 0.1, 0.05)
+    io, so = o.advance(0.0, 0.1, 0.05)
+    assert ig == io == 0 and sg["steps_rejected"] >= 1
+    for key in ("t_reached", "dt_min", "dt_max_taken", "dt_next", "cfl_max_seen", "cfl_last",
+                "steps_taken"):
+        assert sg[key] == so[key], key
+    assert same(g.get_q(), o.get_q())
+    g.close()
+
+
+def _ensemble(sizes, seed0=100):
+    insts = [problems.euler_quadrants(n=n, seed=seed0 + k) for k, n in enumerate(sizes)]
+    return insts
+
+
+def test_batch_matches_oracle_per_instance():
+    """Uneven sizes, per-instance dt: every instance ends bitwise equal to
+    claw2 run on it alone, with its own step count."""
+    sizes = [40, 23, 57, 64, 29, 45, 33, 50]
+    insts = _ensemble(sizes)
+    rds = [i[0] for i in insts]
+    b = BatchSolver(rds, "euler_roe_2d", {"gamma": 1.4})
+    for k, inst in enumerate(insts):
+        b.set_q(k, inst[3])
+    info, stats = b.advance(0.0, 0.25)
+    assert info == 0
+    steps = set()
+    for k, (rd, solver, params, q0, _) in enumerate(insts):
+        o = OracleGrid(rd.clawdata, solver, params)
+        o.set_q(q0)
+        io, so = o.advance(0.0, 0.25, rd.clawdata.dt_initial)
+        assert io == 0
+        for key in ("t_reached", "dt_next", "cfl_max_seen", "steps_taken"):
+            assert stats[k][key] == so[key], (k, key)
+        assert same(b.get_q(k), o.get_q()), k
+        steps.add(stats[k]["steps_taken"])
+    assert len(steps) > 1  # instances really took different step counts
+    b.close()
+
+
+def test_batch_continues_across_calls():
+    """Two advances (two output frames) equal one oracle run with claw2ez's
+    dt carry-over between frames."""
+    sizes = [30, 48, 36]
+    insts = _ensemble(sizes, seed0=300)
+    b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4})
+    for k, inst in enumerate(insts):
+        b.set_q(k, inst[3])
+    info, st1 = b.advance(0.0, 0.1)
+    assert info == 0
+    info, st2 = b.advance(0.1, 0.2, [s["dt_next"] for s in st1])
+    assert info == 0
+    for k, (rd, solver, params, q0, _) in enumerate(insts):
+        o = OracleGrid(rd.clawdata, solver, params)
+        o.set_q(q0)
+        _, so1 = o.advance(0.0, 0.1, rd.clawdata.dt_initial)
+        _, so2 = o.advance(0.1, 0.2, so1["dt_next"])
+        assert st2[k]["steps_taken"] == so2["steps_taken"]
+        assert same(b.get_q(k), o.get_q()), k
+    b.close()
+
+
+def test_batch_rejects_mixed_methods():
+    rd1 = problems.euler_quadrants(n=16)[0]
+    rd2 = problems.euler_quadrants(n=16, limiter="minmod")[0]
+    with pytest.raises(Exception):
+        BatchSolver([rd1, rd2], "euler_roe_2d", {"gamma": 1.4})
