@@ -30,5 +30,7 @@ def rel_diff(a, b):
 
 
 def same(a, b):
-    """Bit-for-bit value equality (+0 == -0), NaN never equal."""
-    return bool(np.array_equal(np.asarray(a), np.asarray(b)))
+    """Bit-for-bit value equality (+0 == -0); a NaN matches only a NaN at the
+    same position (the Roe solver can leave a strong rarefaction with
+    negative pressure, on either side identically)."""
+    return bool(np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True))
