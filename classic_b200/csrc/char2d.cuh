@@ -124,13 +124,24 @@ struct ColSrc {
 #ifndef CLAW_CHAR_MINB
 #define CLAW_CHAR_MINB 3  // 168 registers, 12 warps per SM: no spills in FP64
 #endif
+#ifndef CLAW_CHAR_UNROLL
+#define CLAW_CHAR_UNROLL 2
+#endif
 
-// PX: x-boundaries are periodic, so halo lanes of the edge strips may need
-// a column from the far side of the grid that is not in the ring box; those
-// come from global memory.  Without PX that path is compiled out.
-template <typename real, int LIM, bool PX>
+// Boundary-condition classes compiled separately:
+//   CHAR_BC_EXTRAP  extrapolation on every side (no sign flips)
+//   CHAR_BC_WALLS   any mix without periodic x (wall sign flips applied)
+//   CHAR_BC_PERX    periodic x: halo lanes of the edge strips may need a
+//                   column from the far side of the grid that is not in the
+//                   ring box, read from global memory
+enum { CHAR_BC_EXTRAP = 0, CHAR_BC_WALLS = 1, CHAR_BC_PERX = 2 };
+
+template <typename real, int LIM, int BCM>
 __global__ void __launch_bounds__(32 * WARPS2D, CLAW_CHAR_MINB)
 step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
+    constexpr bool PX = BCM == CHAR_BC_PERX;
+    constexpr bool WALLS = BCM != CHAR_BC_EXTRAP;
+    constexpr int kUnroll = CLAW_CHAR_UNROLL;
     using R = CharRing<real>;
     constexpr int W = R::W;
     constexpr unsigned FULL = 0xffffffffu;
@@ -222,8 +233,10 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
             if constexpr (PX) {
                 if (any_global && cs.glob) v = qold[m * A.fstride + (long long)sr * A.ld + cs.src];
             }
-            if (m == 1 && cs.neg) v = -v;
-            if (m == 2 && nyneg) v = -v;
+            if constexpr (WALLS) {
+                if (m == 1 && cs.neg) v = -v;
+                if (m == 2 && nyneg) v = -v;
+            }
             return v;
         };
         auto row_ptr = [&](int r) -> const real* {
@@ -256,7 +269,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
         }
 
         // two rows per trip: the carried state rotates by renaming, not copies
-#pragma unroll 2
+#pragma unroll kUnroll
         for (int t = r0 - 1; t <= r0 + nr && !failed; ++t) {
             if (!wait_row(t + 1)) { failed = true; fail_row = t + 1; break; }
             bool ngt, ngn;

@@ -11,7 +11,7 @@ namespace clawb200 {
 
 namespace {
 
-template <typename real, int LIM, bool PX>
+template <typename real, int LIM, int BCM>
 struct CharRunner : Runner {
     CharArgs<real> args;
     int grid = 1, smem = 0;
@@ -42,12 +42,12 @@ struct CharRunner : Runner {
             if (rc) return rc;
         }
         smem = R::SMEM;
-        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, PX>,
+        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, BCM>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, PX>,
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
         args.units = (long long)args.nstrips * g.my;
@@ -60,21 +60,25 @@ struct CharRunner : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_char_kernel<real, LIM, PX><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        step2_char_kernel<real, LIM, BCM><<<grid, 32 * WARPS2D, smem, s>>>(args);
         return cudaGetLastError();
     }
 };
 
-template <typename real, bool PX>
+template <typename real, int BCM>
 std::unique_ptr<Runner> pick_lim(int lim) {
-    if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, PX>());
-    return std::unique_ptr<Runner>(new CharRunner<real, -1, PX>());
+    if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, BCM>());
+    return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM>());
 }
 
 template <typename real>
 std::unique_ptr<Runner> pick(const claw_config& cfg) {
     const bool px = cfg.bc_lower[0] == BC_PERIODIC || cfg.bc_upper[0] == BC_PERIODIC;
-    return px ? pick_lim<real, true>(cfg.limiter[0]) : pick_lim<real, false>(cfg.limiter[0]);
+    bool extrap = true;
+    for (int d = 0; d < 2; ++d) extrap = extrap && cfg.bc_lower[d] == BC_EXTRAP && cfg.bc_upper[d] == BC_EXTRAP;
+    if (px) return pick_lim<real, CHAR_BC_PERX>(cfg.limiter[0]);
+    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(cfg.limiter[0]);
+    return pick_lim<real, CHAR_BC_WALLS>(cfg.limiter[0]);
 }
 
 }  // namespace
