@@ -91,6 +91,23 @@ struct EulerRoe2D {
 
     struct Roe { real u, v, enth, a, g1a2, euv, hu; };
 
+    // Interface context: the Roe average of (qL, qR) that rpn and both rpt
+    // calls of one interface share (computed once; the same values).
+    struct Ctx { real u, v, enth, a, g1a2; };
+    __device__ __forceinline__ Ctx context(int ixy, const real* qL, const real* qR) const {
+        const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
+        const Roe r = average(qL, qR, mu, mv);
+        return Ctx{r.u, r.v, r.enth, r.a, r.g1a2};
+    }
+    __device__ __forceinline__ static Roe expand(const Ctx& c) {
+        Roe r;
+        r.u = c.u; r.v = c.v; r.enth = c.enth; r.a = c.a; r.g1a2 = c.g1a2;
+        const real u2v2 = r.u * r.u + r.v * r.v;
+        r.euv = r.enth - u2v2;
+        r.hu = real(0.5) * u2v2;
+        return r;
+    }
+
     __device__ __forceinline__ Roe average(const real* qL, const real* qR, int mu, int mv) const {
         const real rhsqrtl = sqrt(qL[0]);
         const real rhsqrtr = sqrt(qR[0]);
@@ -120,8 +137,14 @@ struct EulerRoe2D {
     __device__ __forceinline__ void rpn(int ixy, const real* qL, const real* qR, const real*,
                                         const real*, real w[mwaves][meqn], real s[mwaves],
                                         real amdq[meqn], real apdq[meqn]) const {
+        rpn_ctx(ixy, context(ixy, qL, qR), qL, qR, w, s, amdq, apdq);
+    }
+
+    __device__ __forceinline__ void rpn_ctx(int ixy, const Ctx& c, const real* qL, const real* qR,
+                                            real w[mwaves][meqn], real s[mwaves], real amdq[meqn],
+                                            real apdq[meqn]) const {
         const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
-        const Roe r = average(qL, qR, mu, mv);
+        const Roe r = expand(c);
         real d[4];
 #pragma unroll
         for (int m = 0; m < 4; ++m) d[m] = qR[m] - qL[m];
@@ -180,11 +203,16 @@ struct EulerRoe2D {
         }
     }
 
-    __device__ __forceinline__ void rpt(int ixy, int, const real* qL, const real* qR, const real*,
+    __device__ __forceinline__ void rpt(int ixy, int imp, const real* qL, const real* qR, const real*,
                                         const real*, const real*, const real* asdq,
                                         real bm[meqn], real bp[meqn]) const {
+        rpt_ctx(ixy, imp, context(ixy, qL, qR), asdq, bm, bp);
+    }
+
+    __device__ __forceinline__ void rpt_ctx(int ixy, int, const Ctx& c, const real* asdq,
+                                            real bm[meqn], real bp[meqn]) const {
         const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
-        const Roe r = average(qL, qR, mu, mv);
+        const Roe r = expand(c);
         const real a3 = r.g1a2 * (r.euv * asdq[0] + r.u * asdq[mu] + r.v * asdq[mv] - asdq[3]);
         const real a2 = asdq[mu] - r.u * asdq[0];
         const real a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) / (real(2) * r.a);

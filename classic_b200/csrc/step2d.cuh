@@ -118,6 +118,28 @@ struct Ring2D {
 // from buffer `cur`.  Per warp; ring/bars/seq_base are the warp's TMA ring.
 // Folds the chunk's Courant numbers into cfl; on a device-wait time-out sets
 // `failed` and the grid's error flag after draining its copies.
+// Optional solver hook: an interface context (S::Ctx, S::context) shared by
+// the normal solve and both transverse splits of one interface.  Solvers
+// without it are called through the plain rpn / rpt contract.
+template <class S, class = void>
+struct solver_ctx {
+    struct type {};
+    static constexpr bool value = false;
+};
+template <class S>
+struct solver_ctx<S, std::void_t<typename S::Ctx>> {
+    using type = typename S::Ctx;
+    static constexpr bool value = true;
+};
+
+template <class S>
+__device__ __forceinline__ typename solver_ctx<S>::type iface_ctx(const S& s, int ixy,
+                                                                  const typename S::real* qL,
+                                                                  const typename S::real* qR) {
+    if constexpr (solver_ctx<S>::value) return s.context(ixy, qL, qR);
+    else return typename solver_ctx<S>::type{};
+}
+
 template <class S>
 struct StepConsts {
     typename S::real dtdx, dtdy;   // dt/dx, dt/dy in the update's precision
@@ -254,6 +276,7 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
     real wy[MW][ME], sy[MW], amy[ME], apy[ME], dotl_y[MW];
     // contributions of y-interface t-1 to cell (c, t-1)
     real P1[ME], P3[ME], P4[ME], Fy_prev[ME];
+    typename solver_ctx<S>::type cy{};  // context of y-interface t
 #pragma unroll
     for (int m = 0; m < ME; ++m) {
         Ax_prev[m] = q2_prev[m] = real(0);
@@ -274,7 +297,9 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
         real a_c[MAX], a_cn[MAX];
         aux_at(rfirst, 0, a_c);
         aux_at(rfirst + 1, 0, a_cn);
-        A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wy, sy, amy, apy);
+        cy = iface_ctx(A.solver, 2, qc_t, qc_n);
+        if constexpr (solver_ctx<S>::value) A.solver.rpn_ctx(2, cy, qc_t, qc_n, wy, sy, amy, apy);
+        else A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wy, sy, amy, apy);
         if (cy_ok && rfirst + 1 >= 0) {
             const double dt0 = capa ? dtdy_d / (double)a_c[ic] : dtdy_d;
             const double dt1 = capa ? dtdy_d / (double)a_cn[ic] : dtdy_d;
@@ -310,7 +335,9 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
         real q3[ME];
         {
             real w[MW][ME], s[MW], amdq[ME], apdq[ME];
-            A.solver.rpn(1, qm_t, qc_t, a_m, a_c, w, s, amdq, apdq);
+            const auto cx = iface_ctx(A.solver, 1, qm_t, qc_t);
+            if constexpr (solver_ctx<S>::value) A.solver.rpn_ctx(1, cx, qm_t, qc_t, w, s, amdq, apdq);
+            else A.solver.rpn(1, qm_t, qc_t, a_m, a_c, w, s, amdq, apdq);
             const real dtm = capa ? dtdx / a_m[ic] : dtdx;  // dtdx1d(i-1)
             const real dtc = capa ? dtdx / a_c[ic] : dtdx;  // dtdx1d(i)
             {
@@ -394,7 +421,8 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                     }
                 }
                 real bm[ME], bp[ME];
-                A.solver.rpt(1, 1, qm_t, qc_t, a_mp, a_m, a_mn, amdq, bm, bp);
+                if constexpr (solver_ctx<S>::value) A.solver.rpt_ctx(1, 1, cx, amdq, bm, bp);
+                else A.solver.rpt(1, 1, qm_t, qc_t, a_mp, a_m, a_mn, amdq, bm, bp);
                 const real hm = real(0.5) * dtm, hc = real(0.5) * dtc;
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
@@ -402,7 +430,8 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                     s3[m] = -(hm * bm[m]);  // gadd(:,1,i-1) from this interface
                     s4[m] = -(hm * bp[m]);  // gadd(:,2,i-1)
                 }
-                A.solver.rpt(1, 2, qm_t, qc_t, a_cp, a_c, a_cn, apdq, bm, bp);
+                if constexpr (solver_ctx<S>::value) A.solver.rpt_ctx(1, 2, cx, apdq, bm, bp);
+                else A.solver.rpt(1, 2, qm_t, qc_t, a_cp, a_c, a_cn, apdq, bm, bp);
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
                     if (S::trans_zero(1, m)) continue;
@@ -450,7 +479,9 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
 
         // ======== y-interface t+1 raw; y-interface t limited; y-part of (c, t-1) ========
         real wn[MW][ME], sn[MW], amn[ME], apn[ME];
-        A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wn, sn, amn, apn);
+        const auto cyn = iface_ctx(A.solver, 2, qc_t, qc_n);
+        if constexpr (solver_ctx<S>::value) A.solver.rpn_ctx(2, cyn, qc_t, qc_n, wn, sn, amn, apn);
+        else A.solver.rpn(2, qc_t, qc_n, a_c, a_cn, wn, sn, amn, apn);
         {
             const double dt0 = capa ? dtdy_d / (double)a_c[ic] : dtdy_d;
             const double dt1 = capa ? dtdy_d / (double)a_cn[ic] : dtdy_d;
@@ -528,8 +559,13 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                     apy[m] = apy[m] - cqy[m];
                 }
             }
-            A.solver.rpt(2, 1, qc_p, qc_t, a_mp, a_cp, a_pp, amy, bma, bpa);
-            A.solver.rpt(2, 2, qc_p, qc_t, a_m, a_c, a_p, apy, bmb, bpb);
+            if constexpr (solver_ctx<S>::value) {
+                A.solver.rpt_ctx(2, 1, cy, amy, bma, bpa);
+                A.solver.rpt_ctx(2, 2, cy, apy, bmb, bpb);
+            } else {
+                A.solver.rpt(2, 1, qc_p, qc_t, a_mp, a_cp, a_pp, amy, bma, bpa);
+                A.solver.rpt(2, 2, qc_p, qc_t, a_m, a_c, a_p, apy, bmb, bpb);
+            }
         }
         const real hp = real(0.5) * dty_p, ht = real(0.5) * dty_t;
         const bool out = (t - 1 >= r0) && (lane >= 1) && (lane <= STRIP) && (c < mx);
@@ -572,6 +608,7 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
             qc_t[m] = qc_n[m];
         }
 #pragma unroll
+        cy = cyn;
         for (int mw = 0; mw < MW; ++mw) {
             dotl_y[mw] = dotr_y[mw];
             sy[mw] = sn[mw];
