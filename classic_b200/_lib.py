@@ -111,6 +111,25 @@ SIGNATURES = {
     "claw_batch_advance": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _D,
                                           ctypes.POINTER(ClawStats)]),
     "claw_last_error": (ctypes.c_char_p, []),
+    # learned corrector kernels (include/claw_nn.h)
+    "nn_conv3x3_forward": (ctypes.c_int, [_P, _P, _P, _P, _P] + [ctypes.c_int] * 7 + [_P]),
+    "nn_conv3x3_wgrad": (ctypes.c_int, [_P] * 6 + [ctypes.c_int] * 5 + [_P]),
+    "nn_flip_weights": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
+    "nn_gelu_backward": (ctypes.c_int, [_P, _P, _P, ctypes.c_longlong, _P]),
+    "nn_mse_grad": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                   _P]),
+    "nn_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_longlong] + [ctypes.c_float] * 4 +
+                [ctypes.c_int, _P]),
+    "nn_block_average": (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.c_longlong, _P,
+                                        ctypes.c_longlong, ctypes.c_longlong] + [ctypes.c_int] * 4 +
+                         [_P]),
+    "nn_features": (ctypes.c_int, [_P, _P, ctypes.c_longlong, ctypes.c_longlong] +
+                    [ctypes.c_int] * 3 + [_P, _P, _P]),
+    "nn_residual_target": (ctypes.c_int, [_P, _P, ctypes.c_longlong, ctypes.c_longlong] +
+                           [ctypes.c_int] * 3 + [_P, _P, _P]),
+    "nn_apply_correction": (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int,
+                                           ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_double,
+                                           ctypes.c_double, _P, _P]),
     "claw_build_info": (ctypes.c_char_p, []),
 }
 

@@ -1,0 +1,583 @@
+// Convolutional coarse-grid corrector: the network's kernels (C ABI, raw
+// device pointers, declared in include/claw_nn.h).
+//
+// The corrector is a stack of 3x3 "same" convolutions over NHWC BF16
+// activations with FP32 accumulation on the tensor cores (mma.sync m16n8k16
+// BF16 -> FP32), GELU between layers.  Training runs on the device with the
+// kernels below: the forward convolution (optionally saving the FP32
+// pre-activation), the data gradient (the same convolution with flipped and
+// transposed weights), the weight/bias gradient (a pixel-reduction GEMM per
+// tile plus a reduction over tiles), GELU's derivative, the MSE loss
+// gradient and Adam.  Glue kernels move between the solver's FP64 SoA q and
+// the network: block averages of a fine grid, input features, residual
+// targets, and the corrector's application with a per-tile conservative
+// projection and a positivity fallback to the plain step.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/claw_nn.h"
+
+namespace {
+
+constexpr int TILE = 16;              // output tile edge (pixels)
+constexpr int HALO = TILE + 2;        // input tile edge with the 3x3 halo
+constexpr int NPIX = TILE * TILE;     // 256 output pixels per CTA
+constexpr int NTHREADS = 256;         // 8 warps
+
+__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) {
+    return *reinterpret_cast<const uint32_t*>(p);
+}
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// GELU(z) = z Phi(z) with Phi the standard normal CDF, and its derivative
+// Phi(z) + z phi(z).
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+// Load a HALO x HALO x CP input tile (zero outside the image) into shared
+// memory with a row pitch of CP + 8 elements (conflict-free fragment loads).
+template <int CP>
+__device__ __forceinline__ void load_halo(__nv_bfloat16* xs, const __nv_bfloat16* x, int n, int h,
+                                          int w, int y0, int x0) {
+    constexpr int CH = CP / 8;  // 16-byte chunks per pixel
+    for (int e = threadIdx.x; e < HALO * HALO * CH; e += NTHREADS) {
+        const int pix = e / CH, ck = e % CH;
+        const int gy = y0 + pix / HALO - 1, gx = x0 + pix % HALO - 1;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (gy >= 0 && gy < h && gx >= 0 && gx < w)
+            v = *reinterpret_cast<const uint4*>(x + (((long long)n * h + gy) * w + gx) * CP + ck * 8);
+        *reinterpret_cast<uint4*>(xs + pix * (CP + 8) + ck * 8) = v;
+    }
+}
+
+// ------------------------------------------------------------ forward conv ---
+// out[p, co] = act(b[co] + sum_{tap, ci} W[co][tap][ci] x[p + off(tap), ci]).
+// Warp w computes output rows 2w and 2w+1 of the tile (two m16 tiles of 16
+// pixels) for all COUT channels (COUT/8 n8 tiles); K runs over 9 taps x CIN.
+template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
+__global__ void __launch_bounds__(NTHREADS) conv3x3_fwd(const __nv_bfloat16* __restrict__ x,
+                                                         const __nv_bfloat16* __restrict__ wt,
+                                                         const float* __restrict__ bias, void* out,
+                                                         float* __restrict__ zsave, int h, int w) {
+    constexpr int XP = CIN + 8, WP = 9 * CIN + 8, NT = COUT / 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* ws = xs + HALO * HALO * XP;
+    float* bs = reinterpret_cast<float*>(ws + COUT * WP);
+    const int n = blockIdx.z, y0 = blockIdx.y * TILE, x0 = blockIdx.x * TILE;
+    load_halo<CIN>(xs, x, n, h, w, y0, x0);
+    constexpr int WCH = 9 * CIN / 8;
+    for (int e = threadIdx.x; e < COUT * WCH; e += NTHREADS) {
+        const int co = e / WCH, ck = e % WCH;
+        *reinterpret_cast<uint4*>(ws + co * WP + ck * 8) =
+            *reinterpret_cast<const uint4*>(wt + (long long)co * 9 * CIN + ck * 8);
+    }
+    for (int e = threadIdx.x; e < COUT; e += NTHREADS) bs[e] = bias[e];
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    float acc[2][NT][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
+
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; ++kc) {
+            uint32_t b[NT][2];
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                const __nv_bfloat16* wp = ws + (nt * 8 + g) * WP + tap * CIN + kc * 16 + 2 * t;
+                b[nt][0] = ld32(wp);
+                b[nt][1] = ld32(wp + 8);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                const int row = 2 * warp + mt + ky;
+                const __nv_bfloat16* p0 = xs + (row * HALO + g + kx) * XP + kc * 16 + 2 * t;
+                const __nv_bfloat16* p1 = p0 + 8 * XP;
+                const uint32_t a[4] = {ld32(p0), ld32(p1), ld32(p0 + 8), ld32(p1 + 8)};
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) mma_bf16(acc[mt][nt], a, b[nt]);
+            }
+        }
+    }
+    // epilogue: bias, activation, store (two channels per value pair)
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int py = y0 + 2 * warp + mt;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int px = x0 + g + 8 * half;
+            const long long pix = ((long long)n * h + py) * w + px;
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                const int co = nt * 8 + 2 * t;
+                const float z0 = acc[mt][nt][2 * half] + bs[co];
+                const float z1 = acc[mt][nt][2 * half + 1] + bs[co + 1];
+                if (SAVEZ) *reinterpret_cast<float2*>(zsave + pix * COUT + co) = make_float2(z0, z1);
+                const float y0v = ACT ? gelu(z0) : z0, y1v = ACT ? gelu(z1) : z1;
+                if (OUTF32)
+                    *reinterpret_cast<float2*>(static_cast<float*>(out) + pix * COUT + co) = make_float2(y0v, y1v);
+                else
+                    *reinterpret_cast<uint32_t*>(static_cast<__nv_bfloat16*>(out) + pix * COUT + co) =
+                        pack2(__float2bfloat16_rn(y0v), __float2bfloat16_rn(y1v));
+            }
+        }
+    }
+}
+
+template <int CIN, int COUT>
+constexpr int fwd_smem() {
+    return HALO * HALO * (CIN + 8) * 2 + COUT * (9 * CIN + 8) * 2 + COUT * 4;
+}
+
+// ------------------------------------------------------- weight gradient ---
+// partial[blk][co][tap*CIN + ci] = sum over the tile's pixels p of
+//   dz[p, co] * x[p + off(tap), ci];  pdb[blk][co] = sum_p dz[p, co].
+// GEMM M = COUT (dz transposed in shared memory), N = 9*CIN (im2col of the
+// halo tile), K = the tile's 256 pixels.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(NTHREADS) conv3x3_wgrad(const __nv_bfloat16* __restrict__ x,
+                                                           const __nv_bfloat16* __restrict__ dz,
+                                                           float* __restrict__ partial,
+                                                           float* __restrict__ pdb, int h, int w) {
+    constexpr int XP = CIN + 8, DP = NPIX + 8;
+    constexpr int MT = COUT / 16, NT = 9 * CIN / 8, TILES = MT * NT, TPW = (TILES + 7) / 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* dzt = xs + HALO * HALO * XP;  // [COUT][NPIX + 8]
+    const int n = blockIdx.z, y0 = blockIdx.y * TILE, x0 = blockIdx.x * TILE;
+    const long long blk = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    load_halo<CIN>(xs, x, n, h, w, y0, x0);
+    for (int e = threadIdx.x; e < NPIX * COUT; e += NTHREADS) {
+        const int p = e / COUT, co = e % COUT;
+        const long long pix = ((long long)n * h + y0 + p / TILE) * w + x0 + p % TILE;
+        dzt[co * DP + p] = dz[pix * COUT + co];
+    }
+    __syncthreads();
+    if (threadIdx.x < COUT) {
+        float s = 0.f;
+        for (int p = 0; p < NPIX; ++p) s += __bfloat162float(dzt[threadIdx.x * DP + p]);
+        pdb[blk * COUT + threadIdx.x] = s;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    float acc[TPW][4];
+#pragma unroll
+    for (int i = 0; i < TPW; ++i)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[i][k] = 0.f;
+#pragma unroll 1
+    for (int k0 = 0; k0 < NPIX; k0 += 16) {
+        // pixels k0+2t, k0+2t+1 (b0) and k0+2t+8, +9 (b1): all in tile row k0/16
+        const int prow = k0 / TILE;
+#pragma unroll
+        for (int i = 0; i < TPW; ++i) {
+            const int tile = warp + 8 * i;
+            if (tile >= TILES) break;
+            const int mt = tile / NT, nt = tile % NT;
+            const int co = mt * 16 + g;
+            const __nv_bfloat16* ap = dzt + co * DP + k0 + 2 * t;
+            const uint32_t a[4] = {ld32(ap), ld32(ap + 8 * DP), ld32(ap + 8), ld32(ap + 8 * DP + 8)};
+            const int tap = (nt * 8) / CIN, ci = (nt * 8) % CIN + g;
+            const int ky = tap / 3, kx = tap % 3;
+            const __nv_bfloat16* xr = xs + ((prow + ky) * HALO + kx) * XP + ci;
+            const int c0 = 2 * t;  // tile column of the first pixel of b0
+            uint32_t b[2];
+            b[0] = pack2(xr[(c0)*XP], xr[(c0 + 1) * XP]);
+            b[1] = pack2(xr[(c0 + 8) * XP], xr[(c0 + 9) * XP]);
+            mma_bf16(acc[i], a, b);
+        }
+    }
+    float* out = partial + blk * (long long)(COUT * 9 * CIN);
+#pragma unroll
+    for (int i = 0; i < TPW; ++i) {
+        const int tile = warp + 8 * i;
+        if (tile >= TILES) break;
+        const int mt = tile / NT, nt = tile % NT;
+        const int col = nt * 8 + 2 * t;
+        const int r0 = mt * 16 + g, r1 = r0 + 8;
+        out[r0 * 9 * CIN + col] = acc[i][0];
+        out[r0 * 9 * CIN + col + 1] = acc[i][1];
+        out[r1 * 9 * CIN + col] = acc[i][2];
+        out[r1 * 9 * CIN + col + 1] = acc[i][3];
+    }
+}
+
+template <int CIN, int COUT>
+constexpr int wgrad_smem() {
+    return HALO * HALO * (CIN + 8) * 2 + COUT * (NPIX + 8) * 2;
+}
+
+// sum over tiles: dst[j] = sum_b src[b][j]
+__global__ void reduce_tiles(const float* __restrict__ src, float* __restrict__ dst, long long nblk,
+                             int len) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < len; j += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (long long b = 0; b < nblk; ++b) s += src[b * len + j];
+        dst[j] = s;
+    }
+}
+
+// Wt[ci][tap][co] = W[co][8 - tap][ci]: the data gradient's weights
+__global__ void flip_weights(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ wt,
+                             int cout, int cin) {
+    const int n = cout * 9 * cin;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int ci = e / (9 * cout), rest = e % (9 * cout), tap = rest / cout, co = rest % cout;
+        wt[e] = w[((long long)co * 9 + (8 - tap)) * cin + ci];
+    }
+}
+
+__global__ void gelu_backward(const __nv_bfloat16* __restrict__ dy, const float* __restrict__ z,
+                              __nv_bfloat16* __restrict__ dz, long long n) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x)
+        dz[e] = __float2bfloat16_rn(__bfloat162float(dy[e]) * gelu_grad(z[e]));
+}
+
+// MSE over the first nc of cp channels: dy = 2 (pred - target) / count,
+// loss accumulated in FP64 (one atomic per block)
+__global__ void mse_grad(const float* __restrict__ pred, const float* __restrict__ target,
+                         __nv_bfloat16* __restrict__ dy, double* __restrict__ loss, long long npix,
+                         int cp, int nc, float inv_count) {
+    __shared__ double red[NTHREADS / 32];
+    double acc = 0.0;
+    const long long n = npix * cp;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e / cp;
+        const int c = (int)(e % cp);
+        float g = 0.f;
+        const float tg = c < nc ? target[p * nc + c] : 0.f;
+        if (c < nc && tg == tg) {  // a NaN target masks the pixel out
+            const float d = pred[e] - tg;
+            acc += (double)d * (double)d;
+            g = 2.f * d * inv_count;
+        }
+        dy[e] = __float2bfloat16_rn(g);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < NTHREADS / 32; ++k) s += red[k];
+        atomicAdd(loss, s);
+    }
+}
+
+__global__ void adam_step(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, __nv_bfloat16* __restrict__ w16, long long n,
+                          float lr, float b1, float b2, float eps, float c1, float c2) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const float ge = g[e];
+        const float me = b1 * m[e] + (1.f - b1) * ge;
+        const float ve = b2 * v[e] + (1.f - b2) * ge * ge;
+        m[e] = me;
+        v[e] = ve;
+        const float wn = w[e] - lr * (me / c1) / (sqrtf(ve / c2) + eps);
+        w[e] = wn;
+        if (w16) w16[e] = __float2bfloat16_rn(wn);
+    }
+}
+
+// ---------------------------------------------------------- solver glue ---
+// coarse[m][j][i] = mean of the r x r fine block (FP64 SoA, row pitches ldf/ldc)
+__global__ void block_average(const double* __restrict__ fine, long long ldf, long long fsf,
+                              double* __restrict__ coarse, long long ldc, long long fsc, int mxc,
+                              int myc, int r, int meqn) {
+    const long long n = (long long)meqn * mxc * myc;
+    const double inv = 1.0 / (double)(r * r);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(e / ((long long)mxc * myc));
+        const long long rest = e % ((long long)mxc * myc);
+        const int j = (int)(rest / mxc), i = (int)(rest % mxc);
+        double s = 0.0;
+        for (int b = 0; b < r; ++b)
+            for (int a = 0; a < r; ++a)
+                s += fine[m * fsf + (long long)(j * r + b) * ldf + (i * r + a)];
+        coarse[m * fsc + (long long)j * ldc + i] = s * inv;
+    }
+}
+
+// features x[p][c] (BF16, 16 channels): c < 4 the normalised state
+// (q - mu_c) / s_c, 4 <= c < 8 the plain step's increment (qs - q) / d_c,
+// the rest zero.
+__global__ void features(const double* __restrict__ q, const double* __restrict__ qs, long long ld,
+                         long long fs, int mx, int my, int img, const float* __restrict__ norm,
+                         __nv_bfloat16* __restrict__ x) {
+    const long long n = (long long)mx * my;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(p / mx), i = (int)(p % mx);
+        __nv_bfloat16 v[8];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double a = q[c * fs + (long long)j * ld + i], b = qs[c * fs + (long long)j * ld + i];
+            v[c] = __float2bfloat16_rn((float)((a - (double)norm[c]) * (double)norm[4 + c]));
+            v[4 + c] = __float2bfloat16_rn((float)((b - a) * (double)norm[8 + c]));
+        }
+        uint4* dst = reinterpret_cast<uint4*>(x + ((long long)img * n + p) * 16);
+        dst[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+        dst[1] = make_uint4(0, 0, 0, 0);
+    }
+}
+
+// target[p][c] = (qf - qs) * norm[12 + c]: the residual the corrector learns
+__global__ void residual_target(const double* __restrict__ qf, const double* __restrict__ qs,
+                                long long ld, long long fs, int mx, int my, int img,
+                                const float* __restrict__ norm, float* __restrict__ target) {
+    const long long n = (long long)mx * my;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(p / mx), i = (int)(p % mx);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const long long o = c * fs + (long long)j * ld + i;
+            target[((long long)img * n + p) * 4 + c] = (float)((qf[o] - qs[o]) * (double)norm[12 + c]);
+        }
+    }
+}
+
+// Apply the corrector to one grid, one CTA per 16x16 tile: the residual of
+// each field (r[p][c] / norm[12+c]) minus its tile mean (so the tile's
+// conserved totals are unchanged), added to the plain step qs; a tile whose
+// corrected density or pressure is not positive, or whose totals moved by
+// more than tol relative, keeps the plain step.  flags[tile] = 1 if
+// corrected, 0 if it fell back.
+__global__ void __launch_bounds__(NTHREADS) apply_correction(double* __restrict__ qs, long long ld,
+                                                             long long fs, int mx, int my,
+                                                             const float* __restrict__ r, int rcp,
+                                                             const float* __restrict__ norm,
+                                                             double gamma, double tol,
+                                                             int* __restrict__ flags) {
+    __shared__ double red[4][NTHREADS / 32];
+    __shared__ double mean[4], tot[4];
+    __shared__ int bad;
+    const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
+    const int i = blockIdx.x * TILE + tx, j = blockIdx.y * TILE + ty;
+    const bool in = i < mx && j < my;
+    const long long p = (long long)j * mx + i;
+    double d[4], q0[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        d[c] = in ? (double)r[p * rcp + c] / (double)norm[12 + c] : 0.0;
+        q0[c] = in ? qs[c * fs + (long long)j * ld + i] : 0.0;
+    }
+    const int cnt = min(TILE, mx - blockIdx.x * TILE) * min(TILE, my - blockIdx.y * TILE);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto block_sum = [&](double v[4], double out[4]) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            double s = v[c];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) red[c][warp] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            double s = 0.0;
+            for (int k = 0; k < NTHREADS / 32; ++k) s += red[threadIdx.x][k];
+            out[threadIdx.x] = s;
+        }
+        __syncthreads();
+    };
+    block_sum(d, mean);
+    double qn[4], aq[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const double dc = in ? d[c] - mean[c] / (double)cnt : 0.0;
+        qn[c] = q0[c] + dc;
+        aq[c] = in ? fabs(q0[c]) : 0.0;
+    }
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    if (in) {
+        const double ke = 0.5 * (qn[1] * qn[1] + qn[2] * qn[2]) / qn[0];
+        const double pr = (gamma - 1.0) * (qn[3] - ke);
+        if (!(qn[0] > 0.0) || !(pr > 0.0)) atomicOr(&bad, 1);
+    }
+    // conserved totals of the tile before and after
+    double diff[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) diff[c] = in ? qn[c] - q0[c] : 0.0;
+    block_sum(diff, tot);
+    double scale[4];
+    block_sum(aq, scale);
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 4; ++c)
+            if (fabs(tot[c]) > tol * (scale[c] > 0.0 ? scale[c] : 1.0)) bad = 1;
+    }
+    __syncthreads();
+    if (in && !bad)
+        for (int c = 0; c < 4; ++c) qs[c * fs + (long long)j * ld + i] = qn[c];
+    if (threadIdx.x == 0) flags[blockIdx.y * gridDim.x + blockIdx.x] = bad ? 0 : 1;
+}
+
+int grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    return (int)(b < 592 ? (b > 0 ? b : 1) : 592);
+}
+
+template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
+int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, int n, int h,
+               int wd, cudaStream_t s) {
+    constexpr int SM = fwd_smem<CIN, COUT>();
+    auto k = conv3x3_fwd<CIN, COUT, ACT, OUTF32, SAVEZ>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess)
+        return NN_E_CUDA;
+    k<<<dim3(wd / TILE, h / TILE, n), NTHREADS, SM, s>>>(
+        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), b, y, z, h, wd);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+template <int CIN, int COUT>
+int launch_wgrad(const void* x, const void* dz, float* partial, float* pdb, int n, int h, int wd,
+                 cudaStream_t s) {
+    constexpr int SM = wgrad_smem<CIN, COUT>();
+    auto k = conv3x3_wgrad<CIN, COUT>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess)
+        return NN_E_CUDA;
+    k<<<dim3(wd / TILE, h / TILE, n), NTHREADS, SM, s>>>(static_cast<const __nv_bfloat16*>(x),
+                                                          static_cast<const __nv_bfloat16*>(dz),
+                                                          partial, pdb, h, wd);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+bool shape_ok(int n, int h, int w) { return n > 0 && h > 0 && w > 0 && h % TILE == 0 && w % TILE == 0; }
+
+}  // namespace
+
+extern "C" {
+
+int nn_conv3x3_forward(const void* x, const void* w, const float* b, void* y, float* z, int n,
+                       int h, int wd, int cin, int cout, int act, int out_f32, void* stream) {
+    if (!x || !w || !b || !y || !shape_ok(n, h, wd)) return NN_E_INVALID;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool save = z != nullptr;
+    if (cin == 16 && cout == 32 && act == 1 && !out_f32)
+        return save ? launch_fwd<16, 32, 1, false, true>(x, w, b, y, z, n, h, wd, s)
+                    : launch_fwd<16, 32, 1, false, false>(x, w, b, y, z, n, h, wd, s);
+    if (cin == 32 && cout == 32 && act == 1 && !out_f32)
+        return save ? launch_fwd<32, 32, 1, false, true>(x, w, b, y, z, n, h, wd, s)
+                    : launch_fwd<32, 32, 1, false, false>(x, w, b, y, z, n, h, wd, s);
+    if (cin == 32 && cout == 16 && act == 0 && out_f32 && !save)
+        return launch_fwd<32, 16, 0, true, false>(x, w, b, y, z, n, h, wd, s);
+    // data gradients: no activation, BF16 out
+    if (cin == 32 && cout == 32 && act == 0 && !out_f32 && !save)
+        return launch_fwd<32, 32, 0, false, false>(x, w, b, y, z, n, h, wd, s);
+    if (cin == 16 && cout == 32 && act == 0 && !out_f32 && !save)
+        return launch_fwd<16, 32, 0, false, false>(x, w, b, y, z, n, h, wd, s);
+    return NN_E_UNSUPPORTED;
+}
+
+int nn_conv3x3_wgrad(const void* x, const void* dz, float* partial, float* pdb, float* dw,
+                     float* db, int n, int h, int wd, int cin, int cout, void* stream) {
+    if (!x || !dz || !partial || !pdb || !dw || !db || !shape_ok(n, h, wd)) return NN_E_INVALID;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc;
+    if (cin == 16 && cout == 32) rc = launch_wgrad<16, 32>(x, dz, partial, pdb, n, h, wd, s);
+    else if (cin == 32 && cout == 32) rc = launch_wgrad<32, 32>(x, dz, partial, pdb, n, h, wd, s);
+    else if (cin == 32 && cout == 16) rc = launch_wgrad<32, 16>(x, dz, partial, pdb, n, h, wd, s);
+    else return NN_E_UNSUPPORTED;
+    if (rc) return rc;
+    const long long nblk = (long long)n * (h / TILE) * (wd / TILE);
+    const int len = cout * 9 * cin;
+    reduce_tiles<<<(len + 255) / 256, 256, 0, s>>>(partial, dw, nblk, len);
+    reduce_tiles<<<1, 256, 0, s>>>(pdb, db, nblk, cout);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_flip_weights(const void* w, void* wt, int cout, int cin, void* stream) {
+    if (!w || !wt || cout <= 0 || cin <= 0) return NN_E_INVALID;
+    const int n = cout * 9 * cin;
+    flip_weights<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(w), static_cast<__nv_bfloat16*>(wt), cout, cin);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_gelu_backward(const void* dy, const float* z, void* dz, long long n, void* stream) {
+    if (!dy || !z || !dz || n < 0) return NN_E_INVALID;
+    gelu_backward<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(dy), z, static_cast<__nv_bfloat16*>(dz), n);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_mse_grad(const float* pred, const float* target, void* dy, double* loss, long long npix,
+                int cp, int nc, void* stream) {
+    if (!pred || !target || !dy || !loss || npix <= 0 || nc > cp) return NN_E_INVALID;
+    const float inv = 1.0f / (float)(npix * nc);
+    mse_grad<<<grid_for(npix * cp), NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+        pred, target, static_cast<__nv_bfloat16*>(dy), loss, npix, cp, nc, inv);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_adam(float* w, const float* g, float* m, float* v, void* w16, long long n, float lr,
+            float b1, float b2, float eps, int step, void* stream) {
+    if (!w || !g || !m || !v || n < 0 || step < 1) return NN_E_INVALID;
+    float c1 = 1.f, c2 = 1.f;
+    for (int k = 0; k < step && k < 100000; ++k) { c1 *= b1; c2 *= b2; }
+    adam_step<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        w, g, m, v, static_cast<__nv_bfloat16*>(w16), n, lr, b1, b2, eps, 1.f - c1, 1.f - c2);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_block_average(const double* fine, long long ldf, long long fsf, double* coarse, long long ldc,
+                     long long fsc, int mxc, int myc, int r, int meqn, void* stream) {
+    if (!fine || !coarse || r < 1 || mxc < 1 || myc < 1) return NN_E_INVALID;
+    block_average<<<grid_for((long long)meqn * mxc * myc), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        fine, ldf, fsf, coarse, ldc, fsc, mxc, myc, r, meqn);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_features(const double* q, const double* qs, long long ld, long long fs, int mx, int my,
+                int img, const float* norm, void* x, void* stream) {
+    if (!q || !qs || !norm || !x) return NN_E_INVALID;
+    features<<<grid_for((long long)mx * my), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        q, qs, ld, fs, mx, my, img, norm, static_cast<__nv_bfloat16*>(x));
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_residual_target(const double* qf, const double* qs, long long ld, long long fs, int mx,
+                       int my, int img, const float* norm, float* target, void* stream) {
+    if (!qf || !qs || !norm || !target) return NN_E_INVALID;
+    residual_target<<<grid_for((long long)mx * my), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        qf, qs, ld, fs, mx, my, img, norm, target);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_apply_correction(double* qs, long long ld, long long fs, int mx, int my, const float* r,
+                        int rcp, const float* norm, double gamma, double tol, int* flags,
+                        void* stream) {
+    if (!qs || !r || !norm || !flags || rcp < 4) return NN_E_INVALID;
+    const dim3 grid((mx + TILE - 1) / TILE, (my + TILE - 1) / TILE);
+    apply_correction<<<grid, NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+        qs, ld, fs, mx, my, r, rcp, norm, gamma, tol, flags);
+    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+}  // extern "C"

@@ -607,8 +607,8 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
             qm_t[m] = qm_n[m];
             qc_t[m] = qc_n[m];
         }
-#pragma unroll
         cy = cyn;
+#pragma unroll
         for (int mw = 0; mw < MW; ++mw) {
             dotl_y[mw] = dotr_y[mw];
             sy[mw] = sn[mw];

