@@ -21,6 +21,8 @@ def _lib():
 
 
 def _p(t):
+    """Device pointer of a tensor; the caller keeps the tensor alive (a
+    temporary's memory would be reused by the next allocation)."""
     return ctypes.c_void_p(t.data_ptr())
 
 
@@ -48,7 +50,8 @@ def test_forward_matches_oracle(cin, cout, act, outf):
     y = torch.empty((n, h, w, cout), dtype=torch.float32 if outf else torch.bfloat16, device="cuda")
     z = torch.empty((n, h, w, cout), dtype=torch.float32, device="cuda") if act else None
     lib = _lib()
-    rc = lib.nn_conv3x3_forward(_p(_bf(x)), _p(_bf(wt)), _p(_f32(b)), _p(y),
+    xd, wd, bd = _bf(x), _bf(wt), _f32(b)  # keep the buffers alive across the launch
+    rc = lib.nn_conv3x3_forward(_p(xd), _p(wd), _p(bd), _p(y),
                                 _p(z) if z is not None else None, n, h, w, cin, cout, act, outf, None)
     assert rc == 0
     torch.cuda.synchronize()
@@ -73,7 +76,8 @@ def test_weight_gradient_matches_oracle(cin, cout):
     pdb = torch.empty(nblk * cout, device="cuda")
     dw = torch.empty((cout, 9, cin), device="cuda")
     db = torch.empty(cout, device="cuda")
-    rc = _lib().nn_conv3x3_wgrad(_p(_bf(x)), _p(_bf(dz)), _p(partial), _p(pdb), _p(dw), _p(db), n,
+    xd, dzd = _bf(x), _bf(dz)
+    rc = _lib().nn_conv3x3_wgrad(_p(xd), _p(dzd), _p(partial), _p(pdb), _p(dw), _p(db), n,
                                  h, w, cin, cout, None)
     assert rc == 0
     torch.cuda.synchronize()
@@ -89,10 +93,11 @@ def test_data_gradient_is_flipped_convolution():
     wt = O.bf16(rng.standard_normal((cout, 9, cin)) * 0.2)
     lib = _lib()
     wflip = torch.empty((cin, 9, cout), dtype=torch.bfloat16, device="cuda")
-    assert lib.nn_flip_weights(_p(_bf(wt)), _p(wflip), cout, cin, None) == 0
+    wd, dzd = _bf(wt), _bf(dz)
+    assert lib.nn_flip_weights(_p(wd), _p(wflip), cout, cin, None) == 0
     dx = torch.empty((n, h, w, cin), dtype=torch.bfloat16, device="cuda")
     zero = torch.zeros(cin, device="cuda")
-    assert lib.nn_conv3x3_forward(_p(_bf(dz)), _p(wflip), _p(zero), _p(dx), None, n, h, w, cout,
+    assert lib.nn_conv3x3_forward(_p(dzd), _p(wflip), _p(zero), _p(dx), None, n, h, w, cout,
                                   cin, 0, 0, None) == 0
     torch.cuda.synchronize()
     ref = O.conv3x3(dz, O.flip(wt))
@@ -117,8 +122,9 @@ def test_network_backward_matches_oracle():
         if k == len(LAYERS) - 1:
             net.w32[k][:4] *= 30.0
             net.w16[k].copy_(net.w32[k].to(torch.bfloat16))
-    pred = net.forward(_bf(x), train=True)
-    dy, loss = net.loss_grad(pred, _f32(target))
+    xd, td = _bf(x), _f32(target)
+    pred = net.forward(xd, train=True)
+    dy, loss = net.loss_grad(pred, td)
     net.backward(dy)
     torch.cuda.synchronize()
     layers = [(net.w16[k].float().cpu().numpy().astype(np.float64), net.b[k].cpu().numpy(),
@@ -173,7 +179,8 @@ def test_apply_correction_conserves_and_falls_back():
     norm = np.ones(16, dtype=np.float32)
     qd = torch.as_tensor(q).cuda().contiguous()
     flags = torch.zeros(4, dtype=torch.int32, device="cuda")
-    rc = lib.nn_apply_correction(_p(qd), n, n * n, n, n, _p(_f32(r)), 16, _p(_f32(norm)), 1.4, 1e-10,
+    rd, nd = _f32(r), _f32(norm)
+    rc = lib.nn_apply_correction(_p(qd), n, n * n, n, n, _p(rd), 16, _p(nd), 1.4, 1e-10,
                                  _p(flags), None)
     assert rc == 0
     out = qd.cpu().numpy()
@@ -201,7 +208,8 @@ def test_glue_block_average_and_features():
     qs = cd + 0.01
     norm = np.arange(16, dtype=np.float32) * 0.1 + 0.5
     x = torch.empty((1, n, n, 16), dtype=torch.bfloat16, device="cuda")
-    assert lib.nn_features(_p(cd), _p(qs), n, n * n, n, n, 0, _p(_f32(norm)), _p(x), None) == 0
+    nd = _f32(norm)
+    assert lib.nn_features(_p(cd), _p(qs), n, n * n, n, n, 0, _p(nd), _p(x), None) == 0
     xs = x.float().cpu().numpy()[0]
     q = cd.cpu().numpy()
     for c in range(4):
