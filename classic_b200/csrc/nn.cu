@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(NTHREADS) apply_correction(double* __restrict_
                                                              double gamma, double tol,
                                                              int* __restrict__ flags) {
     __shared__ double red[4][NTHREADS / 32];
-    __shared__ double mean[4], tot[4];
+    __shared__ double mean[4], tot[4], scale[4];
     __shared__ int bad;
     const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
     const int i = blockIdx.x * TILE + tx, j = blockIdx.y * TILE + ty;
@@ -426,7 +426,6 @@ __global__ void __launch_bounds__(NTHREADS) apply_correction(double* __restrict_
 #pragma unroll
     for (int c = 0; c < 4; ++c) diff[c] = in ? qn[c] - q0[c] : 0.0;
     block_sum(diff, tot);
-    double scale[4];
     block_sum(aq, scale);
     if (threadIdx.x == 0) {
         for (int c = 0; c < 4; ++c)
