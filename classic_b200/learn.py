@@ -1,0 +1,154 @@
+"""Train and evaluate the learned coarse-grid corrector on the seeded 2D
+Euler four-quadrant family.
+
+    python -m classic_b200.learn --train 256 --heldout 16 --truth 4 \\
+        --iters 3000 --out results.json
+
+1. Pairs: for every training seed, coarse (n^2) / fine ((4n)^2) runs to
+   t_final with the coarse Courant-number dt; K coarse steps per seed are
+   kept (features and residual targets, on the device).
+2. Scaling: the feature and target scales are recalibrated on the pairs.
+3. Training: Adam on random 64x64 crops with this library's BF16 kernels.
+4. Evaluation on held-out seeds: plain coarse, corrected coarse and plain
+   fine FP64 runs to t_final; L1 errors against the block-averaged fine run
+   for every held-out seed, and against a (8n)^2 plain run for the first
+   --truth seeds; device times of the plain fine run and the corrected
+   coarse run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import corrector as C
+
+
+def _log(*a):
+    print(*a, flush=True)
+
+
+def generate(seeds, norm, n, keep, rng):
+    torch = C._torch()
+    total = len(seeds) * keep
+    x = torch.empty((total, n, n, 16), dtype=torch.bfloat16, device="cuda")
+    t = torch.empty((total, n, n, 4), dtype=torch.float32, device="cuda")
+    gen = C.PairGenerator(n=n)
+    used = 0
+    steps_all = []
+    for seed in seeds:
+        # the steps kept: spread over the run (about n steps to t_final at 256^2)
+        est = int(0.9 * n)
+        kept = sorted(rng.choice(np.arange(2, est), size=keep, replace=False).tolist())
+        steps, k = gen.run(seed, norm, kept, x, t, used)
+        if k and not (torch.isfinite(x[used:used + k].float()).all() and
+                      torch.isfinite(t[used:used + k]).all()):
+            k = 0  # a run that left the physical states: drop its pairs
+        used += k
+        steps_all.append(steps)
+    return x[:used], t[:used], steps_all
+
+
+def recalibrate(x, t, norm):
+    """Rescale features / targets to unit standard deviation per channel and
+    fold the factors into the normalisation used at inference."""
+    torch = C._torch()
+    v = norm.values.copy()
+    for c in range(8):
+        s = float(x[..., c].float().std())
+        if s > 0:
+            x[..., c] = (x[..., c].float() / s).to(torch.bfloat16)
+            v[4 + c] /= s  # channels 0..3 scale q, 4..7 the increments
+    for c in range(4):
+        s = float(t[..., c].std())
+        if s > 0:
+            t[..., c] /= s
+            v[12 + c] /= s
+    return C.Norm(v)
+
+
+def evaluate(net, norm, seeds, n, truth_count):
+    out = []
+    for k, seed in enumerate(seeds):
+        qc, sc, tc = C.plain_run(seed, n)
+        qk, sk, frac, tk = C.corrected_run(net, norm, seed, n=n)
+        qf, sf, tf = C.plain_run(seed, 4 * n)
+        ref = C.block_average(qf, 4)
+        row = dict(seed=seed, coarse_steps=sc, fine_steps=sf, corrected_steps=sk,
+                   corrected_tile_fraction=frac, fine_seconds=tf, corrected_seconds=tk,
+                   coarse_seconds=tc, finite=bool(np.isfinite(qk).all() and np.isfinite(qf).all()),
+                   err_vs_fine_plain=C.l1_error(qc, ref), err_vs_fine_corrected=C.l1_error(qk, ref))
+        if k < truth_count:
+            qt, st, tt = C.plain_run(seed, 8 * n)
+            truth = C.block_average(qt, 8)
+            row.update(err_truth_plain=C.l1_error(qc, truth), err_truth_corrected=C.l1_error(qk, truth),
+                       err_truth_fine=C.l1_error(C.block_average(qf, 4), truth), truth_steps=st)
+        out.append(row)
+        _log(json.dumps(row))
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--train", type=int, default=256)
+    ap.add_argument("--heldout", type=int, default=16)
+    ap.add_argument("--truth", type=int, default=4)
+    ap.add_argument("--keep", type=int, default=16, help="coarse steps kept per training seed")
+    ap.add_argument("--iters", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args(argv)
+    torch = C._torch()
+    rng = np.random.default_rng(args.seed)
+    train_seeds = list(range(10000, 10000 + args.train))
+    held_seeds = list(range(20000, 20000 + args.heldout))
+    t0 = time.perf_counter()
+    x, t, steps = generate(train_seeds, C.default_norm(), args.n, args.keep, rng)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    _log(f"pairs: {x.shape[0]} from {len(train_seeds)} seeds in {t_gen:.1f} s "
+         f"(coarse steps per run {min(steps)}..{max(steps)})")
+    norm = recalibrate(x, t, C.default_norm())
+    net = C.ConvNet(seed=args.seed)
+    t0 = time.perf_counter()
+    losses = C.train(net, x, t, iters=args.iters, batch=args.batch, lr=args.lr, seed=args.seed,
+                     log=lambda it, l: _log(f"iter {it} loss {l:.4e}"))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del x, t
+    rows = evaluate(net, norm, held_seeds, args.n, args.truth)
+    good = [r for r in rows if r["finite"]]
+    summary = dict(
+        pairs_seconds=t_gen, train_seconds=t_train, iters=args.iters, batch=args.batch,
+        train_seeds=len(train_seeds), heldout_seeds=len(held_seeds), loss_first=losses[0][1],
+        loss_last=losses[-1][1],
+        mean_err_vs_fine_plain=float(np.mean([r["err_vs_fine_plain"] for r in good])),
+        mean_err_vs_fine_corrected=float(np.mean([r["err_vs_fine_corrected"] for r in good])),
+        speedup_fine_over_corrected=float(np.mean([r["fine_seconds"] / r["corrected_seconds"]
+                                                  for r in good])))
+    tr = [r for r in good if "err_truth_fine" in r]
+    if tr:
+        summary.update(
+            mean_err_truth_plain=float(np.mean([r["err_truth_plain"] for r in tr])),
+            mean_err_truth_corrected=float(np.mean([r["err_truth_corrected"] for r in tr])),
+            mean_err_truth_fine=float(np.mean([r["err_truth_fine"] for r in tr])))
+        summary["corrected_over_fine_error"] = (summary["mean_err_truth_corrected"] /
+                                                summary["mean_err_truth_fine"])
+    _log(json.dumps(summary))
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(dict(summary=summary, rows=rows, losses=losses, norm=norm.values.tolist(),
+                           args=vars(args)), f, indent=1)
+        np.savez(args.out.replace(".json", "_weights.npz"),
+                 **{f"w{k}": w for k, w in enumerate(net.state()["w"])},
+                 **{f"b{k}": b for k, b in enumerate(net.state()["b"])})
+    return summary
+
+
+if __name__ == "__main__":
+    main()
