@@ -322,7 +322,8 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
         pred = net.forward(xb, train=True)
         dy, loss = net.loss_grad(pred, tb)
         net.backward(dy)
-        net.adam(lr=lr)
+        # cosine decay of the step size to 1% over the run
+        net.adam(lr=lr * (0.01 + 0.99 * 0.5 * (1.0 + math.cos(math.pi * it / max(iters - 1, 1)))))
         if log is not None and (it % 100 == 0 or it == iters - 1):
             valid = (~mask).sum().item() * OUT_REAL
             losses.append((it, loss.item() / max(valid, 1)))
