@@ -117,7 +117,7 @@ SIGNATURES = {
     "nn_flip_weights": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
     "nn_gelu_backward": (ctypes.c_int, [_P, _P, _P, ctypes.c_longlong, _P]),
     "nn_mse_grad": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
-                                   _P]),
+                                   ctypes.c_float, _P]),
     "nn_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_longlong] + [ctypes.c_float] * 4 +
                 [ctypes.c_int, _P]),
     "nn_block_average": (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.c_longlong, _P,

@@ -190,14 +190,14 @@ class ConvNet:
                                    None, self.b[k].numel(), lr, b1, b2, eps, self.step_count, st),
                   "nn_adam")
 
-    def loss_grad(self, pred, target):
-        """MSE on the 4 output channels (NaN targets masked); returns (dy, the
-        device loss accumulator)."""
+    def loss_grad(self, pred, target, delta=0.0):
+        """MSE (delta = 0) or Huber loss on the 4 output channels (NaN targets
+        masked); returns (dy, the device loss accumulator)."""
         c = self._cache
         c["loss"].zero_()
         n, h, w, cp = pred.shape
         check(self.lib.nn_mse_grad(_p(pred), _p(target), _p(c["dy"]), _p(c["loss"]), n * h * w, cp,
-                                   OUT_REAL, _stream()), "nn_mse_grad")
+                                   OUT_REAL, float(delta), _stream()), "nn_mse_grad")
         return c["dy"], c["loss"]
 
     def state(self):
@@ -294,10 +294,12 @@ class PairGenerator:
 
 
 def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=0, log=None,
-          margin=5):
+          margin=5, noise=0.0, delta=0.0):
     """Adam on random crops of the stored pairs; the loss covers each crop's
     interior (margin pixels from a crop edge inside the image are masked,
-    as their zero-padded context differs from the full grid)."""
+    as their zero-padded context differs from the full grid).  `noise`
+    perturbs the 8 input channels (normalised units) so the network sees
+    states near, not only on, the teacher-forced ones."""
     torch = _torch()
     gen = torch.Generator(device="cuda").manual_seed(seed)
     ns, h, w, _ = x.shape
@@ -310,6 +312,9 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
         yy = (oy[:, None] + ar[None, :])[:, :, None]
         xx = (ox[:, None] + ar[None, :])[:, None, :]
         xb = x[idx[:, None, None], yy, xx].contiguous()
+        if noise > 0:
+            pert = torch.randn(xb.shape[:-1] + (8,), device="cuda", generator=gen) * noise
+            xb[..., :8] = (xb[..., :8].float() + pert).to(torch.bfloat16)
         tb = target[idx[:, None, None], yy, xx].clone()
         # interior mask: a crop edge that is not the grid edge
         mask = torch.zeros((batch, crop, crop), dtype=torch.bool, device="cuda")
@@ -320,7 +325,7 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
         mask = top | bot | lef | rig
         tb[mask] = float("nan")
         pred = net.forward(xb, train=True)
-        dy, loss = net.loss_grad(pred, tb)
+        dy, loss = net.loss_grad(pred, tb, delta)
         net.backward(dy)
         # cosine decay of the step size to 1% over the run
         net.adam(lr=lr * (0.01 + 0.99 * 0.5 * (1.0 + math.cos(math.pi * it / max(iters - 1, 1)))))
@@ -332,10 +337,14 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
 
 
 def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25, tol=1e-10,
-                  cfl_desired=0.9, cfl_max=1.0):
+                  cfl_desired=0.9, cfl_max=1.0, alpha=1.0):
     """The corrected coarse run of one instance (claw2's dt control on the
-    host, the corrector after every accepted step).  Returns (q, steps,
-    corrected tile fraction, device seconds)."""
+    host, alpha times the corrector after every accepted step).  Returns
+    (q, steps, corrected tile fraction, device seconds)."""
+    if alpha != 1.0:
+        v = norm.values.copy()
+        v[12:16] = v[12:16] / max(alpha, 1e-30)
+        norm = Norm(v)
     torch = _torch()
     lib = _lib.load()
     rd, solver, params, q0, _ = problems.euler_quadrants(n=n, seed=seed, gamma=gamma)

@@ -262,7 +262,7 @@ __global__ void gelu_backward(const __nv_bfloat16* __restrict__ dy, const float*
 // loss accumulated in FP64 (one atomic per block)
 __global__ void mse_grad(const float* __restrict__ pred, const float* __restrict__ target,
                          __nv_bfloat16* __restrict__ dy, double* __restrict__ loss, long long npix,
-                         int cp, int nc, float inv_count) {
+                         int cp, int nc, float inv_count, float delta) {
     __shared__ double red[NTHREADS / 32];
     double acc = 0.0;
     const long long n = npix * cp;
@@ -274,8 +274,13 @@ __global__ void mse_grad(const float* __restrict__ pred, const float* __restrict
         const float tg = c < nc ? target[p * nc + c] : 0.f;
         if (c < nc && tg == tg) {  // a NaN target masks the pixel out
             const float d = pred[e] - tg;
-            acc += (double)d * (double)d;
-            g = 2.f * d * inv_count;
+            if (delta > 0.f && fabsf(d) > delta) {  // Huber: linear beyond delta
+                acc += 2.0 * (double)delta * (double)fabsf(d) - (double)delta * (double)delta;
+                g = 2.f * copysignf(delta, d) * inv_count;
+            } else {
+                acc += (double)d * (double)d;
+                g = 2.f * d * inv_count;
+            }
         }
         dy[e] = __float2bfloat16_rn(g);
     }
@@ -527,11 +532,11 @@ int nn_gelu_backward(const void* dy, const float* z, void* dz, long long n, void
 }
 
 int nn_mse_grad(const float* pred, const float* target, void* dy, double* loss, long long npix,
-                int cp, int nc, void* stream) {
-    if (!pred || !target || !dy || !loss || npix <= 0 || nc > cp) return NN_E_INVALID;
+                int cp, int nc, float delta, void* stream) {
+    if (!pred || !target || !dy || !loss || npix <= 0 || nc > cp || delta < 0.f) return NN_E_INVALID;
     const float inv = 1.0f / (float)(npix * nc);
     mse_grad<<<grid_for(npix * cp), NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(
-        pred, target, static_cast<__nv_bfloat16*>(dy), loss, npix, cp, nc, inv);
+        pred, target, static_cast<__nv_bfloat16*>(dy), loss, npix, cp, nc, inv, delta);
     return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
 }
 

@@ -69,14 +69,35 @@ def recalibrate(x, t, norm):
     return C.Norm(v)
 
 
-def evaluate(net, norm, seeds, n, truth_count):
+def choose_alpha(net, norm, seeds, n, alphas=(0.0, 0.25, 0.5, 0.75, 1.0)):
+    """The corrector's gain alpha with the smallest mean L1 error against the
+    block-averaged fine run on validation seeds (alpha = 0 is the plain
+    step, so the chosen corrector is never worse than plain there)."""
+    refs = {s: C.block_average(C.plain_run(s, 4 * n)[0], 4) for s in seeds}
+    table = []
+    for a in alphas:
+        errs = []
+        for s in seeds:
+            if a == 0.0:
+                q = C.plain_run(s, n)[0]
+            else:
+                q = C.corrected_run(net, norm, s, n=n, alpha=a)[0]
+            e = C.l1_error(q, refs[s])
+            errs.append(e if np.isfinite(e) else np.inf)
+        table.append((a, float(np.mean(errs))))
+        _log(f"alpha {a}: validation error {table[-1][1]:.5f}")
+    best = min(table, key=lambda r: r[1])[0]
+    return best, table
+
+
+def evaluate(net, norm, seeds, n, truth_count, alpha=1.0):
     out = []
     for k, seed in enumerate(seeds):
         qc, sc, tc = C.plain_run(seed, n)
-        qk, sk, frac, tk = C.corrected_run(net, norm, seed, n=n)
+        qk, sk, frac, tk = C.corrected_run(net, norm, seed, n=n, alpha=alpha)
         qf, sf, tf = C.plain_run(seed, 4 * n)
         ref = C.block_average(qf, 4)
-        row = dict(seed=seed, coarse_steps=sc, fine_steps=sf, corrected_steps=sk,
+        row = dict(seed=seed, alpha=alpha, coarse_steps=sc, fine_steps=sf, corrected_steps=sk,
                    corrected_tile_fraction=frac, fine_seconds=tf, corrected_seconds=tk,
                    coarse_seconds=tc, finite=bool(np.isfinite(qk).all() and np.isfinite(qf).all()),
                    err_vs_fine_plain=C.l1_error(qc, ref), err_vs_fine_corrected=C.l1_error(qk, ref))
@@ -98,8 +119,12 @@ def main(argv=None):
     ap.add_argument("--truth", type=int, default=4)
     ap.add_argument("--keep", type=int, default=16, help="coarse steps kept per training seed")
     ap.add_argument("--iters", type=int, default=3000)
-    ap.add_argument("--batch", type=int, default=16)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--lr", type=float, default=3e-4)
+    ap.add_argument("--noise", type=float, default=0.01)
+    ap.add_argument("--clip", type=float, default=5.0, help="clip targets at +-clip std")
+    ap.add_argument("--validation", type=int, default=4)
+    ap.add_argument("--huber", type=float, default=1.0, help="Huber delta (0: MSE)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
@@ -114,16 +139,22 @@ def main(argv=None):
     _log(f"pairs: {x.shape[0]} from {len(train_seeds)} seeds in {t_gen:.1f} s "
          f"(coarse steps per run {min(steps)}..{max(steps)})")
     norm = recalibrate(x, t, C.default_norm())
+    if args.clip > 0:
+        t.clamp_(-args.clip, args.clip)  # shock residuals are heavy-tailed
     net = C.ConvNet(seed=args.seed)
     t0 = time.perf_counter()
     losses = C.train(net, x, t, iters=args.iters, batch=args.batch, lr=args.lr, seed=args.seed,
+                     noise=args.noise, delta=args.huber,
                      log=lambda it, l: _log(f"iter {it} loss {l:.4e}"))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     del x, t
-    rows = evaluate(net, norm, held_seeds, args.n, args.truth)
+    val_seeds = list(range(30000, 30000 + args.validation))
+    alpha, table = choose_alpha(net, norm, val_seeds, args.n) if val_seeds else (1.0, [])
+    rows = evaluate(net, norm, held_seeds, args.n, args.truth, alpha=alpha)
     good = [r for r in rows if r["finite"]]
     summary = dict(
+        alpha=alpha, alpha_table=table,
         pairs_seconds=t_gen, train_seconds=t_train, iters=args.iters, batch=args.batch,
         train_seeds=len(train_seeds), heldout_seeds=len(held_seeds), loss_first=losses[0][1],
         loss_last=losses[-1][1],

@@ -35,12 +35,13 @@ int nn_conv3x3_wgrad(const void* x, const void* dz, float* partial, float* pdb, 
 int nn_flip_weights(const void* w, void* wt, int cout, int cin, void* stream);
 /* dz = dy * GELU'(z), n elements. */
 int nn_gelu_backward(const void* dy, const float* z, void* dz, long long n, void* stream);
-/* Mean squared error over the first nc of cp channels of pred [npix][cp]
- * against target [npix][nc]: dy = d(loss)/d(pred) (BF16 [npix][cp]); the sum
- * of squares is added to *loss (FP64, device).  A NaN target value masks
+/* Mean squared error (delta = 0) or Huber loss (quadratic within delta,
+ * linear beyond) over the first nc of cp channels of pred [npix][cp] against
+ * target [npix][nc]: dy = d(loss)/d(pred) (BF16 [npix][cp]); the summed loss
+ * is added to *loss (FP64, device).  A NaN target value masks
  * that entry out (no loss, zero gradient); count is npix * nc. */
 int nn_mse_grad(const float* pred, const float* target, void* dy, double* loss, long long npix,
-                int cp, int nc, void* stream);
+                int cp, int nc, float delta, void* stream);
 /* One Adam step on FP32 weights (step >= 1); w16 (optional) receives the BF16 copy. */
 int nn_adam(float* w, const float* g, float* m, float* v, void* w16, long long n, float lr,
             float b1, float b2, float eps, int step, void* stream);

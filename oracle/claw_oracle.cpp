@@ -14,6 +14,15 @@
 //   step1    : src/1d/step1.f90:4-170
 //   bc1      : src/1d/bc1.f
 //   claw1    : src/1d/claw1.f:394-583
+//   step3    : src/3d/step3.f90:3-873 (serial colour-block order)
+//   flux3    : src/3d/flux3.f90:4-612
+//   bc3      : src/3d/bc3.f (+ the piston BC of examples/acoustics_3d_heterogeneous/bc3.f)
+//   claw3    : src/3d/claw3.f:738-928
+// Pins (tests/test_oracle_golden.py): the 3D regression sums are reproduced
+// exactly, the 1D heterogeneous sums bit for bit, the 1D example to 1e-16.
+// 2D Euler (Roe + Harten-Hyman entropy fix): parity unpinned -- the reference
+// ships no 2D Euler solver, example or regression data; the restatement is
+// checked by conservation and shock-tube properties (tests/test_oracle_euler.py).
 // Arrays use the reference's Fortran layout: q(meqn, 1-mbc:mx+mbc, ...) with
 // the equation index fastest.  Compile with -ffp-contract=off so every
 // multiply and add rounds separately, as the GPU parity build does.
