@@ -65,19 +65,19 @@ struct Runner3D : Runner {
             if (n > 0x7fffffffLL) return fail(CLAW_E_UNSUPPORTED, "3D grid too large");
             grid[dir] = (int)n;
         }
-        CUDA_TRY(cudaFuncSetAttribute(sweep3_kernel<S, 0, M, false>,
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 0, M, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-        CUDA_TRY(cudaFuncSetAttribute(sweep3_kernel<S, 1, M, false>,
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 1, M, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-        CUDA_TRY(cudaFuncSetAttribute(sweep3_kernel<S, 2, M, true>,
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 2, M, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
         return 0;
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        sweep3_kernel<S, 0, M, false><<<grid[0], NT3, SMEM, s>>>(args[0]);
-        sweep3_kernel<S, 1, M, false><<<grid[1], NT3, SMEM, s>>>(args[1]);
-        sweep3_kernel<S, 2, M, true><<<grid[2], NT3, SMEM, s>>>(args[2]);
+        sweep3p_kernel<S, 0, M, false><<<grid[0], NT3P, SMEM, s>>>(args[0]);
+        sweep3p_kernel<S, 1, M, false><<<grid[1], NT3P, SMEM, s>>>(args[1]);
+        sweep3p_kernel<S, 2, M, true><<<grid[2], NT3P, SMEM, s>>>(args[2]);
         return cudaGetLastError();
     }
     int launches_per_step() const override { return 3; }

@@ -51,7 +51,7 @@ struct Sweep3Args {
 
 template <typename real>
 constexpr int sweep3_smem_bytes() {
-    return (RING3 * 2 * NS3 + 2 * NTERM3 * NT3) * (int)sizeof(real) + 8 * (int)sizeof(double);
+    return (RING3 * 2 * NS3 + 2 * NTERM3 * NT3) * (int)sizeof(real) + 16 * (int)sizeof(double);
 }
 
 // Source index of (possibly ghost) cell idx along an axis of n cells, and
@@ -528,6 +528,389 @@ __global__ void __launch_bounds__(NT3, 1) sweep3_kernel(const Sweep3Args<typenam
         if (tid == 0) {
             double m = 0.0;
             for (int w = 0; w < NT3 / 32; ++w) m = fmax(m, red[w]);
+            if (!(m > 0.0)) m = (m != m) ? m : 0.0;
+            atomicMax(&ctl->cfl_bits, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+
+// ------------------------------------------------------------ pair variant ---
+// The same sweep with each slice's work split over a thread pair: both
+// threads solve the normal problem, limit and form cqxx (a few dozen
+// operations, duplicated); thread h = 0 then owns flux3's y-like side (the
+// rpt3 splits in e1, the rptt3 splits of the z-like parts in e1, gadd) and
+// h = 1 the z-like side (splits in e2, hadd).  The four combinations each
+// side needs from the other's splits (flux3.f90:363-376 and :488-495) cross
+// by one shuffle, as do the two centre terms.  Half the registers per thread
+// give twice the resident warps.  Operation order per value is unchanged, so
+// results equal sweep3_kernel's bit for bit.
+constexpr int NT3P = 2 * NT3;
+
+template <class S, int DIR, class M, bool LAST>
+__global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typename S::real> a) {
+    using real = typename S::real;
+    using Split = typename S::Split;
+    constexpr int AXN = DIR, AXA = DIR == 0 ? 1 : 0, AXB = DIR == 2 ? 1 : 2;
+    constexpr bool E1A = DIR != 1;
+    constexpr int CN = 1 + AXN, CE1 = 1 + (E1A ? AXA : AXB), CE2 = 1 + (E1A ? AXB : AXA);
+    constexpr unsigned FULL = 0xffffffffu;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    real* saux = reinterpret_cast<real*>(smem_raw);  // [RING3][2][NS3]
+    real* sterm = saux + RING3 * 2 * NS3;            // [2][NTERM3][NT3]
+    double* red = reinterpret_cast<double*>(sterm + 2 * NTERM3 * NT3);
+
+    ClawCtl* ctl = a.ctl;
+    if (ctl->done) return;
+    const int cur = ctl->cur;
+    const real* __restrict__ qold = a.q[cur];
+    real* __restrict__ qnew = a.q[cur ^ 1];
+    const real* __restrict__ aux = a.aux;
+    const double dt = ctl->dt;
+    const double tbc = ctl->told;
+    const real tn = (real)(dt / a.d[AXN]);
+    const real te1 = (real)(dt / a.d[E1A ? AXA : AXB]);
+    const real te2 = (real)(dt / a.d[E1A ? AXB : AXA]);
+    const real H5 = real(0.5) * tn;
+    const real S6g = (real(1.0) / real(6.0)) * tn * te2;
+    const real S6h = (real(1.0) / real(6.0)) * tn * te1;
+    const real dtdxave = real(0.5) * (tn + tn);
+
+    const int m3 = M::m3 >= 0 ? M::m3 : a.m3;
+    const int m4 = M::m4 >= 0 ? M::m4 : a.m4;
+    const int order = M::m3 >= 0 ? 2 : a.order;
+
+    const int mN = a.m[AXN], mA = a.m[AXA], mB = a.m[AXB];
+    const int bid = blockIdx.x;
+    const int seg = bid % a.nseg, tile = bid / a.nseg;
+    const int A0 = 1 + (tile % a.tilesA) * (T3A - 2);
+    const int B0 = 1 + (tile / a.tilesA) * (T3B - 2);
+    const int p0 = 1 + seg * SEG3;
+    const int p1 = min(p0 + SEG3, mN + 1);
+    const int tid = threadIdx.x;
+    const int h = tid & 1;           // 0: y-like side (gadd), 1: z-like side (hadd)
+    const int sl = tid >> 1;         // slice within the tile
+    const int ta = sl % T3A, tb = sl / T3A;
+    const int A = A0 - 1 + ta, B = B0 - 1 + tb;
+    const bool active = A <= mA + 1 && B <= mB + 1;
+    const bool apply = active && ta >= 1 && ta <= T3A - 2 && tb >= 1 && tb <= T3B - 2 &&
+                       A <= mA && B <= mB;
+    const unsigned amask = __ballot_sync(FULL, active);  // pairs are active together
+
+    unsigned long long perm = 0;
+    {
+        int code[9], key[9];
+        for (int k = 0; k < 9; ++k) {
+            const int da = k % 3 - 1, db = k / 3 - 1;
+            const int sA = A + da, sB = B + db;
+            code[k] = k;
+            key[k] = (((sB >> 1) & 1) << 5) | (((sA >> 1) & 1) << 4) | ((db + 1) << 2) | (da + 1);
+        }
+        for (int i = 1; i < 9; ++i)
+            for (int j = i; j > 0 && key[j - 1] > key[j]; --j) {
+                int t = key[j]; key[j] = key[j - 1]; key[j - 1] = t;
+                t = code[j]; code[j] = code[j - 1]; code[j - 1] = t;
+            }
+        for (int k = 0; k < 9; ++k) perm |= (unsigned long long)code[k] << (4 * k);
+    }
+
+    bool flipA, flipB;
+    const int Am = bc3_src(min(max(A, -1), mA + 2), mA, a.bc[2 * AXA], a.bc[2 * AXA + 1], flipA);
+    const int Bm = bc3_src(min(max(B, -1), mB + 2), mB, a.bc[2 * AXB], a.bc[2 * AXB + 1], flipB);
+    const long long qoffAB = (long long)(Am - 1) * a.qs[AXA] + (long long)(Bm - 1) * a.qs[AXB];
+    const bool pistonB = AXB == 2 && B > mB && a.bc[5] == BC_PISTON;
+
+    auto load_pn = [&](int pos, real& qp, real& qn) {
+        bool fN;
+        const int pm = bc3_src(pos, mN, a.bc[2 * AXN], a.bc[2 * AXN + 1], fN);
+        const long long off = qoffAB + (long long)(pm - 1) * a.qs[AXN];
+        qp = qold[off];
+        qn = qold[off + CN * a.fstride];
+        if (fN) qn = -qn;
+        if (CN == 3) {
+            const bool pist = (AXN == 2 && pos > mN && a.bc[5] == BC_PISTON) || pistonB;
+            if (pist) {
+                const int ci = AXN == 0 ? pos : A;
+                const int cj = AXN == 1 ? pos : (AXA == 1 ? A : B);
+                qn = (real)(2.0 * piston_speed(a, ci, cj, tbc)) - qn;
+            }
+        }
+    };
+    auto load_aux = [&](int pos) {
+        real* dst = saux + (pos & (RING3 - 1)) * 2 * NS3;
+        const long long pofs = (long long)(pos + 1) * a.as[AXN];
+        for (int e = tid; e < NS3; e += NT3P) {
+            const int sa = e % S3A, sb = e / S3A;
+            const int Ai = min(A0 - 2 + sa, mA + 2), Bi = min(B0 - 2 + sb, mB + 2);
+            const long long o = pofs + (long long)(Ai + 1) * a.as[AXA] + (long long)(Bi + 1) * a.as[AXB];
+            dst[e] = aux[o];
+            dst[NS3 + e] = aux[o + a.afstride];
+        }
+    };
+    // shared-memory steps of this thread's own split direction and the other
+    const int sown = (tb + 1) * S3A + (ta + 1);
+    const int e1s = E1A ? 1 : S3A, e2s = E1A ? S3A : 1;
+    const int ownS = h ? e2s : e1s, othS = h ? e1s : e2s;
+    auto Zo = [&](int pos, int o, int w) -> real {
+        return saux[(pos & (RING3 - 1)) * 2 * NS3 + sown + o * ownS + w * othS];
+    };
+    auto Co = [&](int pos, int o, int w) -> real {
+        return saux[(pos & (RING3 - 1)) * 2 * NS3 + NS3 + sown + o * ownS + w * othS];
+    };
+    // split in the own direction of a fluctuation at the cell `w` across
+    auto split_own = [&](real xp, int pos, int w) -> Split {
+        return S::split(xp, Zo(pos, -1, w), Co(pos, -1, w), Zo(pos, 0, w), Zo(pos, 1, w), Co(pos, 1, w));
+    };
+    const real t_own = h ? te2 : te1;
+    const real S6own = h ? S6h : S6g;
+
+    double cfl = 0.0;
+    auto solve = [&](int i, real pL, real uL, real pR, real uR, real w[2][2], real am[2], real ap[2]) {
+        real s[2];
+        S::rpn(pL, uL, pR, uR, Zo(i - 1, 0, 0), Co(i - 1, 0, 0), Zo(i, 0, 0), Co(i, 0, 0), w, s, am, ap);
+        if (i >= 1 && i <= mN + 1) {
+            for (int k = 0; k < 2; ++k) {
+                const double c = (double)(tn * s[k]);
+                cfl = fmax(fmax(cfl, c), -c);
+            }
+        }
+    };
+
+    load_aux(p0 - 2);
+    load_aux(p0 - 1);
+    load_aux(p0);
+    load_aux(p0 + 1);
+    __syncthreads();
+
+    real wA[2][2], wB[2][2];
+    real amB[2], apB[2];
+    real qLp = 0, qLn = 0;
+    real F0[2] = {0, 0};
+    real Qs[2] = {0, 0};
+    real O[2][3][2];  // own side's gadd or hadd (side, level, comp) of cell p
+    for (int s_ = 0; s_ < 2; ++s_)
+        for (int l = 0; l < 3; ++l)
+            for (int c = 0; c < 2; ++c) O[s_][l][c] = 0;
+    if (active) {
+        real q0p, q0n, q1p, q1n;
+        load_pn(p0 - 2, q0p, q0n);
+        load_pn(p0 - 1, q1p, q1n);
+        load_pn(p0, qLp, qLn);
+        real am_[2], ap_[2];
+        solve(p0 - 1, q0p, q0n, q1p, q1n, wA, am_, ap_);
+        solve(p0, q1p, q1n, qLp, qLn, wB, amB, apB);
+    }
+    __syncthreads();
+
+    for (int p = p0 - 1; p < p1; ++p) {
+        const bool emit = p >= p0;
+        const int cA = h ? CE1 : 0, cB = h ? CE2 : CN;  // components this thread updates
+        real vA = 0, vB = 0;
+        if (emit && apply) {
+            const long long off = qoffAB + (long long)(p - 1) * a.qs[AXN];
+            const real* src = DIR == 0 ? qold : qnew;
+            vA = src[off + cA * a.fstride];
+            vB = src[off + cB * a.fstride];
+        }
+        real F1[2] = {0, 0};
+        real Qp[2] = {0, 0};
+        real wC[2][2], amC[2], apC[2], qRp = 0, qRn = 0;
+        real cterm = 0, own_c = 0;  // centre terms: sent to the partner / kept
+        if (active) {
+            load_pn(p + 2, qRp, qRn);
+            solve(p + 2, qLp, qLn, qRp, qRn, wC, amC, apC);
+            real wl[2][2];
+            const real sB[2] = {-Co(p, 0, 0), Co(p + 1, 0, 0)};
+            for (int k = 0; k < 2; ++k) {
+                wl[k][0] = wB[k][0];
+                wl[k][1] = wB[k][1];
+                const int lim = M::lim >= 0 ? M::lim : a.mthlim[k];
+                if (order == 2 && lim > 0) {
+                    const real wn2 = wB[k][0] * wB[k][0] + wB[k][1] * wB[k][1];
+                    if (wn2 != real(0)) {
+                        const real dl = wA[k][0] * wB[k][0] + wA[k][1] * wB[k][1];
+                        const real dr = wB[k][0] * wC[k][0] + wB[k][1] * wC[k][1];
+                        const real r = (sB[k] > real(0) ? dl : dr) / wn2;
+                        const real phi = phi_limiter<real>(lim, r);
+                        wl[k][0] = phi * wB[k][0];
+                        wl[k][1] = phi * wB[k][1];
+                    }
+                }
+            }
+            real cq[2] = {0, 0};
+            if (order == 2) {
+                for (int k = 0; k < 2; ++k) {
+                    const real as_ = fabs(sB[k]);
+                    const real coef = (real(0.5) * as_) * (real(1) - as_ * dtdxave);
+                    cq[0] = cq[0] + coef * wl[k][0];
+                    cq[1] = cq[1] + coef * wl[k][1];
+                }
+            }
+            F1[0] = cq[0];
+            F1[1] = cq[1];
+            Qp[0] = Qs[0] - tn * amB[0];
+            Qp[1] = Qs[1] - tn * amB[1];
+            Qs[0] = real(0) - tn * apB[0];
+            Qs[1] = real(0) - tn * apB[1];
+
+            const int L = p, R = p + 1;
+            // ---- cell p: the amdq side of interface p+1 completes gadd/hadd
+            if (m3 > 0) {
+                const Split ma = split_own(amB[0], L, 0);
+                Split qm = {0, 0, 0, 0};
+                if (m3 == 2) qm = split_own(cq[0], L, 0);
+                O[0][1][0] = O[0][1][0] - H5 * ma.dp;
+                O[0][1][1] = O[0][1][1] - H5 * ma.dt;
+                O[1][1][0] = O[1][1][0] - H5 * ma.up;
+                O[1][1][1] = O[1][1][1] - H5 * ma.ut;
+                if (m4 > 0) {
+                    // the combinations the partner splits (flux3.f90:363-376, 488-495)
+                    real x1 = ma.up, x3 = ma.dp;
+                    if (m4 == 2) {
+                        x1 = ma.up + real(3) * qm.up;
+                        x3 = ma.dp + real(3) * qm.dp;
+                    }
+                    const real y1 = __shfl_xor_sync(amask, x1, 1);
+                    const real y3 = __shfl_xor_sync(amask, x3, 1);
+                    const Split tpm = split_own(y1, L, 1), tmm = split_own(y3, L, -1);
+                    O[1][1][0] = O[1][1][0] + S6own * (tpm.up - tmm.up);
+                    O[1][1][1] = O[1][1][1] + S6own * (tpm.ut - tmm.ut);
+                    O[0][1][0] = O[0][1][0] + S6own * (tpm.dp - tmm.dp);
+                    O[0][1][1] = O[0][1][1] + S6own * (tpm.dt - tmm.dt);
+                    O[1][2][0] = O[1][2][0] - S6own * tpm.up;
+                    O[1][2][1] = O[1][2][1] - S6own * tpm.ut;
+                    O[0][2][0] = O[0][2][0] - S6own * tpm.dp;
+                    O[0][2][1] = O[0][2][1] - S6own * tpm.dt;
+                    O[1][0][0] = O[1][0][0] + S6own * tmm.up;
+                    O[1][0][1] = O[1][0][1] + S6own * tmm.ut;
+                    O[0][0][0] = O[0][0][0] + S6own * tmm.dp;
+                    O[0][0][1] = O[0][0][1] + S6own * tmm.dt;
+                }
+                if (m3 == 2) {
+                    O[1][1][0] = O[1][1][0] - tn * qm.up;
+                    O[1][1][1] = O[1][1][1] - tn * qm.ut;
+                    O[0][1][0] = O[0][1][0] - tn * qm.dp;
+                    O[0][1][1] = O[0][1][1] - tn * qm.dt;
+                }
+            }
+            if (emit) {
+                // terms for the eight neighbours: own offset o (the side), other w (the level)
+                real* out = sterm + (p & 1) * NTERM3 * NT3 + sl;
+                for (int w = -1; w <= 1; ++w)
+                    for (int o = -1; o <= 1; ++o) {
+                        if (o == 0 && w == 0) continue;
+                        const int de1 = h ? w : o, de2 = h ? o : w;
+                        const int idx9 = (de2 + 1) * 3 + (de1 + 1);
+                        const int nb = idx9 < 4 ? idx9 : idx9 - 1;
+                        for (int c = 0; c < 2; ++c) {
+                            const real tv = o < 0 ? -(t_own * O[0][w + 1][c])
+                                          : o == 0 ? -(t_own * (O[1][w + 1][c] - O[0][w + 1][c]))
+                                                   : t_own * O[1][w + 1][c];
+                            out[(nb * 4 + 2 * h + c) * NT3] = tv;
+                        }
+                    }
+                // centre: h = 0 keeps te1*dG_p and sends te1*dG_e1; h = 1
+                // keeps te2*dH_e2 and sends te2*dH_p
+                const real dp_ = t_own * (O[1][1][0] - O[0][1][0]);
+                const real dv_ = t_own * (O[1][1][1] - O[0][1][1]);
+                cterm = h ? dp_ : dv_;
+                own_c = h ? dv_ : dp_;
+            }
+            // ---- cell p+1: the apdq side of interface p+1 starts gadd/hadd
+            for (int s_ = 0; s_ < 2; ++s_)
+                for (int l = 0; l < 3; ++l)
+                    for (int c = 0; c < 2; ++c) O[s_][l][c] = 0;
+            if (m3 > 0) {
+                const Split mp = split_own(apB[0], R, 0);
+                Split qp = {0, 0, 0, 0};
+                if (m3 == 2) qp = split_own(cq[0], R, 0);
+                O[0][1][0] = O[0][1][0] - H5 * mp.dp;
+                O[0][1][1] = O[0][1][1] - H5 * mp.dt;
+                O[1][1][0] = O[1][1][0] - H5 * mp.up;
+                O[1][1][1] = O[1][1][1] - H5 * mp.ut;
+                if (m4 > 0) {
+                    real x0 = mp.up, x2 = mp.dp;
+                    if (m4 == 2) {
+                        x0 = mp.up - real(3) * qp.up;
+                        x2 = mp.dp - real(3) * qp.dp;
+                    }
+                    const real y0 = __shfl_xor_sync(amask, x0, 1);
+                    const real y2 = __shfl_xor_sync(amask, x2, 1);
+                    const Split tpp = split_own(y0, R, 1), tmp = split_own(y2, R, -1);
+                    O[1][1][0] = O[1][1][0] + S6own * (tpp.up - tmp.up);
+                    O[1][1][1] = O[1][1][1] + S6own * (tpp.ut - tmp.ut);
+                    O[0][1][0] = O[0][1][0] + S6own * (tpp.dp - tmp.dp);
+                    O[0][1][1] = O[0][1][1] + S6own * (tpp.dt - tmp.dt);
+                    O[1][2][0] = O[1][2][0] - S6own * tpp.up;
+                    O[1][2][1] = O[1][2][1] - S6own * tpp.ut;
+                    O[0][2][0] = O[0][2][0] - S6own * tpp.dp;
+                    O[0][2][1] = O[0][2][1] - S6own * tpp.dt;
+                    O[1][0][0] = O[1][0][0] + S6own * tmp.up;
+                    O[1][0][1] = O[1][0][1] + S6own * tmp.ut;
+                    O[0][0][0] = O[0][0][0] + S6own * tmp.dp;
+                    O[0][0][1] = O[0][0][1] + S6own * tmp.dt;
+                }
+                if (m3 == 2) {
+                    O[1][1][0] = O[1][1][0] + tn * qp.up;
+                    O[1][1][1] = O[1][1][1] + tn * qp.ut;
+                    O[0][1][0] = O[0][1][0] + tn * qp.dp;
+                    O[0][1][1] = O[0][1][1] + tn * qp.dt;
+                }
+            }
+        }
+        const real crecv = __shfl_xor_sync(FULL, cterm, 1);
+        if (p + 3 <= p1 + 1) load_aux(p + 3);
+        __syncthreads();
+        if (emit && apply) {
+            const real* in = sterm + (p & 1) * NTERM3 * NT3;
+            for (int k = 0; k < 9; ++k) {
+                const int code = (int)((perm >> (4 * k)) & 15ull);
+                if (code == 4) {
+                    if (h == 0) {
+                        vA = vA + Qp[0] - tn * (F1[0] - F0[0]) - own_c - crecv;
+                        vB = vB + Qp[1] - tn * (F1[1] - F0[1]);
+                    } else {
+                        vA = vA - crecv;
+                        vB = vB - own_c;
+                    }
+                } else {
+                    const int da = code % 3 - 1, db = code / 3 - 1;
+                    const int u = E1A ? -da : -db, w = E1A ? -db : -da;
+                    const int idx9 = (w + 1) * 3 + (u + 1);
+                    const int nb = idx9 < 4 ? idx9 : idx9 - 1;
+                    const int src = sl + db * T3A + da;
+                    if (h == 0) {
+                        vA = vA + in[(nb * 4 + 0) * NT3 + src] + in[(nb * 4 + 2) * NT3 + src];
+                    } else {
+                        vA = vA + in[(nb * 4 + 1) * NT3 + src];
+                        vB = vB + in[(nb * 4 + 3) * NT3 + src];
+                    }
+                }
+            }
+            const long long off = qoffAB + (long long)(p - 1) * a.qs[AXN];
+            qnew[off + cA * a.fstride] = vA;
+            qnew[off + cB * a.fstride] = vB;
+        }
+        if (active) {
+            for (int k = 0; k < 2; ++k)
+                for (int c = 0; c < 2; ++c) { wA[k][c] = wB[k][c]; wB[k][c] = wC[k][c]; }
+            amB[0] = amC[0]; amB[1] = amC[1];
+            apB[0] = apC[0]; apB[1] = apC[1];
+            qLp = qRp; qLn = qRn;
+            F0[0] = F1[0]; F0[1] = F1[1];
+        }
+    }
+
+    if (LAST) {
+        cta_cfl_and_control(ctl, cfl, red);
+    } else {
+        for (int off = 16; off > 0; off >>= 1) cfl = fmax(cfl, __shfl_xor_sync(FULL, cfl, off));
+        if ((tid & 31) == 0) red[tid >> 5] = cfl;
+        __syncthreads();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int w = 0; w < NT3P / 32; ++w) m = fmax(m, red[w]);
             if (!(m > 0.0)) m = (m != m) ? m : 0.0;
             atomicMax(&ctl->cfl_bits, (unsigned long long)__double_as_longlong(m));
         }
