@@ -41,7 +41,8 @@ def up_to_date() -> bool:
 # (fast2d.cu) contracts to fused multiply-adds.
 UNITS = [("claw_b200.cu", "--fmad=false"), ("noalloc.cu", "--fmad=false"),
          ("fast2d.cu", "--fmad=true"), ("claw3d.cu", "--fmad=false"),
-         ("batch2d.cu", "--fmad=false"), ("nn.cu", "--fmad=true")]
+         ("batch2d.cu", "--fmad=false"), ("nn.cu", "--fmad=true"),
+         ("fast3d.cu", "--fmad=true")]
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:

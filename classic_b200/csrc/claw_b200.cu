@@ -311,7 +311,6 @@ static int validate(const claw_config* c, SolverShape* sh) {
     if (c->num_dim == 3) {
         if (c->capa_index != 0) return fail(CLAW_E_UNSUPPORTED, "3D capacity is not built");
         if (c->use_fwaves) return fail(CLAW_E_UNSUPPORTED, "3D f-waves are not built");
-        if (c->precision != CLAW_FP64) return fail(CLAW_E_UNSUPPORTED, "3D runs in FP64 only");
     }
     return 0;
 }

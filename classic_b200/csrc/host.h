@@ -44,6 +44,8 @@ std::unique_ptr<Runner> make_char_runner(const claw_config& cfg);
 
 // 3D step (step3d.cuh: one launch per sweep); nullptr if cfg is not served.
 std::unique_ptr<Runner> make_runner3d(const claw_config& cfg);
+// its fused-multiply-add / FP32 builds (fast3d.cu)
+std::unique_ptr<Runner> make_fast_runner3d(const claw_config& cfg);
 
 }  // namespace clawb200
 

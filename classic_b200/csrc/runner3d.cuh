@@ -1,0 +1,95 @@
+// Runner of the 3D step (one launch per sweep: x, y, z; the z-sweep's last
+// CTA runs claw3's dt controller, src/3d/claw3.f:738-904), shared by the
+// reference-order unit (claw3d.cu, --fmad=false) and the fused / FP32 unit
+// (fast3d.cu).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+
+#include "host.h"
+#include "riemann.cuh"
+#include "step3d.cuh"
+
+namespace clawb200 {
+
+template <class S, class M>
+struct Runner3D : Runner {
+    using real = typename S::real;
+    Sweep3Args<real> args[3];
+    int grid[3] = {1, 1, 1};
+    static constexpr int SMEM = sweep3_smem_bytes<real>();
+
+    int prepare(const claw_config& cfg, const Geometry& g) override {
+        Sweep3Args<real> b;
+        std::memset(&b, 0, sizeof(b));
+        b.q[0] = static_cast<real*>(g.q[0]);
+        b.q[1] = static_cast<real*>(g.q[1]);
+        b.aux = static_cast<const real*>(g.aux);
+        b.qs[0] = 1;
+        b.qs[1] = g.ld;
+        b.qs[2] = g.ld * g.my;
+        b.fstride = g.fstride;
+        b.as[0] = 1;
+        b.as[1] = g.ald;
+        b.as[2] = g.ald * (g.my + 4);
+        b.afstride = g.afstride;
+        b.m[0] = g.mx;
+        b.m[1] = g.my;
+        b.m[2] = g.mz;
+        for (int d = 0; d < 3; ++d) {
+            b.bc[2 * d] = cfg.bc_lower[d];
+            b.bc[2 * d + 1] = cfg.bc_upper[d];
+        }
+        b.mthlim[0] = cfg.limiter[0];
+        b.mthlim[1] = cfg.limiter[1];
+        b.order = cfg.order;
+        b.m3 = cfg.transverse_waves / 10;
+        b.m4 = cfg.transverse_waves - 10 * b.m3;
+        b.d[0] = g.dx;
+        b.d[1] = g.dy;
+        b.d[2] = g.dz;
+        b.xlower = cfg.lower[0];
+        b.ylower = cfg.lower[1];
+        b.ctl = g.ctl;
+        const int m[3] = {g.mx, g.my, g.mz};
+        for (int dir = 0; dir < 3; ++dir) {
+            const int axa = dir == 0 ? 1 : 0, axb = dir == 2 ? 1 : 2;
+            args[dir] = b;
+            args[dir].tilesA = (m[axa] + T3A - 3) / (T3A - 2);
+            args[dir].tilesB = (m[axb] + T3B - 3) / (T3B - 2);
+            args[dir].nseg = (m[dir] + SEG3 - 1) / SEG3;
+            const long long n = (long long)args[dir].tilesA * args[dir].tilesB * args[dir].nseg;
+            if (n > 0x7fffffffLL) return fail(CLAW_E_UNSUPPORTED, "3D grid too large");
+            grid[dir] = (int)n;
+        }
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 0, M, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 1, M, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 2, M, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        return 0;
+    }
+
+    cudaError_t launch(cudaStream_t s) override {
+        sweep3p_kernel<S, 0, M, false><<<grid[0], NT3P, SMEM, s>>>(args[0]);
+        sweep3p_kernel<S, 1, M, false><<<grid[1], NT3P, SMEM, s>>>(args[1]);
+        sweep3p_kernel<S, 2, M, true><<<grid[2], NT3P, SMEM, s>>>(args[2]);
+        return cudaGetLastError();
+    }
+    int launches_per_step() const override { return 3; }
+};
+
+
+template <typename real>
+std::unique_ptr<Runner> runner3d_for(const claw_config& cfg) {
+    using S = VCAcoustics3D<real>;
+    if (cfg.order == 2 && cfg.transverse_waves == 22 && cfg.limiter[0] == 4 && cfg.limiter[1] == 4)
+        return std::unique_ptr<Runner>(new Runner3D<S, MethodMC3D>());
+    return std::unique_ptr<Runner>(new Runner3D<S, MethodGeneric3D>());
+}
+
+}  // namespace clawb200

@@ -100,451 +100,17 @@ struct Method3D {
 using MethodGeneric3D = Method3D<-1, -1, -1>;
 using MethodMC3D = Method3D<2, 2, 4>;  // transverse_waves 22, MC on both waves
 
-template <class S, int DIR, class M, bool LAST>
-__global__ void __launch_bounds__(NT3, 1) sweep3_kernel(const Sweep3Args<typename S::real> a) {
-    using real = typename S::real;
-    using Split = typename S::Split;
-    // sweep axis N; slice axes A (lower-numbered) and B; flux3's y-like (e1)
-    // and z-like (e2) directions: x-sweep (y, z), y-sweep (z, x), z-sweep (x, y)
-    constexpr int AXN = DIR, AXA = DIR == 0 ? 1 : 0, AXB = DIR == 2 ? 1 : 2;
-    constexpr bool E1A = DIR != 1;
-    constexpr int CN = 1 + AXN, CE1 = 1 + (E1A ? AXA : AXB), CE2 = 1 + (E1A ? AXB : AXA);
-
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    real* saux = reinterpret_cast<real*>(smem_raw);  // [RING3][2][NS3]
-    real* sterm = saux + RING3 * 2 * NS3;            // [2][NTERM3][NT3]
-    double* red = reinterpret_cast<double*>(sterm + 2 * NTERM3 * NT3);
-
-    ClawCtl* ctl = a.ctl;
-    if (ctl->done) return;
-    const int cur = ctl->cur;
-    const real* __restrict__ qold = a.q[cur];
-    real* __restrict__ qnew = a.q[cur ^ 1];
-    const real* __restrict__ aux = a.aux;
-    const double dt = ctl->dt;
-    const double tbc = ctl->told;
-    const real tn = (real)(dt / a.d[AXN]);
-    const real te1 = (real)(dt / a.d[E1A ? AXA : AXB]);
-    const real te2 = (real)(dt / a.d[E1A ? AXB : AXA]);
-    const real H5 = real(0.5) * tn;
-    const real S6g = (real(1.0) / real(6.0)) * tn * te2;  // (1/6) dtdx1d * dtdz of flux3
-    const real S6h = (real(1.0) / real(6.0)) * tn * te1;  // (1/6) dtdx1d * dtdy
-    const real dtdxave = real(0.5) * (tn + tn);
-
-    const int m3 = M::m3 >= 0 ? M::m3 : a.m3;
-    const int m4 = M::m4 >= 0 ? M::m4 : a.m4;
-    const int order = M::m3 >= 0 ? 2 : a.order;
-
-    const int mN = a.m[AXN], mA = a.m[AXA], mB = a.m[AXB];
-    const int bid = blockIdx.x;
-    const int seg = bid % a.nseg, tile = bid / a.nseg;
-    const int A0 = 1 + (tile % a.tilesA) * (T3A - 2);
-    const int B0 = 1 + (tile / a.tilesA) * (T3B - 2);
-    const int p0 = 1 + seg * SEG3;
-    const int p1 = min(p0 + SEG3, mN + 1);
-    const int tid = threadIdx.x;
-    const int ta = tid % T3A, tb = tid / T3A;
-    const int A = A0 - 1 + ta, B = B0 - 1 + tb;
-    const bool active = A <= mA + 1 && B <= mB + 1;
-    const bool apply = active && ta >= 1 && ta <= T3A - 2 && tb >= 1 && tb <= T3B - 2 &&
-                       A <= mA && B <= mB;
-
-    // order of the nine contributions to this thread's cell: sort the slices
-    // (A+a', B+b') by (colour of B+b', colour of A+a', B+b', A+a')
-    unsigned long long perm = 0;
-    {
-        int code[9], key[9];
-        for (int k = 0; k < 9; ++k) {
-            const int da = k % 3 - 1, db = k / 3 - 1;
-            const int sA = A + da, sB = B + db;
-            code[k] = k;
-            key[k] = (((sB >> 1) & 1) << 5) | (((sA >> 1) & 1) << 4) | ((db + 1) << 2) | (da + 1);
-        }
-        for (int i = 1; i < 9; ++i)
-            for (int j = i; j > 0 && key[j - 1] > key[j]; --j) {
-                int t = key[j]; key[j] = key[j - 1]; key[j - 1] = t;
-                t = code[j]; code[j] = code[j - 1]; code[j - 1] = t;
-            }
-        for (int k = 0; k < 9; ++k) perm |= (unsigned long long)code[k] << (4 * k);
-    }
-
-    // the slice's fixed coordinates, mapped through the boundary conditions
-    bool flipA, flipB;
-    const int Am = bc3_src(min(max(A, -1), mA + 2), mA, a.bc[2 * AXA], a.bc[2 * AXA + 1], flipA);
-    const int Bm = bc3_src(min(max(B, -1), mB + 2), mB, a.bc[2 * AXB], a.bc[2 * AXB + 1], flipB);
-    const long long qoffAB = (long long)(Am - 1) * a.qs[AXA] + (long long)(Bm - 1) * a.qs[AXB];
-    const bool pistonB = AXB == 2 && B > mB && a.bc[5] == BC_PISTON;
-
-    // (p, normal velocity) of the slice's cell at position pos
-    auto load_pn = [&](int pos, real& qp, real& qn) {
-        bool fN;
-        const int pm = bc3_src(pos, mN, a.bc[2 * AXN], a.bc[2 * AXN + 1], fN);
-        const long long off = qoffAB + (long long)(pm - 1) * a.qs[AXN];
-        qp = qold[off];
-        qn = qold[off + CN * a.fstride];
-        if (fN) qn = -qn;
-        if (CN == 1 + AXA && flipA) qn = -qn;
-        if (CN == 1 + AXB && flipB) qn = -qn;
-        if (CN == 3) {  // the piston sets w in the z-upper ghost cells
-            const bool pist = (AXN == 2 && pos > mN && a.bc[5] == BC_PISTON) || pistonB;
-            if (pist) {
-                const int ci = AXN == 0 ? pos : A;
-                const int cj = AXN == 1 ? pos : (AXA == 1 ? A : B);
-                qn = (real)(2.0 * piston_speed(a, ci, cj, tbc)) - qn;
-            }
-        }
-    };
-
-    // cooperative load of the aux tile (with its ring) at position pos
-    auto load_aux = [&](int pos) {
-        real* dst = saux + (pos & (RING3 - 1)) * 2 * NS3;
-        const long long pofs = (long long)(pos + 1) * a.as[AXN];
-        for (int e = tid; e < NS3; e += NT3) {
-            const int sa = e % S3A, sb = e / S3A;
-            const int Ai = min(A0 - 2 + sa, mA + 2), Bi = min(B0 - 2 + sb, mB + 2);
-            const long long o = pofs + (long long)(Ai + 1) * a.as[AXA] + (long long)(Bi + 1) * a.as[AXB];
-            dst[e] = aux[o];
-            dst[NS3 + e] = aux[o + a.afstride];
-        }
-    };
-    // aux of the cell at (e1 offset u, e2 offset w) from this slice, position slot
-    const int sown = (tb + 1) * S3A + (ta + 1);
-    auto AZ = [&](int pos, int u, int w) -> real {
-        const int da = E1A ? u : w, db = E1A ? w : u;
-        return saux[(pos & (RING3 - 1)) * 2 * NS3 + sown + db * S3A + da];
-    };
-    auto AC = [&](int pos, int u, int w) -> real {
-        const int da = E1A ? u : w, db = E1A ? w : u;
-        return saux[(pos & (RING3 - 1)) * 2 * NS3 + NS3 + sown + db * S3A + da];
-    };
-    // rpt3 / rptt3 splits in e1 at e2 level w, in e2 at e1 row u
-    auto split1 = [&](real xp, int pos, int w) -> Split {
-        return S::split(xp, AZ(pos, -1, w), AC(pos, -1, w), AZ(pos, 0, w), AZ(pos, 1, w), AC(pos, 1, w));
-    };
-    auto split2 = [&](real xp, int pos, int u) -> Split {
-        return S::split(xp, AZ(pos, u, -1), AC(pos, u, -1), AZ(pos, u, 0), AZ(pos, u, 1), AC(pos, u, 1));
-    };
-
-    double cfl = 0.0;
-    // one normal solve at interface i (cells i-1 | i)
-    auto solve = [&](int i, real pL, real uL, real pR, real uR, real w[2][2], real am[2], real ap[2]) {
-        real s[2];
-        S::rpn(pL, uL, pR, uR, AZ(i - 1, 0, 0), AC(i - 1, 0, 0), AZ(i, 0, 0), AC(i, 0, 0), w, s, am, ap);
-        if (i >= 1 && i <= mN + 1) {
-            for (int k = 0; k < 2; ++k) {
-                const double c = (double)(tn * s[k]);
-                cfl = fmax(fmax(cfl, c), -c);
-            }
-        }
-    };
-
-    // ---------------------------------------------------------------- prologue
-    load_aux(p0 - 2);
-    load_aux(p0 - 1);
-    load_aux(p0);
-    load_aux(p0 + 1);
-    __syncthreads();
-
-    real wA[2][2], wB[2][2];          // unlimited waves at interfaces p, p+1
-    real amB[2], apB[2];              // fluctuations at interface p+1
-    real qLp = 0, qLn = 0;            // q (p, un) at cell p+1
-    real F0[2] = {0, 0};              // fadd(p) = cqxx(p)
-    real Qs[2] = {0, 0};              // qadd(p) after its apdq(p) term
-    real G[2][3][2], H[2][3][2];      // gadd / hadd (side, level, comp) of cell p
-    for (int s_ = 0; s_ < 2; ++s_)
-        for (int l = 0; l < 3; ++l)
-            for (int c = 0; c < 2; ++c) { G[s_][l][c] = 0; H[s_][l][c] = 0; }
-    if (active) {
-        real q0p, q0n, q1p, q1n;
-        load_pn(p0 - 2, q0p, q0n);
-        load_pn(p0 - 1, q1p, q1n);
-        load_pn(p0, qLp, qLn);
-        real am_[2], ap_[2];
-        solve(p0 - 1, q0p, q0n, q1p, q1n, wA, am_, ap_);
-        solve(p0, q1p, q1n, qLp, qLn, wB, amB, apB);
-    }
-    __syncthreads();  // the first iteration overwrites the slot of p0-2
-
-    // -------------------------------------------------------------- the march
-    for (int p = p0 - 1; p < p1; ++p) {
-        const bool emit = p >= p0;
-        real v[4];
-        if (emit && apply) {
-            const long long off = qoffAB + (long long)(p - 1) * a.qs[AXN];
-            const real* src = DIR == 0 ? qold : qnew;
-            for (int c = 0; c < 4; ++c) v[c] = src[off + c * a.fstride];
-        }
-        real Gn[2][3][2], Hn[2][3][2];  // gadd / hadd of cell p+1 (apdq side of p+1)
-        real F1[2] = {0, 0};
-        real Qp[2] = {0, 0};
-        real wC[2][2], amC[2], apC[2], qRp = 0, qRn = 0;
-        if (active) {
-            // normal solve at p+2
-            load_pn(p + 2, qRp, qRn);
-            solve(p + 2, qLp, qLn, qRp, qRn, wC, amC, apC);
-            // limiter at p+1 from unlimited neighbours (src/3d/limiter.f90)
-            real wl[2][2];
-            const real sB[2] = {-AC(p, 0, 0), AC(p + 1, 0, 0)};
-            for (int k = 0; k < 2; ++k) {
-                wl[k][0] = wB[k][0];
-                wl[k][1] = wB[k][1];
-                const int lim = M::lim >= 0 ? M::lim : a.mthlim[k];
-                if (order == 2 && lim > 0) {
-                    const real wn2 = wB[k][0] * wB[k][0] + wB[k][1] * wB[k][1];
-                    if (wn2 != real(0)) {
-                        const real dl = wA[k][0] * wB[k][0] + wA[k][1] * wB[k][1];
-                        const real dr = wB[k][0] * wC[k][0] + wB[k][1] * wC[k][1];
-                        const real r = (sB[k] > real(0) ? dl : dr) / wn2;
-                        const real phi = phi_limiter<real>(lim, r);
-                        wl[k][0] = phi * wB[k][0];
-                        wl[k][1] = phi * wB[k][1];
-                    }
-                }
-            }
-            // second-order correction cqxx(p+1) (src/3d/flux3.f90:240-255)
-            real cq[2] = {0, 0};
-            if (order == 2) {
-                for (int k = 0; k < 2; ++k) {
-                    const real as_ = fabs(sB[k]);
-                    const real coef = (real(0.5) * as_) * (real(1) - as_ * dtdxave);
-                    cq[0] = cq[0] + coef * wl[k][0];
-                    cq[1] = cq[1] + coef * wl[k][1];
-                }
-            }
-            F1[0] = cq[0];
-            F1[1] = cq[1];
-            // qadd(p) and the start of qadd(p+1) (src/3d/flux3.f90:211-214)
-            Qp[0] = Qs[0] - tn * amB[0];
-            Qp[1] = Qs[1] - tn * amB[1];
-            Qs[0] = real(0) - tn * apB[0];
-            Qs[1] = real(0) - tn * apB[1];
-
-            for (int s_ = 0; s_ < 2; ++s_)
-                for (int l = 0; l < 3; ++l)
-                    for (int c = 0; c < 2; ++c) { Gn[s_][l][c] = 0; Hn[s_][l][c] = 0; }
-            if (m3 > 0) {
-                const int L = p, R = p + 1;
-                // transverse splits of interface p+1 (src/3d/flux3.f90:286-358)
-                const Split bma = split1(amB[0], L, 0), bmp = split1(apB[0], R, 0);
-                const Split cma = split2(amB[0], L, 0), cmp = split2(apB[0], R, 0);
-                Split bqm = {0, 0, 0, 0}, bqp = bqm, cqm = bqm, cqp = bqm;
-                if (m3 == 2) {
-                    bqm = split1(cq[0], L, 0);
-                    bqp = split1(cq[0], R, 0);
-                    cqm = split2(cq[0], L, 0);
-                    cqp = split2(cq[0], R, 0);
-                }
-                // ---- G (y-like) fluxes, src/3d/flux3.f90:363-480
-                Split tpp = bqm, tpm = bqm, tmp = bqm, tmm = bqm;  // rptt3 results
-                if (m4 > 0) {
-                    real cpap2 = cmp.up, cpam2 = cma.up, cmap2 = cmp.dp, cmam2 = cma.dp;
-                    if (m4 == 2) {
-                        cpap2 = cmp.up - real(3) * cqp.up;
-                        cpam2 = cma.up + real(3) * cqm.up;
-                        cmap2 = cmp.dp - real(3) * cqp.dp;
-                        cmam2 = cma.dp + real(3) * cqm.dp;
-                    }
-                    tpp = split1(cpap2, R, 1);   // bm/bp c p apdq
-                    tpm = split1(cpam2, L, 1);   // bm/bp c p amdq
-                    tmp = split1(cmap2, R, -1);  // bm/bp c m apdq
-                    tmm = split1(cmam2, L, -1);  // bm/bp c m amdq
-                }
-                // cell p (the amdq side of interface p+1)
-                G[0][1][0] = G[0][1][0] - H5 * bma.dp;
-                G[0][1][1] = G[0][1][1] - H5 * bma.dt;
-                G[1][1][0] = G[1][1][0] - H5 * bma.up;
-                G[1][1][1] = G[1][1][1] - H5 * bma.ut;
-                // cell p+1 (the apdq side)
-                Gn[0][1][0] = Gn[0][1][0] - H5 * bmp.dp;
-                Gn[0][1][1] = Gn[0][1][1] - H5 * bmp.dt;
-                Gn[1][1][0] = Gn[1][1][0] - H5 * bmp.up;
-                Gn[1][1][1] = Gn[1][1][1] - H5 * bmp.ut;
-                if (m4 > 0) {
-                    Gn[1][1][0] = Gn[1][1][0] + S6g * (tpp.up - tmp.up);
-                    Gn[1][1][1] = Gn[1][1][1] + S6g * (tpp.ut - tmp.ut);
-                    Gn[0][1][0] = Gn[0][1][0] + S6g * (tpp.dp - tmp.dp);
-                    Gn[0][1][1] = Gn[0][1][1] + S6g * (tpp.dt - tmp.dt);
-                    Gn[1][2][0] = Gn[1][2][0] - S6g * tpp.up;
-                    Gn[1][2][1] = Gn[1][2][1] - S6g * tpp.ut;
-                    Gn[0][2][0] = Gn[0][2][0] - S6g * tpp.dp;
-                    Gn[0][2][1] = Gn[0][2][1] - S6g * tpp.dt;
-                    Gn[1][0][0] = Gn[1][0][0] + S6g * tmp.up;
-                    Gn[1][0][1] = Gn[1][0][1] + S6g * tmp.ut;
-                    Gn[0][0][0] = Gn[0][0][0] + S6g * tmp.dp;
-                    Gn[0][0][1] = Gn[0][0][1] + S6g * tmp.dt;
-                    G[1][1][0] = G[1][1][0] + S6g * (tpm.up - tmm.up);
-                    G[1][1][1] = G[1][1][1] + S6g * (tpm.ut - tmm.ut);
-                    G[0][1][0] = G[0][1][0] + S6g * (tpm.dp - tmm.dp);
-                    G[0][1][1] = G[0][1][1] + S6g * (tpm.dt - tmm.dt);
-                    G[1][2][0] = G[1][2][0] - S6g * tpm.up;
-                    G[1][2][1] = G[1][2][1] - S6g * tpm.ut;
-                    G[0][2][0] = G[0][2][0] - S6g * tpm.dp;
-                    G[0][2][1] = G[0][2][1] - S6g * tpm.dt;
-                    G[1][0][0] = G[1][0][0] + S6g * tmm.up;
-                    G[1][0][1] = G[1][0][1] + S6g * tmm.ut;
-                    G[0][0][0] = G[0][0][0] + S6g * tmm.dp;
-                    G[0][0][1] = G[0][0][1] + S6g * tmm.dt;
-                }
-                if (m3 == 2) {
-                    Gn[1][1][0] = Gn[1][1][0] + tn * bqp.up;
-                    Gn[1][1][1] = Gn[1][1][1] + tn * bqp.ut;
-                    Gn[0][1][0] = Gn[0][1][0] + tn * bqp.dp;
-                    Gn[0][1][1] = Gn[0][1][1] + tn * bqp.dt;
-                    G[1][1][0] = G[1][1][0] - tn * bqm.up;
-                    G[1][1][1] = G[1][1][1] - tn * bqm.ut;
-                    G[0][1][0] = G[0][1][0] - tn * bqm.dp;
-                    G[0][1][1] = G[0][1][1] - tn * bqm.dt;
-                }
-                // ---- H (z-like) fluxes, src/3d/flux3.f90:482-609
-                if (m4 > 0) {
-                    real bpap = bmp.up, bpam = bma.up, bmap = bmp.dp, bmam = bma.dp;
-                    if (m4 == 2) {
-                        bpap = bmp.up - real(3) * bqp.up;
-                        bpam = bma.up + real(3) * bqm.up;
-                        bmap = bmp.dp - real(3) * bqp.dp;
-                        bmam = bma.dp + real(3) * bqm.dp;
-                    }
-                    tpp = split2(bpap, R, 1);
-                    tpm = split2(bpam, L, 1);
-                    tmp = split2(bmap, R, -1);
-                    tmm = split2(bmam, L, -1);
-                }
-                H[0][1][0] = H[0][1][0] - H5 * cma.dp;
-                H[0][1][1] = H[0][1][1] - H5 * cma.dt;
-                H[1][1][0] = H[1][1][0] - H5 * cma.up;
-                H[1][1][1] = H[1][1][1] - H5 * cma.ut;
-                Hn[0][1][0] = Hn[0][1][0] - H5 * cmp.dp;
-                Hn[0][1][1] = Hn[0][1][1] - H5 * cmp.dt;
-                Hn[1][1][0] = Hn[1][1][0] - H5 * cmp.up;
-                Hn[1][1][1] = Hn[1][1][1] - H5 * cmp.ut;
-                if (m4 > 0) {
-                    Hn[1][1][0] = Hn[1][1][0] + S6h * (tpp.up - tmp.up);
-                    Hn[1][1][1] = Hn[1][1][1] + S6h * (tpp.ut - tmp.ut);
-                    Hn[0][1][0] = Hn[0][1][0] + S6h * (tpp.dp - tmp.dp);
-                    Hn[0][1][1] = Hn[0][1][1] + S6h * (tpp.dt - tmp.dt);
-                    Hn[1][2][0] = Hn[1][2][0] - S6h * tpp.up;
-                    Hn[1][2][1] = Hn[1][2][1] - S6h * tpp.ut;
-                    Hn[0][2][0] = Hn[0][2][0] - S6h * tpp.dp;
-                    Hn[0][2][1] = Hn[0][2][1] - S6h * tpp.dt;
-                    Hn[1][0][0] = Hn[1][0][0] + S6h * tmp.up;
-                    Hn[1][0][1] = Hn[1][0][1] + S6h * tmp.ut;
-                    Hn[0][0][0] = Hn[0][0][0] + S6h * tmp.dp;
-                    Hn[0][0][1] = Hn[0][0][1] + S6h * tmp.dt;
-                    H[1][1][0] = H[1][1][0] + S6h * (tpm.up - tmm.up);
-                    H[1][1][1] = H[1][1][1] + S6h * (tpm.ut - tmm.ut);
-                    H[0][1][0] = H[0][1][0] + S6h * (tpm.dp - tmm.dp);
-                    H[0][1][1] = H[0][1][1] + S6h * (tpm.dt - tmm.dt);
-                    H[1][2][0] = H[1][2][0] - S6h * tpm.up;
-                    H[1][2][1] = H[1][2][1] - S6h * tpm.ut;
-                    H[0][2][0] = H[0][2][0] - S6h * tpm.dp;
-                    H[0][2][1] = H[0][2][1] - S6h * tpm.dt;
-                    H[1][0][0] = H[1][0][0] + S6h * tmm.up;
-                    H[1][0][1] = H[1][0][1] + S6h * tmm.ut;
-                    H[0][0][0] = H[0][0][0] + S6h * tmm.dp;
-                    H[0][0][1] = H[0][0][1] + S6h * tmm.dt;
-                }
-                if (m3 == 2) {
-                    Hn[1][1][0] = Hn[1][1][0] + tn * cqp.up;
-                    Hn[1][1][1] = Hn[1][1][1] + tn * cqp.ut;
-                    Hn[0][1][0] = Hn[0][1][0] + tn * cqp.dp;
-                    Hn[0][1][1] = Hn[0][1][1] + tn * cqp.dt;
-                    H[1][1][0] = H[1][1][0] - tn * cqm.up;
-                    H[1][1][1] = H[1][1][1] - tn * cqm.ut;
-                    H[0][1][0] = H[0][1][0] - tn * cqm.dp;
-                    H[0][1][1] = H[0][1][1] - tn * cqm.dt;
-                }
-            }
-            // publish the terms this slice adds to its eight neighbour cells
-            if (emit) {
-                real* out = sterm + (p & 1) * NTERM3 * NT3 + tid;
-                int nb = 0;
-                for (int w = -1; w <= 1; ++w)
-                    for (int u = -1; u <= 1; ++u) {
-                        if (u == 0 && w == 0) continue;
-                        for (int c = 0; c < 2; ++c) {
-                            const real g = u < 0 ? -(te1 * G[0][w + 1][c])
-                                         : u == 0 ? -(te1 * (G[1][w + 1][c] - G[0][w + 1][c]))
-                                                  : te1 * G[1][w + 1][c];
-                            const real h = w < 0 ? -(te2 * H[0][u + 1][c])
-                                         : w == 0 ? -(te2 * (H[1][u + 1][c] - H[0][u + 1][c]))
-                                                  : te2 * H[1][u + 1][c];
-                            out[(nb * 4 + c) * NT3] = g;
-                            out[(nb * 4 + 2 + c) * NT3] = h;
-                        }
-                        ++nb;
-                    }
-            }
-        }
-        if (p + 3 <= p1 + 1) load_aux(p + 3);
-        __syncthreads();
-        if (emit && apply) {
-            const real* in = sterm + (p & 1) * NTERM3 * NT3;
-            for (int k = 0; k < 9; ++k) {
-                const int code = (int)((perm >> (4 * k)) & 15ull);
-                if (code == 4) {
-                    // the slice's own cell (src/3d/step3.f90:293-299)
-                    v[0] = v[0] + Qp[0] - tn * (F1[0] - F0[0]) - te1 * (G[1][1][0] - G[0][1][0]) -
-                           te2 * (H[1][1][0] - H[0][1][0]);
-                    v[CN] = v[CN] + Qp[1] - tn * (F1[1] - F0[1]);
-                    v[CE1] = v[CE1] - te1 * (G[1][1][1] - G[0][1][1]);
-                    v[CE2] = v[CE2] - te2 * (H[1][1][1] - H[0][1][1]);
-                } else {
-                    const int da = code % 3 - 1, db = code / 3 - 1;
-                    // this cell seen from slice (A+da, B+db)
-                    const int u = E1A ? -da : -db, w = E1A ? -db : -da;
-                    const int idx9 = (w + 1) * 3 + (u + 1);
-                    const int nb = idx9 < 4 ? idx9 : idx9 - 1;
-                    const int src = tid + db * T3A + da;
-                    v[0] = v[0] + in[(nb * 4 + 0) * NT3 + src] + in[(nb * 4 + 2) * NT3 + src];
-                    v[CE1] = v[CE1] + in[(nb * 4 + 1) * NT3 + src];
-                    v[CE2] = v[CE2] + in[(nb * 4 + 3) * NT3 + src];
-                }
-            }
-            const long long off = qoffAB + (long long)(p - 1) * a.qs[AXN];
-            for (int c = 0; c < 4; ++c) qnew[off + c * a.fstride] = v[c];
-        }
-        if (active) {
-            // shift the march by one cell
-            for (int k = 0; k < 2; ++k)
-                for (int c = 0; c < 2; ++c) { wA[k][c] = wB[k][c]; wB[k][c] = wC[k][c]; }
-            amB[0] = amC[0]; amB[1] = amC[1];
-            apB[0] = apC[0]; apB[1] = apC[1];
-            qLp = qRp; qLn = qRn;
-            F0[0] = F1[0]; F0[1] = F1[1];
-            for (int s_ = 0; s_ < 2; ++s_)
-                for (int l = 0; l < 3; ++l)
-                    for (int c = 0; c < 2; ++c) { G[s_][l][c] = Gn[s_][l][c]; H[s_][l][c] = Hn[s_][l][c]; }
-        }
-    }
-
-    // Courant number of this sweep: max over the CTA, one atomic per CTA; the
-    // last sweep of a step also runs the dt controller in its last CTA
-    if (LAST) {
-        cta_cfl_and_control(ctl, cfl, red);
-    } else {
-        for (int off = 16; off > 0; off >>= 1) cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
-        if ((tid & 31) == 0) red[tid >> 5] = cfl;
-        __syncthreads();
-        if (tid == 0) {
-            double m = 0.0;
-            for (int w = 0; w < NT3 / 32; ++w) m = fmax(m, red[w]);
-            if (!(m > 0.0)) m = (m != m) ? m : 0.0;
-            atomicMax(&ctl->cfl_bits, (unsigned long long)__double_as_longlong(m));
-        }
-    }
-}
-
-
 // ------------------------------------------------------------ pair variant ---
-// The same sweep with each slice's work split over a thread pair: both
+// Each slice's work is split over a thread pair: both
 // threads solve the normal problem, limit and form cqxx (a few dozen
 // operations, duplicated); thread h = 0 then owns flux3's y-like side (the
 // rpt3 splits in e1, the rptt3 splits of the z-like parts in e1, gadd) and
 // h = 1 the z-like side (splits in e2, hadd).  The four combinations each
 // side needs from the other's splits (flux3.f90:363-376 and :488-495) cross
 // by one shuffle, as do the two centre terms.  Half the registers per thread
-// give twice the resident warps.  Operation order per value is unchanged, so
-// results equal sweep3_kernel's bit for bit.
+// give twice the resident warps of a thread per slice (which needs 255
+// registers).  Operation order per value is flux3's, so results are
+// bit-identical to the serial reference order in FP64 without contraction.
 constexpr int NT3P = 2 * NT3;
 
 template <class S, int DIR, class M, bool LAST>
@@ -569,7 +135,8 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
     const real* __restrict__ aux = a.aux;
     const double dt = ctl->dt;
     const double tbc = ctl->told;
-    const real tn = (real)(dt / a.d[AXN]);
+    const double tn_d = dt / a.d[AXN];
+    const real tn = (real)tn_d;
     const real te1 = (real)(dt / a.d[E1A ? AXA : AXB]);
     const real te2 = (real)(dt / a.d[E1A ? AXB : AXA]);
     const real H5 = real(0.5) * tn;
@@ -670,8 +237,8 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
         real s[2];
         S::rpn(pL, uL, pR, uR, Zo(i - 1, 0, 0), Co(i - 1, 0, 0), Zo(i, 0, 0), Co(i, 0, 0), w, s, am, ap);
         if (i >= 1 && i <= mN + 1) {
-            for (int k = 0; k < 2; ++k) {
-                const double c = (double)(tn * s[k]);
+            for (int k = 0; k < 2; ++k) {  // Courant number in FP64 (FP32 builds too)
+                const double c = tn_d * (double)s[k];
                 cfl = fmax(fmax(cfl, c), -c);
             }
         }

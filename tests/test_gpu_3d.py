@@ -157,3 +157,37 @@ def test_full_size_256_determinism_and_mirror_symmetry():
     assert same(outs[0], outs[1])
     mir = outs[2][:, :, :, ::-1] * np.array([1, -1, 1, 1])[:, None, None, None]
     assert np.all(rel_diff(mir, outs[0]) < 1e-12)
+
+
+def test_fused_fp64_within_1e12_and_same_dt():
+    """CLAW_FP64_FMA: the same kernels with contraction; the Courant number
+    is a single product, so the dt sequence is identical."""
+    rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=48)
+    g = Solver(rd.clawdata, solver, params, precision="fp64_fma")
+    o = OracleGrid(rd.clawdata, solver, params)
+    for s in (g, o):
+        s.set_q(q0)
+        s.set_aux(aux)
+    ig, sg = g.advance(0.0, 0.1, 0.01)
+    io, so = o.advance(0.0, 0.1, 0.01)
+    assert ig == io == 0
+    for key in ("t_reached", "dt_next", "steps_taken", "cfl_max_seen"):
+        assert sg[key] == so[key], key
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 1e-12)
+    g.close()
+
+
+def test_fp32_tracks_fp64():
+    """CLAW_FP32: FP32 update, FP64 Courant number / dt / time."""
+    rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=48)
+    g = Solver(rd.clawdata, solver, params, precision="fp32")
+    o = OracleGrid(rd.clawdata, solver, params)
+    for s in (g, o):
+        s.set_q(q0)
+        s.set_aux(aux)
+    ig, sg = g.advance(0.0, 0.1, 0.01)
+    io, so = o.advance(0.0, 0.1, 0.01)
+    assert ig == io == 0
+    assert abs(sg["t_reached"] - so["t_reached"]) < 1e-12
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 5e-5)
+    g.close()
