@@ -15,7 +15,7 @@
 
 namespace clawb200 {
 
-template <class S, class M>
+template <class S, class M, int BUILD>
 struct Runner3D : Runner {
     using real = typename S::real;
     Sweep3Args<real> args[3];
@@ -65,31 +65,31 @@ struct Runner3D : Runner {
             if (n > 0x7fffffffLL) return fail(CLAW_E_UNSUPPORTED, "3D grid too large");
             grid[dir] = (int)n;
         }
-        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 0, M, false>,
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 0, M, false, BUILD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 1, M, false>,
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 1, M, false, BUILD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 2, M, true>,
+        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 2, M, true, BUILD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
         return 0;
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        sweep3p_kernel<S, 0, M, false><<<grid[0], NT3P, SMEM, s>>>(args[0]);
-        sweep3p_kernel<S, 1, M, false><<<grid[1], NT3P, SMEM, s>>>(args[1]);
-        sweep3p_kernel<S, 2, M, true><<<grid[2], NT3P, SMEM, s>>>(args[2]);
+        sweep3p_kernel<S, 0, M, false, BUILD><<<grid[0], NT3P, SMEM, s>>>(args[0]);
+        sweep3p_kernel<S, 1, M, false, BUILD><<<grid[1], NT3P, SMEM, s>>>(args[1]);
+        sweep3p_kernel<S, 2, M, true, BUILD><<<grid[2], NT3P, SMEM, s>>>(args[2]);
         return cudaGetLastError();
     }
     int launches_per_step() const override { return 3; }
 };
 
 
-template <typename real>
+template <typename real, int BUILD>
 std::unique_ptr<Runner> runner3d_for(const claw_config& cfg) {
     using S = VCAcoustics3D<real>;
     if (cfg.order == 2 && cfg.transverse_waves == 22 && cfg.limiter[0] == 4 && cfg.limiter[1] == 4)
-        return std::unique_ptr<Runner>(new Runner3D<S, MethodMC3D>());
-    return std::unique_ptr<Runner>(new Runner3D<S, MethodGeneric3D>());
+        return std::unique_ptr<Runner>(new Runner3D<S, MethodMC3D, BUILD>());
+    return std::unique_ptr<Runner>(new Runner3D<S, MethodGeneric3D, BUILD>());
 }
 
 }  // namespace clawb200

@@ -113,7 +113,10 @@ using MethodMC3D = Method3D<2, 2, 4>;  // transverse_waves 22, MC on both waves
 // bit-identical to the serial reference order in FP64 without contraction.
 constexpr int NT3P = 2 * NT3;
 
-template <class S, int DIR, class M, bool LAST>
+// BUILD tells apart the instantiations of the reference-order unit (0,
+// --fmad=false) and the contracted unit (1, --fmad=true): the same template
+// arguments in both would be one symbol with two different bodies.
+template <class S, int DIR, class M, bool LAST, int BUILD>
 __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typename S::real> a) {
     using real = typename S::real;
     using Split = typename S::Split;
