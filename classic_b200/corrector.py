@@ -306,8 +306,9 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
     losses = []
     for it in range(iters):
         idx = torch.randint(0, ns, (batch,), device="cuda", generator=gen)
-        oy = torch.randint(0, h - crop + 1, (batch,), device="cuda", generator=gen)
-        ox = torch.randint(0, w - crop + 1, (batch,), device="cuda", generator=gen)
+        # crops start on the 16x16 tile grid the correction is projected on
+        oy = torch.randint(0, (h - crop) // 16 + 1, (batch,), device="cuda", generator=gen) * 16
+        ox = torch.randint(0, (w - crop) // 16 + 1, (batch,), device="cuda", generator=gen) * 16
         ar = torch.arange(crop, device="cuda")
         yy = (oy[:, None] + ar[None, :])[:, :, None]
         xx = (ox[:, None] + ar[None, :])[:, None, :]
@@ -410,3 +411,26 @@ def l1_error(q, ref):
     magnitude, averaged over the four fields."""
     return float(np.mean([np.mean(np.abs(q[c] - ref[c])) / max(np.mean(np.abs(ref[c])), 1e-12)
                           for c in range(q.shape[0])]))
+
+
+def project_tiles(t, tile=16):
+    """Subtract each 16x16 tile's mean from the targets [n][h][w][c] (in
+    place): the correction the network learns is the one applied, which keeps
+    every tile's conserved totals."""
+    n, h, w, c = t.shape
+    v = t.view(n, h // tile, tile, w // tile, tile, c)
+    v -= v.mean(dim=(2, 4), keepdim=True)
+    return t
+
+
+def one_step_gain(net, x, t, batch=8):
+    """Relative L2 error of the network's prediction of the held-out targets
+    (1 = no better than predicting zero)."""
+    torch = _torch()
+    num = den = 0.0
+    for k in range(0, x.shape[0], batch):
+        pred = net.forward(x[k:k + batch].contiguous())[..., :OUT_REAL]
+        tt = t[k:k + batch]
+        num += float(((pred - tt) ** 2).sum())
+        den += float((tt ** 2).sum())
+    return math.sqrt(num / max(den, 1e-300))

@@ -141,6 +141,7 @@ def main(argv=None):
     norm = recalibrate(x, t, C.default_norm())
     if args.clip > 0:
         t.clamp_(-args.clip, args.clip)  # shock residuals are heavy-tailed
+    C.project_tiles(t)
     net = C.ConvNet(seed=args.seed)
     t0 = time.perf_counter()
     losses = C.train(net, x, t, iters=args.iters, batch=args.batch, lr=args.lr, seed=args.seed,
@@ -149,12 +150,28 @@ def main(argv=None):
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     del x, t
+    # one-step skill on pairs of unseen seeds (same scaling and projection)
+    xv, tv, _ = generate(list(range(40000, 40004)), C.Norm(C.default_norm().values), args.n, 4, rng)
+    if xv.shape[0]:
+        sc = C.default_norm().values
+        for c in range(8):
+            xv[..., c] = (xv[..., c].float() * float(norm.values[4 + c] / sc[4 + c])).to(torch.bfloat16)
+        for c in range(4):
+            tv[..., c] *= float(norm.values[12 + c] / sc[12 + c])
+        if args.clip > 0:
+            tv.clamp_(-args.clip, args.clip)
+        C.project_tiles(tv)
+        gain = C.one_step_gain(net, xv, tv)
+        _log(f"one-step relative error on unseen pairs: {gain:.3f}")
+    else:
+        gain = float("nan")
+    del xv, tv
     val_seeds = list(range(30000, 30000 + args.validation))
     alpha, table = choose_alpha(net, norm, val_seeds, args.n) if val_seeds else (1.0, [])
     rows = evaluate(net, norm, held_seeds, args.n, args.truth, alpha=alpha)
     good = [r for r in rows if r["finite"]]
     summary = dict(
-        alpha=alpha, alpha_table=table,
+        alpha=alpha, alpha_table=table, one_step_relative_error=gain,
         pairs_seconds=t_gen, train_seconds=t_train, iters=args.iters, batch=args.batch,
         train_seeds=len(train_seeds), heldout_seeds=len(held_seeds), loss_first=losses[0][1],
         loss_last=losses[-1][1],
