@@ -180,6 +180,68 @@ def run_reference_arm(args):
     return 0
 
 
+def other_configs(peaks):
+    """The other workloads of the suite, measured once each after the
+    headline (device time from CUDA events inside the library): 1D acoustics
+    (800 cells, 10 frames to t=1), 3D heterogeneous acoustics (256^3, the
+    first frame t=0..0.1, FP64 reference order and FP32) and the batched 2D
+    Euler ensemble (256 instances, sides log-uniform in 128..1024, to
+    t=0.25)."""
+    from classic_b200 import problems
+    from classic_b200.solver import BatchSolver, Solver
+    out = {}
+    try:
+        rd, solver, params, q0, _ = problems.acoustics_1d_config()
+        s = Solver(rd.clawdata, solver, params)
+        s.set_q(q0)
+        t, dt, steps, ms = 0.0, float(rd.clawdata.dt_initial), 0, 0.0
+        for _ in range(10):
+            info, st = s.advance(t, t + 0.1, dt)
+            t, dt = st["t_reached"], st["dt_next"]
+            steps += st["steps_taken"]
+            ms += st["device_ms"]
+        s.close()
+        out["acoustics_1d_800"] = {"cell_updates_per_s": 800 * steps / (ms * 1e-3), "steps": steps,
+                                   "device_ms": ms, "note": "one CTA runs the whole claw1 loop per frame"}
+    except Exception as e:  # a failed side measurement must not hide the headline
+        out["acoustics_1d_800"] = {"error": str(e)}
+    for prec in ("fp64", "fp32"):
+        key = f"hetero_acoustics_3d_256_{prec}"
+        try:
+            rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=256)
+            s = Solver(rd.clawdata, solver, params, precision=prec)
+            s.set_q(q0)
+            s.set_aux(aux)
+            info, st = s.advance(0.0, 0.1, 0.01)
+            s.close()
+            n3 = 256 ** 3
+            upd = n3 * (st["steps_taken"] + st["steps_rejected"])
+            es = 4 if prec == "fp32" else 8
+            rate = upd / (st["device_ms"] * 1e-3)
+            out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
+                        "device_ms": st["device_ms"],
+                        "hbm_frac_algorithmic": rate * 10 * es / 1e9 / peaks["hbm_gbs"]}
+        except Exception as e:
+            out[key] = {"error": str(e)}
+    try:
+        sizes = problems.euler_ensemble_sizes(256, seed=0)
+        insts = [problems.euler_quadrants(n=nn, seed=1000 + k) for k, nn in enumerate(sizes)]
+        b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4})
+        for k, inst in enumerate(insts):
+            b.set_q(k, inst[3])
+        info, st = b.advance(0.0, 0.25)
+        b.close()
+        upd = sum(nn * nn * (x["steps_taken"] + x["steps_rejected"]) for nn, x in zip(sizes, st))
+        ms = st[0]["device_ms"]
+        out["euler_batch_256"] = {"cell_updates_per_s": upd / (ms * 1e-3), "cell_updates": upd,
+                                  "device_ms": ms, "launches": st[0]["launches"],
+                                  "steps_min_max": [min(x["steps_taken"] for x in st),
+                                                    max(x["steps_taken"] for x in st)]}
+    except Exception as e:
+        out["euler_batch_256"] = {"error": str(e)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -191,6 +253,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other workloads")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -332,6 +395,10 @@ def main():
                                          "fp64_fma": "within 1e-12 relative of fp64, same dt sequence",
                                          "fp32": "within 1e-5 relative of fp64"}[prec]}
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = other_configs(peaks)
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_steps > 0:
         rate, sec, cores = cpu_reference_sample(n, args.cpu_steps)
@@ -362,6 +429,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clk,
             "variants": variants,
+            "other_configs": configs,
         }
         print(json.dumps(line), flush=True)
     s.close()

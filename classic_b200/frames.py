@@ -1,6 +1,6 @@
 """fort.qNNNN / fort.tNNNN frame files in the reference's ASCII format.
 
-Writer: src/2d/out2.f:20-111 (1D: src/1d/out1.f).  Values are written with
+Writer: src/2d/out2.f:20-111 (1D: src/1d/out1.f; 3D: src/3d/out3.f).  Values are written with
 Fortran ``e26.16`` (16 significant digits in 0.d...dE+ee form) after the
 in-place flush of |q| < 1e-99 (src/2d/out2.f:70); the header carries grid
 number, AMR level, mx, my, xlow, ylow, dx, dy, and fort.t carries time, meqn,
@@ -49,7 +49,7 @@ def flush_tiny(q: np.ndarray) -> np.ndarray:
 
 def write_frame(outdir: str, frame: int, t: float, q: np.ndarray, lower, dxs,
                 maux: int = 0, nghost: int = 2) -> tuple[str, str]:
-    """Write fort.qNNNN and fort.tNNNN for a 1D or 2D grid (q: [meqn][my][mx])."""
+    """Write fort.qNNNN and fort.tNNNN for a 1D, 2D or 3D grid (q: [meqn]([mz])([my])[mx])."""
     q = flush_tiny(q)
     meqn = q.shape[0]
     ndim = q.ndim - 1
@@ -65,6 +65,23 @@ def write_frame(outdir: str, frame: int, t: float, q: np.ndarray, lower, dxs,
         for i in range(mx):
             lines.append("".join(fortran_e(q[m, i]) for m in range(meqn)))
         lines.append(" ")
+        lines.append(" ")
+    elif ndim == 3:
+        mz, my, mx = q.shape[1], q.shape[2], q.shape[3]
+        lines.append(_i5(mx) + "                 mx")
+        lines.append(_i5(my) + "                 my")
+        lines.append(_i5(mz) + "                 mz")
+        for d, nm in enumerate(("xlow", "ylow", "zlow")):
+            lines.append(fortran_e(lower[d]) + "    " + nm)
+        for d, nm in enumerate(("dx", "dy", "dz")):
+            lines.append(fortran_e(dxs[d]) + "    " + nm)
+        lines.append("")
+        for k in range(mz):
+            for j in range(my):
+                for i in range(mx):
+                    lines.append("".join(fortran_e(q[m, k, j, i]) for m in range(meqn)))
+                lines.append(" ")
+            lines.append(" ")
         lines.append(" ")
     else:
         my, mx = q.shape[1], q.shape[2]
@@ -92,7 +109,7 @@ def write_frame(outdir: str, frame: int, t: float, q: np.ndarray, lower, dxs,
 
 
 def read_frame(outdir: str, frame: int):
-    """Read fort.qNNNN/fort.tNNNN back: returns (t, q[meqn][my][mx] or [meqn][mx])."""
+    """Read fort.qNNNN/fort.tNNNN back: returns (t, q[meqn]([mz])([my])[mx])."""
     with open(os.path.join(outdir, f"fort.t{frame:04d}")) as f:
         tl = f.read().split("\n")
     t = float(tl[0].split()[0].replace("D", "E"))
@@ -101,17 +118,24 @@ def read_frame(outdir: str, frame: int):
     with open(os.path.join(outdir, f"fort.q{frame:04d}")) as f:
         ql = f.read().split("\n")
     mx = int(ql[2].split()[0])
+    mz = 1
     if ndim == 1:
         start, my = 6, 1
-    else:
+    elif ndim == 2:
         my = int(ql[3].split()[0])
         start = 9
+    else:
+        my = int(ql[3].split()[0])
+        mz = int(ql[4].split()[0])
+        start = 12
     vals = []
     for ln in ql[start:]:
         toks = ln.split()
         if toks:
             vals.extend(float(x.replace("D", "E")) for x in toks)
-    a = np.array(vals, dtype=np.float64).reshape(my * mx, meqn)
+    a = np.array(vals, dtype=np.float64).reshape(mz * my * mx, meqn)
     if ndim == 1:
         return t, a.T.reshape(meqn, mx).copy()
-    return t, a.T.reshape(meqn, my, mx).copy()
+    if ndim == 2:
+        return t, a.T.reshape(meqn, my, mx).copy()
+    return t, a.T.reshape(meqn, mz, my, mx).copy()

@@ -201,34 +201,58 @@ def frame_times(cd: ClawInputData):
     raise ValueError(f"bad output_style {style}")
 
 
-def run(rundata, solver: str, params: dict | None, q0: np.ndarray,
+def run(rundata, solver: str, params: dict | None, q0: np.ndarray | None,
         aux: np.ndarray | None = None, precision: str = "fp64",
         on_frame: Callable[[Frame], None] | None = None, keep_frames: bool = True,
-        flush_tiny: bool = True, solver_obj: Solver | None = None, user_bc: str | None = None):
-    """claw{1,2}ez's frame loop on the GPU.  Returns the list of frames
-    (frame 0 included when output_t0); raises on a nonzero info."""
+        flush_tiny: bool = True, solver_obj: Solver | None = None, user_bc: str | None = None,
+        outdir: str | None = None):
+    """claw{1,2,3}ez's frame loop on the GPU.  Returns the list of frames
+    (frame 0 included when output_t0); raises on a nonzero info.
+
+    With ``outdir`` every output frame is also written as fort.qNNNN /
+    fort.tNNNN (out2.f's format), and a restart run (clawdata.restart)
+    reads its q and start time from the frame clawdata.restart_file names in
+    that directory and continues the frame numbering from it, as claw2ez does
+    (src/2d/claw2ez.f:236-271; dtout keeps the data's t0)."""
+    from . import frames as _frames
     cd = rundata.clawdata if isinstance(rundata, ClawRunData) else rundata
     s = solver_obj or Solver(cd, solver, params, precision, user_bc)
-    q = np.array(q0, dtype=np.float64, copy=True)
+    nd = int(cd.num_dim)
+    lower = [float(cd.lower[d]) for d in range(nd)]
+    dxs = [(float(cd.upper[d]) - float(cd.lower[d])) / float(np.float32(int(cd.num_cells[d])))
+           for d in range(nd)]
+    rest = bool(getattr(cd, "restart", False))
+    iframe0 = 0
+    t0 = float(cd.t0)
+    dtout0 = t0  # claw2ez computes dtout from the data's t0
+    if rest:
+        if outdir is None:
+            raise ValueError("a restart run needs outdir holding the restart frame")
+        iframe0 = int("".join(ch for ch in str(cd.restart_file) if ch.isdigit()) or 0)
+        t0, q = _frames.read_frame(outdir, iframe0)
+    else:
+        q = np.array(q0, dtype=np.float64, copy=True)
     if flush_tiny:
         q[np.abs(q) < 1e-99] = 0.0
     s.set_q(q)
     if aux is not None:
         s.set_aux(aux)
     frames = []
-    t0 = float(cd.t0)
-    if cd.output_t0 or int(cd.output_style) == 2:
+    if not rest and (cd.output_t0 or int(cd.output_style) == 2):
         f0 = Frame(0, t0, q.copy())
+        if outdir is not None:
+            _frames.write_frame(outdir, 0, t0, q, lower, dxs, maux=int(cd.num_aux),
+                                nghost=int(cd.num_ghost))
         if on_frame:
             on_frame(f0)
         if keep_frames:
             frames.append(f0)
     nout, nstepout = frame_times(cd)
     # dtout = (tfinal - t0)/float(nout), src/2d/claw2ez.f:197-199
-    dtout = (float(cd.tfinal) - t0) / float(np.float32(nout)) if int(cd.output_style) == 1 else None
+    dtout = (float(cd.tfinal) - dtout0) / float(np.float32(nout)) if int(cd.output_style) == 1 else None
     tend = t0
     dt = float(cd.dt_initial)
-    for n in range(1, nout + 1):
+    for n in range(iframe0 * nstepout + 1, nout + 1):
         tstart = tend
         style = int(cd.output_style)
         if style == 1:
@@ -251,6 +275,9 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray,
                     q[tiny] = 0.0
                     s.set_q(q)
             fr = Frame(iframe, tend, q, st)
+            if outdir is not None:
+                _frames.write_frame(outdir, iframe, tend, q, lower, dxs, maux=int(cd.num_aux),
+                                    nghost=int(cd.num_ghost))
             if on_frame:
                 on_frame(fr)
             if keep_frames:

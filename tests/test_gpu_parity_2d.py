@@ -206,3 +206,30 @@ def test_fast_fp32_tracks_fp64_all_bcs():
             assert abs(cg - co) <= 1e-7 * co
         assert np.all(rel_diff(g.get_q(), o.get_q()) < 1e-5)
         g.close()
+
+
+def test_frames_written_and_restart_continues(tmp_path):
+    """run() with outdir writes fort.q/fort.t per frame; a restart from frame
+    1 reads that file's q and t and continues frames 2.. exactly as claw2
+    does from that state (checked against the oracle started from the same
+    file)."""
+    from classic_b200 import frames as F
+    from classic_b200.solver import run
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=64, nout=3, tfinal=0.3)
+    out = str(tmp_path)
+    fr = run(rd, solver, params, q0, outdir=out)
+    assert [f.frame for f in fr] == [0, 1, 2, 3]
+    for k in range(4):
+        t, q = F.read_frame(out, k)
+        assert abs(t - fr[k].t) <= 1e-15 and np.allclose(q, fr[k].q, rtol=1e-15, atol=1e-99)
+    rd.clawdata.restart = True
+    rd.clawdata.restart_file = "fort.q0001"
+    fr2 = run(rd, solver, params, None, outdir=out)
+    assert [f.frame for f in fr2] == [2, 3]
+    t1, q1 = F.read_frame(out, 1)
+    o = OracleGrid(rd.clawdata, solver, params)
+    o.set_q(q1)
+    dtout = 0.3 / 3
+    info, st = o.advance(t1, t1 + dtout, float(rd.clawdata.dt_initial))
+    assert info == 0 and st["t_reached"] == fr2[0].t
+    assert same(fr2[0].q, o.get_q())
