@@ -241,10 +241,16 @@ class PairGenerator:
         self.n, self.r, self.gamma, self.tfinal = n, ratio, gamma, tfinal
         self.lib = _lib.load()
 
-    def run(self, seed, norm: Norm, keep_steps, x_out, t_out, slot0, cfl_desired=0.9):
+    def run(self, seed, norm: Norm, keep_steps, x_out, t_out, slot0, cfl_desired=0.9,
+            net=None, alpha=1.0, gamma_tol=1e-10):
         """Advance one instance to tfinal; for the coarse steps whose index is
         in keep_steps write features / targets into x_out[slot] / t_out[slot].
-        Returns (steps, slots used)."""
+        Without `net` every coarse step starts from the block-averaged fine
+        state (teacher forcing).  With `net` the coarse grid runs its own
+        corrected trajectory (alpha times the network after each step), so
+        the pairs cover the states the corrector meets at inference, with
+        targets from the fine run at the same times.  Returns (steps, slots
+        used)."""
         torch = _torch()
         n, r = self.n, self.r
         rdf, solver, params, qf0, _ = problems.euler_quadrants(n=n * r, seed=seed, gamma=self.gamma)
@@ -259,32 +265,52 @@ class PairGenerator:
         qfa = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
         step, slot = 0, slot0
         keep = set(keep_steps)
-        while t < self.tfinal:
-            dt = min(dt, self.tfinal - t)
+        if net is not None:
+            xin = torch.empty((1, n, n, 16), dtype=torch.bfloat16, device="cuda")
+            flags = torch.empty(((n + 15) // 16) ** 2, dtype=torch.int32, device="cuda")
+            va = norm.values.copy()
+            va[12:16] = va[12:16] / max(alpha, 1e-30)
+            nda = Norm(va).device()
             qf, ldf, fsf = q_view(fine)
             qc, ldc, fsc = q_view(coarse)
             check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qc), ldc, fsc, n, n, r, 4, st),
                   "nn_block_average")
+        while t < self.tfinal:
+            dt = min(dt, self.tfinal - t)
+            qf, ldf, fsf = q_view(fine)
+            qc, ldc, fsc = q_view(coarse)
+            if net is None:
+                check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qc), ldc, fsc, n, n, r, 4, st),
+                      "nn_block_average")
             qold.copy_(qc)
             cfl = coarse.step(dt)
             if cfl > 1.0:  # rejected: retry from the same state with a smaller dt
+                qn, _, _ = q_view(coarse)
+                qn.copy_(qold)
                 dt = dt * cfl_desired / cfl
                 continue
-            qs, _, _ = q_view(coarse)
+            qs, ldc, fsc = q_view(coarse)
             info, sf = fine.advance(t, t + dt, dtf)
             if info != 0:
                 raise RuntimeError(f"fine run info {info}")
             dtf = sf["dt_next"]
+            qsc = qs.contiguous()
             if step in keep:
                 qf, _, _ = q_view(fine)
                 check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qfa), n, n * n, n, n, r, 4, st),
                       "nn_block_average")
-                qsc = qs.contiguous()
                 check(self.lib.nn_features(_p(qold), _p(qsc), n, n * n, n, n, slot, _p(nd), _p(x_out),
                                            st), "nn_features")
                 check(self.lib.nn_residual_target(_p(qfa), _p(qsc), n, n * n, n, n, slot, _p(nd),
                                                   _p(t_out), st), "nn_residual_target")
                 slot += 1
+            if net is not None:
+                check(self.lib.nn_features(_p(qold), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(xin), st),
+                      "nn_features")
+                out = net.forward(xin)
+                check(self.lib.nn_apply_correction(_p(qs), ldc, fsc, n, n, _p(out), 16, _p(nda),
+                                                   self.gamma, gamma_tol, _p(flags), st),
+                      "nn_apply_correction")
             t = sf["t_reached"]
             dt = dt * cfl_desired / cfl if cfl > 0 else dt
             step += 1

@@ -30,7 +30,7 @@ def _log(*a):
     print(*a, flush=True)
 
 
-def generate(seeds, norm, n, keep, rng):
+def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0):
     torch = C._torch()
     total = len(seeds) * keep
     x = torch.empty((total, n, n, 16), dtype=torch.bfloat16, device="cuda")
@@ -39,10 +39,10 @@ def generate(seeds, norm, n, keep, rng):
     used = 0
     steps_all = []
     for seed in seeds:
-        # the steps kept: spread over the run (about n steps to t_final at 256^2)
-        est = int(0.9 * n)
+        # the steps kept: spread over the run (90..250 coarse steps to t_final at 256^2)
+        est = int(0.6 * n)
         kept = sorted(rng.choice(np.arange(2, est), size=keep, replace=False).tolist())
-        steps, k = gen.run(seed, norm, kept, x, t, used)
+        steps, k = gen.run(seed, norm, kept, x, t, used, net=net, alpha=alpha)
         if k and not (torch.isfinite(x[used:used + k].float()).all() and
                       torch.isfinite(t[used:used + k]).all()):
             k = 0  # a run that left the physical states: drop its pairs
@@ -125,6 +125,10 @@ def main(argv=None):
     ap.add_argument("--clip", type=float, default=5.0, help="clip targets at +-clip std")
     ap.add_argument("--validation", type=int, default=4)
     ap.add_argument("--huber", type=float, default=1.0, help="Huber delta (0: MSE)")
+    ap.add_argument("--rounds", type=int, default=2,
+                    help="on-policy rounds: pairs from corrected trajectories of new seeds")
+    ap.add_argument("--round-seeds", type=int, default=128)
+    ap.add_argument("--round-iters", type=int, default=6000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
@@ -149,6 +153,25 @@ def main(argv=None):
                      log=lambda it, l: _log(f"iter {it} loss {l:.4e}"))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
+    # on-policy rounds: pairs along the corrected coarse trajectories, where
+    # the network's own errors have moved the state, then more training on
+    # all pairs (DAgger)
+    for rnd in range(args.rounds):
+        seeds_r = list(range(50000 + 1000 * rnd, 50000 + 1000 * rnd + args.round_seeds))
+        xr, tr_, _ = generate(seeds_r, norm, args.n, args.keep, rng, net=net, alpha=0.5)
+        if args.clip > 0:
+            tr_.clamp_(-args.clip, args.clip)
+        C.project_tiles(tr_)
+        x = torch.cat([x, xr])
+        t = torch.cat([t, tr_])
+        del xr, tr_
+        _log(f"round {rnd + 1}: {x.shape[0]} pairs")
+        t1 = time.perf_counter()
+        losses += C.train(net, x, t, iters=args.round_iters, batch=args.batch, lr=args.lr * 0.5,
+                          seed=args.seed + rnd + 1, noise=args.noise, delta=args.huber,
+                          log=lambda it, l: _log(f"round {rnd + 1} iter {it} loss {l:.4e}"))
+        torch.cuda.synchronize()
+        t_train += time.perf_counter() - t1
     del x, t
     # one-step skill on pairs of unseen seeds (same scaling and projection)
     xv, tv, _ = generate(list(range(40000, 40004)), C.Norm(C.default_norm().values), args.n, 4, rng)
