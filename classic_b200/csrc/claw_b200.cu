@@ -198,6 +198,7 @@ template <typename real>
 std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
     const int id = cfg.solver_id;
     if (cfg.num_dim == 3) return make_runner3d(cfg);
+    if (cfg.dimensional_split > 0) return make_split_runner(cfg);
     if (cfg.precision != CLAW_FP64) {
         // fused / FP32 arithmetic: constant-coefficient acoustics runs in
         // characteristic variables when the method allows it
@@ -302,7 +303,10 @@ static int validate(const claw_config* c, SolverShape* sh) {
             return fail(CLAW_E_INVALID, "periodic BCs must be set on both sides");
     }
     if (c->order < 1 || c->order > 2) return fail(CLAW_E_INVALID, "order must be 1 or 2");
-    if (c->dimensional_split != 0) return fail(CLAW_E_UNSUPPORTED, "dimensional splitting is not built");
+    if (c->dimensional_split < 0 || c->dimensional_split > 2)
+        return fail(CLAW_E_INVALID, "dimensional_split must be 0 (unsplit), 1 (Godunov) or 2 (Strang)");
+    if (c->dimensional_split != 0 && c->num_dim == 1)
+        return fail(CLAW_E_INVALID, "dimensional splitting needs 2 or 3 dimensions");
     if (c->source_split != 0) return fail(CLAW_E_UNSUPPORTED, "source terms are not built");
     if (c->capa_index < 0) return fail(CLAW_E_INVALID, "capa_index < 0");
     for (int k = 0; k < c->num_waves; ++k)
@@ -491,6 +495,7 @@ int claw_step(claw_handle* h, double dt, double* cfl) {
     c->dt = dt;
     c->cur = h->cur;
     c->maxn = 1;
+    c->cfl_max = h->cfg.cfl_max;  // dimensional splitting stops at a sweep above it
     c->t = c->told = h->t_now;
     int rc = push_ctl(h);
     if (rc) return rc;
@@ -557,8 +562,10 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
     }
     if (!info && cfg.dt_variable && cfg.cfl_desired > cfg.cfl_max) info = 3;
     if (!info && cfg.capa_index > cfg.num_aux) info = 5;
-    if (!info && cfg.order < cfg.transverse_waves && cfg.num_dim == 2) info = 6;
-    if (!info && cfg.num_dim == 3) {
+    // with dimensional splitting method(3) < 0 passes both checks
+    const bool split = cfg.dimensional_split > 0;
+    if (!info && !split && cfg.order < cfg.transverse_waves && cfg.num_dim == 2) info = 6;
+    if (!info && !split && cfg.num_dim == 3) {
         // src/3d/chkmth.f: the unsplit transverse codes allowed per order
         const int t3 = cfg.transverse_waves;
         const bool ok = t3 == 0 || t3 == 10 || t3 == 11 ||

@@ -26,6 +26,8 @@ struct ClawCtl {
     int dt_variable;
     int err;                       // device error flags (CTL_ERR_*)
     int pad;
+    unsigned long long cfl_sweep[2];  // dimensional splitting: Courant maxima of the
+                                      // y-sweep and of Strang's last x-sweep
 };
 
 enum { CTL_ADVANCE = 0, CTL_SINGLE = 1 };

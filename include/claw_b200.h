@@ -82,7 +82,7 @@ typedef struct claw_config {
     int dt_variable;          /* method(1)                                         */
     int order;                /* method(2): 1 or 2                                 */
     int transverse_waves;     /* method(3): 0,1,2 (2D); 0,10,11,20,21,22 (3D)      */
-    int dimensional_split;    /* 0 unsplit (only unsplit is built)                 */
+    int dimensional_split;    /* 0 unsplit, 1 Godunov, 2 Strang (3D: Godunov)      */
     int verbosity;            /* method(4)                                         */
     int source_split;         /* method(5): 0 (source terms are not built)         */
     int use_fwaves;
@@ -138,7 +138,12 @@ int claw_set_aux(claw_handle* h, const double* aux);
  * src/2d/step2.f90:2-251; bc3 + step3 in 3D, src/3d/step3.f90:3-873).
  * Writes the Courant number to *cfl and makes the new q current; no
  * accept/reject.  The step starts at the time the last advance reached
- * (0 after claw_create), advanced by dt per claw_step. */
+ * (0 after claw_create), advanced by dt per claw_step.  With dimensional
+ * splitting (dimensional_split 1 or 2) the step is dimsp2 / dimsp3
+ * (src/2d/dimsp2.f:1-99, src/3d/dimsp3.f:1-87): when a sweep's Courant
+ * number exceeds cfl_max, *cfl is that sweep's number as dimsp2 returns it;
+ * the state is then the whole split step (dimsp2 stops part-way, and claw2
+ * discards the state either way). */
 int claw_step(claw_handle* h, double dt, double* cfl);
 
 /* Advance from tstart to tend with claw2's variable/fixed dt control,

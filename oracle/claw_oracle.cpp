@@ -11,6 +11,7 @@
 //   step2    : src/2d/step2.f90:2-251
 //   bc2      : src/2d/bc2.f:4-215
 //   claw2    : src/2d/claw2.f:494-784            (dt / CFL control loop)
+//   dimsp2   : src/2d/dimsp2.f, src/2d/step2ds.f90 (dimensional splitting)
 //   step1    : src/1d/step1.f90:4-170
 //   bc1      : src/1d/bc1.f
 //   claw1    : src/1d/claw1.f:394-583
@@ -18,6 +19,7 @@
 //   flux3    : src/3d/flux3.f90:4-612
 //   bc3      : src/3d/bc3.f (+ the piston BC of examples/acoustics_3d_heterogeneous/bc3.f)
 //   claw3    : src/3d/claw3.f:738-928
+//   dimsp3   : src/3d/dimsp3.f, src/3d/step3ds.f90 (dimensional splitting)
 // Pins (tests/test_oracle_golden.py): the 3D regression sums are reproduced
 // exactly, the 1D heterogeneous sums bit for bit, the 1D example to 1e-16.
 // 2D Euler (Roe + Harten-Hyman entropy fix): parity unpinned -- the reference
@@ -660,6 +662,118 @@ int orc_step2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const dou
     return 0;
 }
 
+// ----------------------------------------------------------------- step2ds ---
+// src/2d/step2ds.f90:1-275: one directional sweep of dimensional splitting.
+// ids = 1: x-slices over every row j = 1-mbc..my+mbc (ghost rows included, so
+// the following y-sweep sees x-updated ghost rows); ids = 2: y-slices over
+// every column i = 1-mbc..mx+mbc.  Only the cells 1..mx (1..my) of each slice
+// are updated; flux2 returns before its transverse part (method(3) < 0).
+// qold supplies the slices and may alias qnew (each slice is gathered before
+// its own update, and slices do not overlap).
+int orc_step2ds(int meqn, int mwaves, int maux, int mbc, int mx, int my, const double* qold,
+                double* qnew, const double* aux, double dx, double dy, double dt,
+                const int* method, const int* mthlim, int ids, int use_fwave, double* cfl_out) {
+    rpn2_t rpn2;
+    rpt2_t rpt2;
+    if (!pick2(g_solver, &rpn2, &rpt2)) return -1;
+    const int maxm = std::max(mx, my);
+    const int n = maxm + 2 * mbc;
+    const int nx = mx + 2 * mbc;
+    auto at = [&](int m, int i, int j) {
+        return (size_t)(m - 1) + (size_t)meqn * ((i - (1 - mbc)) + (size_t)nx * (j - (1 - mbc)));
+    };
+    auto A = [&](int ma, int i, int j) {
+        return aux[(ma - 1) + maux * ((i - (1 - mbc)) + nx * (j - (1 - mbc)))];
+    };
+    std::vector<double> qadd(meqn * n), fadd(meqn * n), gadd(2 * meqn * n), q1d(meqn * n);
+    std::vector<double> dtdx1d(n), dtdy1d(n), aux1(std::max(maux, 1) * n),
+        aux2(std::max(maux, 1) * n), aux3(std::max(maux, 1) * n);
+    std::vector<double> wave(meqn * mwaves * n), s(mwaves * n), amdq(meqn * n), apdq(meqn * n),
+        cqxx(meqn * n), bmasdq(meqn * n), bpasdq(meqn * n);
+    const Slice sl{meqn, 1 - mbc}, sa{maux, 1 - mbc};
+    const int index_capa = method[5];
+    double cfl = 0.0;
+    const double dtdx = dt / dx, dtdy = dt / dy;
+    if (index_capa == 0)
+        for (int i = 0; i < n; ++i) { dtdx1d[i] = dtdx; dtdy1d[i] = dtdy; }
+    const int nslice = ids == 1 ? my : mx;   // slices across
+    const int mlen = ids == 1 ? mx : my;     // cells along
+    const double dtd = ids == 1 ? dtdx : dtdy;
+    double* dtd1d = ids == 1 ? dtdx1d.data() : dtdy1d.data();
+    for (int k = 1 - mbc; k <= nslice + mbc; ++k) {
+        // (i, j) of cell l of slice k
+        auto ij = [&](int l, int& i, int& j) {
+            if (ids == 1) { i = l; j = k; } else { i = k; j = l; }
+        };
+        for (int l = 1 - mbc; l <= mlen + mbc; ++l) {
+            int i, j;
+            ij(l, i, j);
+            for (int m = 1; m <= meqn; ++m) q1d[sl.at(m, l)] = qold[at(m, i, j)];
+        }
+        if (index_capa > 0)
+            for (int l = 1 - mbc; l <= mlen + mbc; ++l) {
+                int i, j;
+                ij(l, i, j);
+                dtd1d[l - (1 - mbc)] = dtd / A(index_capa, i, j);
+            }
+        if (maux > 0)
+            for (int l = 1 - mbc; l <= mlen + mbc; ++l) {
+                int i, j;
+                ij(l, i, j);
+                for (int ma = 1; ma <= maux; ++ma) aux2[sa.at(ma, l)] = A(ma, i, j);
+            }
+        double cfl1d;
+        flux2(ids, maxm, meqn, mwaves, maux, mbc, mlen, q1d.data(), dtd1d, aux1.data(),
+              aux2.data(), aux3.data(), method, mthlim, qadd.data(), fadd.data(), gadd.data(),
+              &cfl1d, wave.data(), s.data(), amdq.data(), apdq.data(), cqxx.data(),
+              bmasdq.data(), bpasdq.data(), rpn2, rpt2, use_fwave != 0);
+        cfl = std::fmax(cfl, cfl1d);
+        for (int l = 1; l <= mlen; ++l) {
+            int i, j;
+            ij(l, i, j);
+            for (int m = 1; m <= meqn; ++m) {
+                double& qn = qnew[at(m, i, j)];
+                if (index_capa == 0)
+                    qn = qn + qadd[sl.at(m, l)] - dtd * (fadd[sl.at(m, l + 1)] - fadd[sl.at(m, l)]);
+                else
+                    qn = qn + qadd[sl.at(m, l)] -
+                         dtd * (fadd[sl.at(m, l + 1)] - fadd[sl.at(m, l)]) / A(index_capa, i, j);
+            }
+        }
+    }
+    *cfl_out = cfl;
+    return 0;
+}
+
+// ------------------------------------------------------------------ dimsp2 ---
+// src/2d/dimsp2.f:1-99: Godunov (method(3) = -1: x by dt, then y by dt) or
+// Strang (method(3) = -2: x by dt/2, y by dt, x by dt/2) splitting.  A sweep
+// whose Courant number exceeds cflv(1) ends the step with that number.
+int orc_dimsp2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const double* qold,
+               double* qnew, const double* aux, double dx, double dy, double dt,
+               const int* method, const int* mthlim, const double* cflv, int use_fwave,
+               double* cfl_out) {
+    const double dt2 = dt / 2.0;
+    double cflx, cfly;
+    int rc = orc_step2ds(meqn, mwaves, maux, mbc, mx, my, qold, qnew, aux, dx, dy,
+                         method[2] == -2 ? dt2 : dt, method, mthlim, 1, use_fwave, &cflx);
+    if (rc) return rc;
+    if (cflx > cflv[0]) { *cfl_out = cflx; return 0; }
+    rc = orc_step2ds(meqn, mwaves, maux, mbc, mx, my, qnew, qnew, aux, dx, dy, dt, method,
+                     mthlim, 2, use_fwave, &cfly);
+    if (rc) return rc;
+    double cfl = std::fmax(cflx, cfly);
+    if (method[2] == -2) {
+        if (cfly > cflv[0]) { *cfl_out = cfly; return 0; }
+        rc = orc_step2ds(meqn, mwaves, maux, mbc, mx, my, qnew, qnew, aux, dx, dy, dt2, method,
+                         mthlim, 1, use_fwave, &cflx);
+        if (rc) return rc;
+        cfl = std::fmax(cfl, cflx);
+    }
+    *cfl_out = cfl;
+    return 0;
+}
+
 // -------------------------------------------------------------------- bc2 ---
 // src/2d/bc2.f:4-215.  mthbc: 1 extrap, 2 periodic, 3 wall; order L, R, B, T.
 // Returns -1 for a user BC (mthbc=0), which the reference stops on.
@@ -750,8 +864,12 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
         for (;;) {
             if (orc_bc2(meqn, mbc, mx, my, q, mthbc) != 0) { info = -2; goto done; }
             std::memcpy(qwork.data(), q, nq * sizeof(double));
-            if (orc_step2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q, aux, dx, dy, dt,
-                          method, mthlim, use_fwaves, &cfl) != 0) {
+            const int rc = method[2] >= 0
+                               ? orc_step2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q, aux,
+                                           dx, dy, dt, method, mthlim, use_fwaves, &cfl)
+                               : orc_dimsp2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q, aux,
+                                            dx, dy, dt, method, mthlim, cflv, use_fwaves, &cfl);
+            if (rc != 0) {
                 info = -1;
                 goto done;
             }
@@ -1225,6 +1343,96 @@ int orc_step3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, c
     return 0;
 }
 
+// ----------------------------------------------------------------- step3ds ---
+// src/3d/step3ds.f90:3-408: one directional sweep of dimensional splitting
+// (idir 1 = x, 2 = y, 3 = z).  The slices cover one ghost layer across
+// (x-sweeps: j = 0..my+1, k = 0..mz+1, and likewise for y and z); each slice
+// updates its cells 1..len with qadd and fadd only (flux3 returns before the
+// transverse part when method(3) < 0).  qold may alias qnew.
+int orc_step3ds(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz,
+                const double* qold, double* qnew, const double* aux, double dx, double dy,
+                double dz, double dt, const int* method, const int* mthlim, int idir,
+                int use_fwave, double* cfl_out) {
+    if (g_solver != ORC_VC_ACOUSTICS_3D || maux < 2) return -1;
+    if (method[5] != 0) return -3;  // capacity not restated for 3D
+    const int nx = mx + 2 * mbc, ny = my + 2 * mbc;
+    const int maxm = std::max(mx, std::max(my, mz));
+    const int n1 = maxm + 2 * mbc;
+    auto idx = [&](int i, int j, int k) {
+        return (size_t)(i - (1 - mbc)) + (size_t)nx * ((j - (1 - mbc)) + (size_t)ny * (k - (1 - mbc)));
+    };
+    std::vector<double> q1d(meqn * n1), dtd1d(n1), qadd(meqn * n1), fadd(meqn * n1),
+        gadd(meqn * 6 * n1), hadd(meqn * 6 * n1), x2(maux * n1 * 3), xdummy(maux * n1 * 3, 0.0);
+    const Slice Q{meqn, 1 - mbc};
+    const int dims[3] = {mx, my, mz};
+    const double dtd[3] = {dt / dx, dt / dy, dt / dz};
+    const int dn = idir - 1, d1 = trans_dir(idir, 2) - 1, d2 = trans_dir(idir, 3) - 1;
+    const int len = dims[dn];
+    const double tn = dtd[dn];
+    for (int i = 0; i < n1; ++i) dtd1d[i] = tn;
+    const int outer = std::max(d1, d2), inner = std::min(d1, d2);
+    double cfl = 0.0;
+    for (int so = 0; so <= dims[outer] + 1; ++so)
+        for (int si = 0; si <= dims[inner] + 1; ++si) {
+            int P[3];
+            P[outer] = so;
+            P[inner] = si;
+            auto cell = [&](int a, int de2, int* c) {
+                c[dn] = a;
+                c[d1] = P[d1];
+                c[d2] = P[d2] + de2;
+            };
+            for (int a = 1 - mbc; a <= len + mbc; ++a) {
+                int c[3];
+                cell(a, 0, c);
+                for (int m = 1; m <= meqn; ++m) q1d[Q.at(m, a)] = qold[(m - 1) + meqn * idx(c[0], c[1], c[2])];
+            }
+            // only aux2 is gathered (its e2 offsets -1..1); flux3 reads its middle
+            for (int a = 1 - mbc; a <= len + mbc; ++a)
+                for (int l = -1; l <= 1; ++l)
+                    for (int ma = 1; ma <= maux; ++ma) {
+                        int c[3];
+                        cell(a, l, c);
+                        x2[(ma - 1) + maux * ((a - (1 - mbc)) + n1 * (l + 1))] =
+                            aux[(ma - 1) + maux * idx(c[0], c[1], c[2])];
+                    }
+            const Aux3 A2{x2.data(), maux, 1 - mbc, n1}, AD{xdummy.data(), maux, 1 - mbc, n1};
+            double cfl1d;
+            flux3(idir, meqn, mwaves, mbc, len, q1d.data(), dtd1d.data(), dtd[d1], dtd[d2], AD,
+                  A2, AD, method, mthlim, qadd.data(), fadd.data(), gadd.data(), hadd.data(),
+                  &cfl1d, use_fwave != 0);
+            cfl = std::fmax(cfl, cfl1d);
+            for (int a = 1; a <= len; ++a) {
+                int c[3];
+                cell(a, 0, c);
+                for (int m = 1; m <= meqn; ++m) {
+                    double& v = qnew[(m - 1) + meqn * idx(c[0], c[1], c[2])];
+                    v = v + qadd[Q.at(m, a)] - tn * (fadd[Q.at(m, a + 1)] - fadd[Q.at(m, a)]);
+                }
+            }
+        }
+    *cfl_out = cfl;
+    return 0;
+}
+
+// ------------------------------------------------------------------ dimsp3 ---
+// src/3d/dimsp3.f:1-87: Godunov splitting only (x, y, z by dt each); a sweep
+// whose Courant number exceeds cflv(1) ends the step with that number.
+int orc_dimsp3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz,
+               const double* qold, double* qnew, const double* aux, double dx, double dy,
+               double dz, double dt, const int* method, const int* mthlim, const double* cflv,
+               int use_fwave, double* cfl_out) {
+    double c[3];
+    for (int d = 1; d <= 3; ++d) {
+        const int rc = orc_step3ds(meqn, mwaves, maux, mbc, mx, my, mz, d == 1 ? qold : qnew, qnew,
+                                   aux, dx, dy, dz, dt, method, mthlim, d, use_fwave, &c[d - 1]);
+        if (rc) return rc;
+        if (d < 3 && c[d - 1] > cflv[0]) { *cfl_out = c[d - 1]; return 0; }
+    }
+    *cfl_out = std::fmax(std::fmax(c[0], c[1]), c[2]);
+    return 0;
+}
+
 // claw3 (src/3d/claw3.f:738-928): the control flow of claw2 around bc3/step3.
 int orc_claw3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, double* q,
               const double* aux, double xlower, double ylower, double dx, double dy, double dz,
@@ -1254,8 +1462,12 @@ int orc_claw3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, d
         for (;;) {
             if (orc_bc3(meqn, mbc, mx, my, mz, q, mthbc, told, xlower, ylower, dx, dy) != 0) { info = -2; goto done; }
             std::memcpy(qwork.data(), q, nq * sizeof(double));
-            const int rc = orc_step3(meqn, mwaves, maux, mbc, mx, my, mz, qwork.data(), q, aux, dx, dy,
-                                     dz, dt, method, mthlim, use_fwaves, &cfl);
+            const int rc = method[2] >= 0
+                               ? orc_step3(meqn, mwaves, maux, mbc, mx, my, mz, qwork.data(), q,
+                                           aux, dx, dy, dz, dt, method, mthlim, use_fwaves, &cfl)
+                               : orc_dimsp3(meqn, mwaves, maux, mbc, mx, my, mz, qwork.data(), q,
+                                            aux, dx, dy, dz, dt, method, mthlim, cflv, use_fwaves,
+                                            &cfl);
             if (rc != 0) { info = rc; goto done; }
             t = told + dt;
             if (cfl <= cflv[0]) { cflmax = std::fmax(cfl, cflmax); break; }

@@ -80,6 +80,12 @@ def _load(variant: str):
     lib.orc_step3.restype = ctypes.c_int
     lib.orc_bc3.argtypes = [ctypes.c_int] * 5 + [_D, _I] + [ctypes.c_double] * 5
     lib.orc_bc3.restype = ctypes.c_int
+    lib.orc_dimsp2.argtypes = [ctypes.c_int] * 6 + [_D, _D, _D, ctypes.c_double, ctypes.c_double,
+                                                    ctypes.c_double, _I, _I, _D, ctypes.c_int, _D]
+    lib.orc_dimsp2.restype = ctypes.c_int
+    lib.orc_dimsp3.argtypes = [ctypes.c_int] * 7 + [_D, _D, _D] + [ctypes.c_double] * 4 + [
+        _I, _I, _D, ctypes.c_int, _D]
+    lib.orc_dimsp3.restype = ctypes.c_int
     return lib
 
 
@@ -96,7 +102,8 @@ def _codes(cd):
     method[2] = cd.transverse_code() if nd > 1 else 0
     split = cd.split_code() if nd > 1 else 0
     if split > 0:
-        method[2] = -split
+        # src/2d/claw2ez.f:126 (-1 Godunov, -2 Strang); src/3d/claw3ez.f:136 (always -1)
+        method[2] = -split if nd == 2 else -1
     method[3] = int(cd.verbosity)
     method[4] = cd.source_code()
     method[5] = int(cd.capa_index)
@@ -159,6 +166,9 @@ class OracleGrid:
         if self.maux:
             self.af[...] = np.moveaxis(np.asarray(aux, dtype=np.float64), 0, -1)
 
+    def _cflv(self):
+        return np.array([float(self.cd.cfl_max), float(self.cd.cfl_desired), 0.0, 0.0])
+
     def advance(self, tstart, tend, dt_initial):
         """claw{1,2}: returns (info, stats dict)."""
         self._set_solver()
@@ -200,20 +210,34 @@ class OracleGrid:
             mx, my = self.cells
             self.lib.orc_bc2(self.meqn, self.mbc, mx, my, _p(self.qf), _p(self.mthbc, _I))
             qold = self.qf.copy()
-            rc = self.lib.orc_step2(self.meqn, self.mwaves, self.maux, self.mbc, mx, my,
-                                    _p(qold), _p(self.qf), _p(self.af), self.dxs[0], self.dxs[1],
-                                    float(dt), _p(self.method, _I), _p(self.mthlim, _I),
-                                    self.use_fwaves, ctypes.byref(cfl))
+            if self.method[2] >= 0:
+                rc = self.lib.orc_step2(self.meqn, self.mwaves, self.maux, self.mbc, mx, my,
+                                        _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                        self.dxs[1], float(dt), _p(self.method, _I),
+                                        _p(self.mthlim, _I), self.use_fwaves, ctypes.byref(cfl))
+            else:
+                rc = self.lib.orc_dimsp2(self.meqn, self.mwaves, self.maux, self.mbc, mx, my,
+                                         _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                         self.dxs[1], float(dt), _p(self.method, _I),
+                                         _p(self.mthlim, _I), _p(self._cflv()), self.use_fwaves,
+                                         ctypes.byref(cfl))
         elif self.nd == 3:
             mx, my, mz = self.cells
             self.lib.orc_bc3(self.meqn, self.mbc, mx, my, mz, _p(self.qf), _p(self.mthbc, _I),
                              float(t), float(self.cd.lower[0]), float(self.cd.lower[1]),
                              self.dxs[0], self.dxs[1])
             qold = self.qf.copy()
-            rc = self.lib.orc_step3(self.meqn, self.mwaves, self.maux, self.mbc, mx, my, mz,
-                                    _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
-                                    self.dxs[1], self.dxs[2], float(dt), _p(self.method, _I),
-                                    _p(self.mthlim, _I), self.use_fwaves, ctypes.byref(cfl))
+            if self.method[2] >= 0:
+                rc = self.lib.orc_step3(self.meqn, self.mwaves, self.maux, self.mbc, mx, my, mz,
+                                        _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                        self.dxs[1], self.dxs[2], float(dt), _p(self.method, _I),
+                                        _p(self.mthlim, _I), self.use_fwaves, ctypes.byref(cfl))
+            else:
+                rc = self.lib.orc_dimsp3(self.meqn, self.mwaves, self.maux, self.mbc, mx, my, mz,
+                                         _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                         self.dxs[1], self.dxs[2], float(dt),
+                                         _p(self.method, _I), _p(self.mthlim, _I),
+                                         _p(self._cflv()), self.use_fwaves, ctypes.byref(cfl))
         else:
             (mx,) = self.cells
             self.lib.orc_bc1(self.meqn, self.mbc, mx, _p(self.qf), _p(self.mthbc, _I))
