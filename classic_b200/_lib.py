@@ -59,7 +59,9 @@ class ClawConfig(ctypes.Structure):
         ("solver_id", ctypes.c_int),
         ("solver_params", ctypes.c_double * 8),
         ("precision", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("source_id", ctypes.c_int),
+        ("source_ndim", ctypes.c_int),
+        ("reserved", ctypes.c_int * 5),
     ]
 
 

@@ -74,7 +74,7 @@ namespace {
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
 // ------------------------------------------------------------------ runners ---
-template <class S, class M>
+template <class S, class M, bool SRC = false>
 struct Runner2D : Runner {
     Step2Args<S> args;
     int grid = 1, smem = 0;
@@ -105,6 +105,10 @@ struct Runner2D : Runner {
         args.dx = g.dx;
         args.dy = g.dy;
         args.ctl = g.ctl;
+        args.src_split = (SRC && cfg.source_id == CLAW_SOURCE_RADIAL) ? cfg.source_split : 0;
+        args.src_nd1 = (double)(cfg.source_ndim - 1);
+        args.src_bulk = cfg.solver_params[1];
+        args.xlower = cfg.lower[0];
         for (int k = 0; k < 2; ++k) {
             int rc = make_map3(&args.tmq[k], g.q[k], g.es, g.mx, g.my, S::meqn, g.ld, g.fstride,
                                R::W, 1, S::meqn);
@@ -116,12 +120,12 @@ struct Runner2D : Runner {
             if (rc) return rc;
         }
         smem = R::SMEM;
-        CUDA_TRY(cudaFuncSetAttribute(step2_kernel<S, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(cudaFuncSetAttribute(step2_kernel<S, M, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_kernel<S, M>,
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_kernel<S, M, SRC>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "step2 kernel cannot be resident on an SM");
         args.units = (long long)args.nstrips * g.my;
@@ -136,7 +140,7 @@ struct Runner2D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_kernel<S, M><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        step2_kernel<S, M, SRC><<<grid, 32 * WARPS2D, smem, s>>>(args);
         return cudaGetLastError();
     }
 };
@@ -163,8 +167,15 @@ struct Runner1D : Runner {
         args.capa = cfg.capa_index;
         args.dx = g.dx;
         args.ctl = g.ctl;
+        args.src_split = cfg.source_id == CLAW_SOURCE_RADIAL ? cfg.source_split : 0;
+        args.src_nd1 = (double)(cfg.source_ndim - 1);
+        args.src_bulk = cfg.solver_params[1];
+        args.xlower = cfg.lower[0];
         smem = step1_smem_bytes<S>(g.mx);
-        if (smem > 200 * 1024)
+        int dev = 0, optin = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (smem + 1024 > optin)
             return fail(CLAW_E_UNSUPPORTED, "1D grid of %d cells exceeds the single-CTA kernel", g.mx);
         CUDA_TRY(cudaFuncSetAttribute(step1_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
@@ -188,6 +199,11 @@ bool all_limiters(const claw_config& cfg, int lim) {
 // f-waves) runs a fully specialised kernel; every other method the generic one.
 template <class S>
 std::unique_ptr<Runner> runner2d(const claw_config& cfg, const S& s) {
+    if constexpr (std::is_same<S, Acoustics2D<typename S::real>>::value) {
+        // the radial source (src/2d/claw2.f:635-738 with 1drad/src1.f) fused into the step
+        if (cfg.source_id == CLAW_SOURCE_RADIAL && cfg.source_split != 0)
+            return std::unique_ptr<Runner>(new Runner2D<S, MethodGeneric2D, true>(s));
+    }
     if (cfg.order == 2 && cfg.transverse_waves == 2 && all_limiters(cfg, 4) &&
         cfg.capa_index == 0 && !cfg.use_fwaves)
         return std::unique_ptr<Runner>(new Runner2D<S, MethodMC2D>(s));
@@ -199,7 +215,8 @@ std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
     const int id = cfg.solver_id;
     if (cfg.num_dim == 3) return make_runner3d(cfg);
     if (cfg.dimensional_split > 0) return make_split_runner(cfg);
-    if (cfg.precision != CLAW_FP64) {
+    const bool source = cfg.source_id != CLAW_SOURCE_NONE && cfg.source_split != 0;
+    if (cfg.precision != CLAW_FP64 && !source) {
         // fused / FP32 arithmetic: constant-coefficient acoustics runs in
         // characteristic variables when the method allows it
         auto r = make_char_runner(cfg);
@@ -307,7 +324,15 @@ static int validate(const claw_config* c, SolverShape* sh) {
         return fail(CLAW_E_INVALID, "dimensional_split must be 0 (unsplit), 1 (Godunov) or 2 (Strang)");
     if (c->dimensional_split != 0 && c->num_dim == 1)
         return fail(CLAW_E_INVALID, "dimensional splitting needs 2 or 3 dimensions");
-    if (c->source_split != 0) return fail(CLAW_E_UNSUPPORTED, "source terms are not built");
+    if (c->source_split < 0 || c->source_split > 2)
+        return fail(CLAW_E_INVALID, "source_split must be 0, 1 (Godunov) or 2 (Strang)");
+    if (c->source_id != CLAW_SOURCE_NONE) {
+        if (c->source_id != CLAW_SOURCE_RADIAL) return fail(CLAW_E_INVALID, "unknown source_id %d", c->source_id);
+        if (c->solver_id != CLAW_SOLVER_ACOUSTICS_1D && c->solver_id != CLAW_SOLVER_ACOUSTICS_2D)
+            return fail(CLAW_E_UNSUPPORTED, "the radial source is built for constant-coefficient acoustics");
+        if (c->source_ndim < 1 || c->source_ndim > 3) return fail(CLAW_E_INVALID, "source_ndim must be 1..3");
+        if (c->lower[0] < 0.0) return fail(CLAW_E_INVALID, "the radial source needs xlower >= 0 (x is the radius)");
+    }
     if (c->capa_index < 0) return fail(CLAW_E_INVALID, "capa_index < 0");
     for (int k = 0; k < c->num_waves; ++k)
         if (c->limiter[k] < 0 || c->limiter[k] > 5) return fail(CLAW_E_INVALID, "invalid limiter %d", c->limiter[k]);

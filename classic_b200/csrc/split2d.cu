@@ -12,7 +12,7 @@
 namespace clawb200 {
 namespace {
 
-template <class S, class M, bool STRANG>
+template <class S, class M, bool STRANG, bool SRC = false>
 struct SplitRunner2D : Runner {
     using L = SplitLayout<S, STRANG>;
     Step2Args<S> args;
@@ -43,6 +43,10 @@ struct SplitRunner2D : Runner {
         args.dx = g.dx;
         args.dy = g.dy;
         args.ctl = g.ctl;
+        args.src_split = (SRC && cfg.source_id == CLAW_SOURCE_RADIAL) ? cfg.source_split : 0;
+        args.src_nd1 = (double)(cfg.source_ndim - 1);
+        args.src_bulk = cfg.solver_params[1];
+        args.xlower = cfg.lower[0];
         for (int k = 0; k < 2; ++k) {
             int rc = make_map3(&args.tmq[k], g.q[k], g.es, g.mx, g.my, S::meqn, g.ld, g.fstride,
                                L::W, 1, S::meqn);
@@ -54,7 +58,7 @@ struct SplitRunner2D : Runner {
             if (rc) return rc;
         }
         smem = L::SMEM;
-        auto kern = split2_kernel<S, M, STRANG>;
+        auto kern = split2_kernel<S, M, STRANG, SRC>;
         CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
@@ -73,13 +77,20 @@ struct SplitRunner2D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        split2_kernel<S, M, STRANG><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        split2_kernel<S, M, STRANG, SRC><<<grid, 32 * WARPS2D, smem, s>>>(args);
         return cudaGetLastError();
     }
 };
 
 template <class S>
 std::unique_ptr<Runner> split_for(const claw_config& cfg, const S& s) {
+    if constexpr (std::is_same<S, Acoustics2D<typename S::real>>::value) {
+        if (cfg.source_id == CLAW_SOURCE_RADIAL && cfg.source_split != 0) {
+            if (cfg.dimensional_split == 2)
+                return std::unique_ptr<Runner>(new SplitRunner2D<S, MethodGeneric2D, true, true>(s));
+            return std::unique_ptr<Runner>(new SplitRunner2D<S, MethodGeneric2D, false, true>(s));
+        }
+    }
     bool mc = cfg.order == 2 && cfg.capa_index == 0 && !cfg.use_fwaves;
     for (int k = 0; k < cfg.num_waves; ++k) mc = mc && cfg.limiter[k] == 4;
     // order 2, MC, no capacity, no f-waves: the specialised policy; the

@@ -26,15 +26,33 @@ struct Step1Args {
     int mthlim[8];
     int order, fwave, capa;
     double dx;
+    // source term (src/1d/claw1.f:486-509): src_split 0 none, 1 Godunov, 2
+    // Strang; the radial term of examples/acoustics_2d_radial/1drad/src1.f
+    int src_split;
+    double src_nd1, src_bulk, xlower;  // ndim - 1, bulk, xlower
     ClawCtl* ctl;
     S solver;
 };
 
+// src1.f:18-23 on cells 0..mx+1 (i = 1..mx+2): p -= dt (ndim-1) bulk / x_i u.
+// Thread tid owns the cells k = tid mod blockDim, as the update phases do.
+template <class S>
+__device__ __forceinline__ void step1_source(const Step1Args<S>& A, typename S::real* qs, int n,
+                                             double dts) {
+    using real = typename S::real;
+    for (int k = threadIdx.x; k < A.mx + 2; k += blockDim.x) {
+        const double xcell = A.xlower + ((double)(k + 1) - 0.5) * A.dx;
+        const double coef = dts * A.src_nd1 * A.src_bulk / xcell;
+        qs[k + 2] = qs[k + 2] - (real)(coef * (double)qs[n + k + 2]);
+    }
+}
+
 template <class S>
 __host__ __device__ constexpr int step1_smem_doubles(int mx) {
-    // q, saved q, aux, dtdx, per-interface wave/s/amdq/apdq/f, reduction
-    return (2 * S::meqn + S::maux + 1) * (mx + 4) +
-           (S::mwaves * S::meqn + S::mwaves + 3 * S::meqn) * (mx + 4) + 32;
+    // q, aux, dtdx, per-interface wave/s/amdq/apdq (f reuses amdq), reduction;
+    // the copy kept for a rejected step lives in the output buffer
+    return (S::meqn + S::maux + 1) * (mx + 4) +
+           (S::mwaves * S::meqn + S::mwaves + 2 * S::meqn) * (mx + 4) + 32;
 }
 
 template <class S>
@@ -52,20 +70,24 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
     const int ne = mx + 4;            // interface e in [-1, mx+1] lives at e+1
     extern __shared__ __align__(16) unsigned char smem_raw[];
     real* qs = reinterpret_cast<real*>(smem_raw);
-    real* qsave = qs + ME * n;
-    real* as = qsave + ME * n;
+    real* as = qs + ME * n;
     real* dtdx = as + MA * n;
     real* wv = dtdx + n;            // [MW][ME][ne]
     real* sv = wv + MW * ME * ne;   // [MW][ne]
     real* amd = sv + MW * ne;       // [ME][ne]
     real* apd = amd + ME * ne;
-    real* fl = apd + ME * ne;       // [ME][ne]
+    real* fl = amd;                 // [ME][ne], once the Godunov update has used amdq
     __shared__ double red[STEP1_THREADS / 32];
     __shared__ double sh_dt, sh_cfl;
     __shared__ int sh_state;  // 0 continue, 1 retry, 2 stop
 
     const int tid = threadIdx.x;
     const int cur = ctl->cur;
+    real* __restrict__ qsave = A.q[cur ^ 1];  // interior copy for a rejected step
+    // a single step (claw_step) is step1 alone: accepted whatever its Courant
+    // number, without the source steps that claw1 wraps around it
+    const bool single = ctl->mode == CTL_SINGLE;
+    const int src_split = single ? 0 : A.src_split;
     const real* qin = A.q[cur];
     for (int i = tid; i < ME * mx; i += blockDim.x) {
         const int m = i / mx, k = i % mx;
@@ -86,7 +108,8 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
     for (int step = 0; step < maxn && !stop; ++step) {
         const double told = t;
         if (told + dt > tend && tstart < tend) dt = tend - told;
-        for (int i = tid; i < ME * n; i += blockDim.x) qsave[i] = qs[i];
+        for (int i = tid; i < ME * mx; i += blockDim.x)
+            qsave[(i / mx) * A.fstride + i % mx] = qs[(i / mx) * n + i % mx + 2];
         __syncthreads();
         for (;;) {
             t = told + dt;
@@ -111,6 +134,10 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
                 else dtdx[k] = (real)(dt / dxd);
             }
             __syncthreads();
+            if (src_split == 2) {  // Strang: dt/2 of source before the step
+                step1_source(A, qs, n, dt / 2.0);
+                __syncthreads();
+            }
             // ---- rp1 at interfaces e = -1 .. mx+1 (src/1d/step1.f90:82) + CFL
             double c_loc = 0.0;
             for (int e = tid - 1; e <= mx + 1; e += blockDim.x) {
@@ -139,6 +166,7 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
                     qs[m * n + k + 2] = (qs[m * n + k + 2] - d * apd[m * ne + k + 1]) - d * amd[m * ne + k + 2];
             }
             if (A.order != 1) {
+                __syncthreads();  // f overwrites amdq
                 for (int e = tid; e <= mx; e += blockDim.x) {
                     real w[MW][ME];
                     for (int mw = 0; mw < MW; ++mw)
@@ -184,6 +212,9 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
                         qs[m * n + k + 2] = qs[m * n + k + 2] - d * (fl[m * ne + k + 2] - fl[m * ne + k + 1]);
                 }
             }
+            // source after the step, before the Courant check (claw1.f:499-509)
+            if (src_split == 2) step1_source(A, qs, n, dt / 2.0);
+            if (src_split == 1) step1_source(A, qs, n, dt);
             if (tid == 0) {
                 double cm = 0.0;
                 for (int w = 0; w < STEP1_THREADS / 32; ++w) cm = fmax(cm, red[w]);
@@ -201,8 +232,8 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
                 }
                 sh_dt = dtn;
                 // ... then check the Courant number (src/1d/claw1.f:533-554)
-                if (cm != cm) sh_state = 3;
-                else if (cm <= ctl->cfl_max) sh_state = 0;
+                if (cm != cm) sh_state = single ? 0 : 3;
+                else if (single || cm <= ctl->cfl_max) sh_state = 0;
                 else sh_state = ctl->dt_variable ? 1 : 2;
             }
             __syncthreads();
@@ -214,7 +245,8 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
                 break;
             }
             t = told;
-            for (int i = tid; i < ME * n; i += blockDim.x) qs[i] = qsave[i];
+            for (int i = tid; i < ME * mx; i += blockDim.x)
+                qs[(i / mx) * n + i % mx + 2] = qsave[(i / mx) * A.fstride + i % mx];
             __syncthreads();
             if (st == 1) { ++nrej; continue; }
             if (st == 3) { if (tid == 0) ctl->err |= CTL_ERR_NAN_CFL; stop = true; break; }

@@ -75,9 +75,25 @@ struct Step2Args {
     double dx, dy;
     long long units;          // nstrips * my
     int nwarps;               // warps sharing the units
+    // source term (src/2d/claw2.f:635-738): 0 none, 1 Godunov, 2 Strang; the
+    // radial term of examples/acoustics_2d_radial/1drad/src1.f on every row
+    int src_split;
+    double src_nd1, src_bulk, xlower;  // ndim - 1, bulk, xlower
     ClawCtl* ctl;
     S solver;
 };
+
+// The radial source at 0-based column c (src1.f:18-23 covers the cells
+// i = c+1 >= 1 of a row, right ghosts included): p -= dts (ndim-1) bulk / x u.
+// q[0] is the pressure and q[1] the radial velocity.
+template <class S>
+__device__ __forceinline__ void src_radial_cell(const Step2Args<S>& A, typename S::real* q, int c,
+                                                double dts) {
+    if (c < 0) return;
+    const double xcell = A.xlower + ((double)(c + 1) - 0.5) * A.dx;
+    const double coef = dts * A.src_nd1 * A.src_bulk / xcell;
+    q[0] = q[0] - (typename S::real)(coef * (double)q[1]);
+}
 
 // Map a (possibly ghost) index to its source interior index under the BC of
 // that side.  Returns the source index; sets neg when a wall reflects it.
@@ -147,6 +163,8 @@ struct StepConsts {
     const typename S::real* qold;
     typename S::real* qnew;
     const CUtensorMap* tmq;        // TMA map of qold
+    int src;                       // source split of this launch (0 in claw_step / batches)
+    double src_pre, src_post;      // source time steps before / after the step
 };
 
 template <class S>
@@ -160,10 +178,13 @@ __device__ __forceinline__ StepConsts<S> step_consts(const Step2Args<S>& A, int 
     k.qold = A.q[cur];
     k.qnew = A.q[cur ^ 1];
     k.tmq = &A.tmq[cur];
+    k.src = 0;
+    k.src_pre = dtd / 2.0;
+    k.src_post = dtd;
     return k;
 }
 
-template <class S, class M>
+template <class S, class M, bool SRC = false>
 __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepConsts<S>& K,
                                            const int strip, const int r0, const int nr,
                                            unsigned char* ring, uint64_t* bars,
@@ -256,6 +277,12 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
             if (m == 2 && nyneg) { vm = -vm; vc = -vc; }
             qm[m] = vm;
             qc[m] = vc;
+        }
+        if constexpr (SRC) {
+            if (K.src == 2) {  // Strang: dt/2 of source on the data the step reads
+                src_radial_cell(A, qm, c - 1, K.src_pre);
+                src_radial_cell(A, qc, c, K.src_pre);
+            }
         }
     };
     // aux of column (c + dc) at row r (ring already resident).
@@ -570,6 +597,7 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
         const real hp = real(0.5) * dty_p, ht = real(0.5) * dty_t;
         const bool out = (t - 1 >= r0) && (lane >= 1) && (lane <= STRIP) && (c < mx);
         real* __restrict__ dst = qnew + (long long)(t - 1) * A.ld + c;
+        real qo[ME];
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
             const bool wz = S::wave_zero(2, m), tz = S::trans_zero(2, m) || trans <= 0;
@@ -592,7 +620,14 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                 const real q5 = (q4 + qa) - (dtdy * dF + dtdx * (G2 - G1)) / a_cp[ic];
                 q6 = q5 - Br;
             }
-            if (out) dst[m * A.fstride] = q6;
+            qo[m] = q6;
+        }
+        if constexpr (SRC) {
+            if (K.src != 0) src_radial_cell(A, qo, c, K.src == 2 ? K.src_pre : K.src_post);
+        }
+        if (out) {
+#pragma unroll
+            for (int m = 0; m < ME; ++m) dst[m * A.fstride] = qo[m];
         }
         // contributions of y-interface t to cell (c, t); roll the window
 #pragma unroll
@@ -638,7 +673,7 @@ struct step2_minb { static constexpr int value = CLAW_STEP2_MINB; };
 template <class S>
 struct step2_minb<S, std::void_t<decltype(S::min_blocks)>> { static constexpr int value = S::min_blocks; };
 
-template <class S, class M>
+template <class S, class M, bool SRC = false>
 __global__ void __launch_bounds__(32 * WARPS2D, step2_minb<S>::value)
 step2_kernel(const __grid_constant__ Step2Args<S> A) {
     ClawCtl* ctl = A.ctl;
@@ -666,14 +701,16 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
     const long long gw = (long long)blockIdx.x * WARPS2D + warp;
     long long u0 = (gw < A.nwarps) ? gw * A.units / A.nwarps : 0;
     const long long u1 = (gw < A.nwarps) ? (gw + 1) * A.units / A.nwarps : 0;
-    const StepConsts<S> K = step_consts(A, cur, dtd);
+    StepConsts<S> K = step_consts(A, cur, dtd);
+    // claw2 wraps the source steps around step2; a single step (claw_step) is step2 alone
+    if (SRC && ctl->mode == CTL_ADVANCE) K.src = A.src_split;
 
     while (u0 < u1 && !failed) {
         const int strip = (int)(u0 / my);
         const int r0 = (int)(u0 % my);
         const int nr = (int)min((long long)(my - r0), u1 - u0);
         u0 += nr;
-        step2_rows<S, M>(A, K, strip, r0, nr, ring, bars, seq_base, cfl, failed);
+        step2_rows<S, M, SRC>(A, K, strip, r0, nr, ring, bars, seq_base, cfl, failed);
     }
 
     cta_cfl_and_control(ctl, cfl, red);

@@ -62,6 +62,8 @@ struct SplitConsts {
     const typename S::real* qold;
     typename S::real* qnew;
     const CUtensorMap* tmq;
+    int src;                       // source split of this launch (0 in claw_step)
+    double src_pre, src_post;      // source time steps before / after the step
 };
 
 // One x-slice step on the row the warp holds (lane l: own column c, values qc
@@ -183,7 +185,7 @@ __device__ __forceinline__ void split_xslice(const Step2Args<S>& A, const typena
     }
 }
 
-template <class S, class M, bool STRANG>
+template <class S, class M, bool STRANG, bool SRC>
 __device__ __forceinline__ void split2_rows(const Step2Args<S>& A, const SplitConsts<S>& K,
                                             const int strip, const int r0, const int nr,
                                             unsigned char* ring, uint64_t* bars,
@@ -271,6 +273,9 @@ __device__ __forceinline__ void split2_rows(const Step2Args<S>& A, const SplitCo
             if (m == 2 && nyneg) v = -v;
             qv[m] = v;
         }
+        if constexpr (SRC) {
+            if (K.src == 2) src_radial_cell(A, qv, c, K.src_pre);  // Strang: before the step
+        }
         if constexpr (MA > 0) {
             const real* sa = reinterpret_cast<const real*>(slot_ptr(r) + L::QBP);
 #pragma unroll
@@ -320,6 +325,9 @@ __device__ __forceinline__ void split2_rows(const Step2Args<S>& A, const SplitCo
         real out[ME];
         split_xslice<S, M>(A, yb, av, K.dtdx_c, K.dtdx_c_d, interior_col && lane >= 4 && lane <= 27,
                            cc_ok, out, cfl[2]);
+        if constexpr (SRC) {
+            if (write && K.src != 0) src_radial_cell(A, out, c, K.src == 2 ? K.src_pre : K.src_post);
+        }
         if (write && out_lane) {
             real* __restrict__ dst = qnew + (long long)r * A.ld + c;
 #pragma unroll
@@ -425,6 +433,9 @@ __device__ __forceinline__ void split2_rows(const Step2Args<S>& A, const SplitCo
             // neighbours; ghost rows (not y-updated) are exact
             if (ro >= r0 || ro < 0) stage_c(ro, yb, aux_p, ro >= r0);
         } else {
+            if constexpr (SRC) {
+                if (K.src != 0) src_radial_cell(A, yb, c, K.src == 2 ? K.src_pre : K.src_post);
+            }
             if (ro >= r0 && out_lane) {
                 real* __restrict__ dst = qnew + (long long)ro * A.ld + c;
 #pragma unroll
@@ -520,7 +531,7 @@ __device__ __forceinline__ void cta_split_cfl_and_control(ClawCtl* ctl, const do
     }
 }
 
-template <class S, class M, bool STRANG>
+template <class S, class M, bool STRANG, bool SRC = false>
 __global__ void __launch_bounds__(32 * WARPS2D, step2_minb<S>::value)
 split2_kernel(const __grid_constant__ Step2Args<S> A) {
     using L = SplitLayout<S, STRANG>;
@@ -552,6 +563,10 @@ split2_kernel(const __grid_constant__ Step2Args<S> A) {
     K.qold = A.q[cur];
     K.qnew = A.q[cur ^ 1];
     K.tmq = &A.tmq[cur];
+    // claw2 wraps the source steps around the split step; claw_step runs it alone
+    K.src = (SRC && ctl->mode == CTL_ADVANCE) ? A.src_split : 0;
+    K.src_pre = dtd / 2.0;
+    K.src_post = dtd;
 
     const int my = A.my;
     double cfl[3] = {0.0, 0.0, 0.0};
@@ -565,7 +580,7 @@ split2_kernel(const __grid_constant__ Step2Args<S> A) {
         const int r0 = (int)(u0 % my);
         const int nr = (int)min((long long)(my - r0), u1 - u0);
         u0 += nr;
-        split2_rows<S, M, STRANG>(A, K, strip, r0, nr, ring, bars, seq_base, cfl, failed);
+        split2_rows<S, M, STRANG, SRC>(A, K, strip, r0, nr, ring, bars, seq_base, cfl, failed);
     }
     cta_split_cfl_and_control(ctl, cfl, STRANG ? 3 : 2, red);
 }

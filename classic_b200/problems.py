@@ -57,6 +57,77 @@ def acoustics_1d_config(mx=800, nout=10, tfinal=1.0):
     return rd, solver, params, q0, None
 
 
+def radial_pulse(r, width=0.2):
+    """qinit of examples/acoustics_2d_radial (qinit.f:17-28) and of its 1drad
+    companion (1drad/qinit.f): p = 1 + cos(pi (r-0.5)/width) for
+    |r-0.5| <= width, else 0."""
+    return np.where(np.abs(r - 0.5) <= width, 1.0 + np.cos(np.pi * (r - 0.5) / width), 0.0)
+
+
+def radial_acoustics_1d(mx=2000, nout=20, tfinal=1.0, order=1, source_split="godunov"):
+    """examples/acoustics_2d_radial/1drad (setrun.py, qinit.f, setprob.f,
+    src1.f): 1D acoustics in the radius r on [0, 1.5], rho=1, bulk=4, ndim=2
+    (cylindrical symmetry) through the geometric source term of src1.f with
+    Godunov source splitting; wall at r=0, extrapolation at 1.5; order 1,
+    cfl 1.0, dt_initial 0.5, 20 outputs to t=1.  Run it with
+    user_source="radial"."""
+    rd = ClawRunData("classic", 1)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("ndim", 2)
+    pd.add_param("rho", 1.0)
+    pd.add_param("bulk", 4.0)
+    cd = rd.clawdata
+    cd.lower[0], cd.upper[0], cd.num_cells[0] = 0.0, 1.5, mx
+    cd.num_eqn, cd.num_aux, cd.capa_index = 2, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 0.5, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 1.0, 1.0, 50000
+    cd.order, cd.num_waves, cd.limiter = order, 2, ["superbee", "superbee"]
+    cd.source_split = source_split
+    cd.bc_lower[0], cd.bc_upper[0] = "wall", "extrap"
+    x, _ = _centres(0.0, 1.5, mx)
+    q0 = np.zeros((2, mx))
+    q0[0] = radial_pulse(x)
+    return rd, "acoustics_1d", {"rho": 1.0, "bulk": 4.0, "ndim": 2}, q0, None
+
+
+def axisymmetric_acoustics_2d(nr=300, nz=40, tfinal=0.4, nout=2, source_split="godunov",
+                              split="unsplit", zdata=True, seed=0):
+    """2D acoustics in the (r, z) half-plane [0, 1.5] x [-0.2, 0.2] of a
+    cylindrically symmetric field: the radial source of
+    examples/acoustics_2d_radial/1drad/src1.f on every row (run with
+    user_source="radial"); wall at r=0, extrapolation at r=1.5, periodic in z.
+    The 1drad pulse in r; with zdata a seeded z-dependent perturbation is
+    added, otherwise every row follows the 1D radial solution."""
+    rd = ClawRunData("classic", 2)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("ndim", 2)
+    pd.add_param("rho", 1.0)
+    pd.add_param("bulk", 4.0)
+    cd = rd.clawdata
+    cd.lower, cd.upper, cd.num_cells = [0.0, -0.2], [1.5, 0.2], [nr, nz]
+    cd.num_eqn, cd.num_aux, cd.capa_index = 3, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 0.5, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 50000
+    cd.order, cd.transverse_waves, cd.dimensional_split = 2, 2, split
+    cd.num_waves, cd.limiter = 2, ["mc", "mc"]
+    cd.source_split = source_split
+    cd.bc_lower, cd.bc_upper = ["wall", "periodic"], ["extrap", "periodic"]
+    r, _ = _centres(0.0, 1.5, nr)
+    z, _ = _centres(-0.2, 0.2, nz)
+    R, Z = np.meshgrid(r, z, indexing="xy")
+    q0 = np.zeros((3, nz, nr))
+    q0[0] = radial_pulse(R)
+    if zdata:
+        rng = np.random.default_rng(seed)
+        q0[0] += 0.05 * np.cos(2 * np.pi * Z / 0.4) * np.exp(-20 * (R - 0.8) ** 2)
+        q0[2] = 0.01 * rng.standard_normal((nz, nr))
+    return rd, "acoustics_2d", {"rho": 1.0, "bulk": 4.0, "ndim": 2}, q0, None
+
+
 def acoustics_1d_heterogeneous(mx=500, nout=2, tfinal=5.0, ic=1, beta=5.0):
     """examples/acoustics_1d_heterogeneous (setrun.py, qinit.f, setaux.f,
     setprob.f) with the test's overrides (test_acoustics_1d_heterogeneous.py:23-25)."""

@@ -51,6 +51,18 @@ enum claw_solver_id {
  * bc_upper[2] with CLAW_SOLVER_VC_ACOUSTICS_3D; t is the step's start time. */
 enum claw_bc { CLAW_BC_PISTON = 10 };
 
+/* Built-in source terms psi(q) for source_split 1 (Godunov: src after each
+ * step over dt) and 2 (Strang: dt/2 before and after), the src1 / src2 hooks
+ * of src/1d/claw1.f:486-509 and src/2d/claw2.f:635-738.  The reference's
+ * default src routine does nothing, which source_id CLAW_SOURCE_NONE keeps.
+ * CLAW_SOURCE_RADIAL is examples/acoustics_2d_radial/1drad/src1.f:18-23: the
+ * geometric term of radially symmetric acoustics with x as the radius,
+ *     p <- p - dt (ndim - 1) bulk / x_i  u    for cells i = 1 .. mx+2,
+ * ndim = source_ndim (2 cylindrical, 3 spherical), bulk = solver_params[1];
+ * for CLAW_SOLVER_ACOUSTICS_1D, and for CLAW_SOLVER_ACOUSTICS_2D as the
+ * axisymmetric (r, z) form (every row, u the radial velocity). */
+enum claw_source_id { CLAW_SOURCE_NONE = 0, CLAW_SOURCE_RADIAL = 1 };
+
 /* Arithmetic of the Riemann/limiter/update path. */
 enum claw_precision {
     CLAW_FP64 = 0,      /* every multiply and add rounded separately: same
@@ -84,7 +96,7 @@ typedef struct claw_config {
     int transverse_waves;     /* method(3): 0,1,2 (2D); 0,10,11,20,21,22 (3D)      */
     int dimensional_split;    /* 0 unsplit, 1 Godunov, 2 Strang (3D: Godunov)      */
     int verbosity;            /* method(4)                                         */
-    int source_split;         /* method(5): 0 (source terms are not built)         */
+    int source_split;         /* method(5): 0 none, 1 Godunov, 2 Strang             */
     int use_fwaves;
     int limiter[CLAW_MAX_WAVES]; /* mthlim: 0 none,1 minmod,2 superbee,3 vanleer,4 MC,5 BW */
     int num_ghost;            /* mbc, must be 2                                    */
@@ -99,7 +111,9 @@ typedef struct claw_config {
     int solver_id;            /* enum claw_solver_id                               */
     double solver_params[8];  /* problem parameters of the solver (setprob)        */
     int precision;            /* enum claw_precision                               */
-    int reserved[7];
+    int source_id;            /* enum claw_source_id (the src1 / src2 routine)     */
+    int source_ndim;          /* CLAW_SOURCE_RADIAL: 2 cylindrical, 3 spherical    */
+    int reserved[5];
 } claw_config;
 
 /* What claw2 returns through dtv / cflv / nv (src/2d/claw2.f:776-781). */

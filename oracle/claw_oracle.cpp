@@ -62,6 +62,19 @@ static int g_solver = 0;
 static double g_rho = 1.0, g_bulk = 1.0, g_cc = 1.0, g_zz = 1.0, g_hz = 0.5;
 static double g_gamma = 1.4;
 
+// Source term (the example's src1 / src2; 0 = the reference's default no-op).
+// 1: examples/acoustics_2d_radial/1drad/src1.f:18-23, radial symmetry with x
+// as the radius; bulk is the solver's (the shared /cparam/ block).
+static int g_src = 0, g_src_ndim = 2;
+static double g_src_xlower = 0.0;
+
+int orc_set_source(int id, int ndim, double xlower) {
+    g_src = id;
+    g_src_ndim = ndim;
+    g_src_xlower = xlower;
+    return 0;
+}
+
 int orc_set_solver(int solver_id, const double* params, int nparams) {
     g_solver = solver_id;
     if (solver_id == ORC_ACOUSTICS_2D || solver_id == ORC_ACOUSTICS_1D) {
@@ -529,6 +542,16 @@ void flux2(int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
     }
 }
 
+// src1.f:18-23 on the cells i = 1..mx+mbc of one slice (stride `st` doubles
+// between cells, p at +0 and the radial velocity at +1)
+void src_radial_slice(int mbc, int mx, double dx, double* q, int st, double dt) {
+    for (int i = 1; i <= mx + mbc; ++i) {
+        const double xcell = g_src_xlower + ((double)i - 0.5) * dx;
+        double* c = q + (size_t)st * (i - (1 - mbc));
+        c[0] = c[0] - dt * (double)(g_src_ndim - 1) * g_bulk / xcell * c[1];
+    }
+}
+
 bool pick2(int solver, rpn2_t* rpn, rpt2_t* rpt) {
     switch (solver) {
         case ORC_ACOUSTICS_2D: *rpn = rpn2_acoustics; *rpt = rpt2_acoustics; return true;
@@ -843,7 +866,13 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
     double cflmax = 0.0, dtmin = dt, dtmax = dt, cfl = 0.0;
     nv[1] = 0;
     const size_t nq = (size_t)meqn * (mx + 2 * mbc) * (my + 2 * mbc);
-    std::vector<double> qwork(nq);
+    std::vector<double> qwork(nq), qwork2(method[4] == 2 ? nq : 0);
+    // the source routine over every row j = 1-mbc..my+mbc (0 = default no-op)
+    auto src2 = [&](double* qq, double dts) {
+        if (g_src != 1) return;
+        for (int j = 0; j < my + 2 * mbc; ++j)
+            src_radial_slice(mbc, mx, dx, qq + (size_t)meqn * (mx + 2 * mbc) * j, meqn, dts);
+    };
     if (method[0] == 0) {
         if (tend < tstart) maxn = 1;
         else {
@@ -863,6 +892,11 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
         if (told + dt > tend && tstart < tend) dt = tend - told;
         for (;;) {
             if (orc_bc2(meqn, mbc, mx, my, q, mthbc) != 0) { info = -2; goto done; }
+            if (method[4] == 2) {
+                // src/2d/claw2.f:635-647: keep q for a retry, then dt/2 of source
+                std::memcpy(qwork2.data(), q, nq * sizeof(double));
+                src2(q, dt / 2.0);
+            }
             std::memcpy(qwork.data(), q, nq * sizeof(double));
             const int rc = method[2] >= 0
                                ? orc_step2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q, aux,
@@ -879,7 +913,7 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
                 break;
             }
             t = told;
-            std::memcpy(q, qwork.data(), nq * sizeof(double));
+            std::memcpy(q, method[4] == 2 ? qwork2.data() : qwork.data(), nq * sizeof(double));
             if (method[0] == 1) {
                 dt = std::fmin(dtv[1], dt * cflv[1] / cfl);
                 continue;
@@ -887,6 +921,9 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
             cflmax = std::fmax(cfl, cflmax);
             goto done;
         }
+        // src/2d/claw2.f:726-738: the source step after an accepted step
+        if (method[4] == 2) src2(q, dt / 2.0);
+        if (method[4] == 1) src2(q, dt);
         if (method[0] == 1) {
             if (cfl == 0.0) dt = dtv[1];
             else dt = std::fmin(dtv[1], dt * cflv[1] / cfl);
@@ -1621,9 +1658,14 @@ int orc_claw1(int meqn, int mwaves, int maux, int mbc, int mx, double* q, const 
         for (;;) {
             t = told + dt;
             if (orc_bc1(meqn, mbc, mx, q, mthbc) != 0) { info = -2; goto done; }
+            // src/1d/claw1.f:486-509: the source steps sit around step1, before
+            // the Courant check (a rejected step restores q saved before bc1)
+            if (method[4] == 2 && g_src == 1) src_radial_slice(mbc, mx, dx, q, meqn, dt / 2.0);
             const int rc = orc_step1(meqn, mwaves, mbc, maux, mx, q, aux, dx, dt, method, mthlim,
                                      use_fwaves, &cfl);
             if (rc != 0) { info = rc == -3 ? -3 : -1; goto done; }
+            if (method[4] == 2 && g_src == 1) src_radial_slice(mbc, mx, dx, q, meqn, dt / 2.0);
+            if (method[4] == 1 && g_src == 1) src_radial_slice(mbc, mx, dx, q, meqn, dt);
             if (method[0] == 1) {
                 if (cfl > 0.0) {
                     dt = std::fmin(dtv[1], dt * cflv[1] / cfl);

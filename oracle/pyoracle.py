@@ -36,6 +36,8 @@ SOLVER_PARAMS = {
 
 # bc code of the restated user BC (examples/acoustics_3d_heterogeneous/bc3.f:282-312)
 PISTON_BC = 10
+# restated source routines (examples/acoustics_2d_radial/1drad/src1.f:18-23)
+SOURCE_IDS = {"radial": 1}
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -55,6 +57,8 @@ def _load(variant: str):
     lib = ctypes.CDLL(path)
     lib.orc_set_solver.argtypes = [ctypes.c_int, _D, ctypes.c_int]
     lib.orc_set_solver.restype = ctypes.c_int
+    lib.orc_set_source.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    lib.orc_set_source.restype = ctypes.c_int
     lib.orc_claw2.argtypes = [ctypes.c_int] * 6 + [_D, _D, ctypes.c_double, ctypes.c_double,
                                                    ctypes.c_double, _D, _D, _D, _I, _I, _I, _I,
                                                    ctypes.c_int]
@@ -125,7 +129,8 @@ def _codes(cd):
 class OracleGrid:
     """Reference-layout state of one grid driven by the CPU restatement."""
 
-    def __init__(self, cd, solver: str, params: dict | None = None, variant: str = "parity"):
+    def __init__(self, cd, solver: str, params: dict | None = None, variant: str = "parity",
+                 user_source: str | None = None):
         self.lib = _load(variant)
         self.cd = cd
         self.nd = int(cd.num_dim)
@@ -143,6 +148,9 @@ class OracleGrid:
         params = params or {}
         pv = np.array([float(params[k]) for k in SOLVER_PARAMS.get(solver, ())] or [0.0])
         self.pv = pv
+        # the example's src routine (0 = the reference's default no-op)
+        self.src = SOURCE_IDS[user_source] if user_source is not None else 0
+        self.src_ndim = int(params.get("ndim", 2))
         g = tuple(n + 2 * self.mbc for n in reversed(self.cells))  # (my+4, mx+4) C order
         self.qf = np.zeros(g + (self.meqn,), dtype=np.float64)
         self.af = np.zeros(g + (max(self.maux, 1),), dtype=np.float64)
@@ -150,6 +158,7 @@ class OracleGrid:
 
     def _set_solver(self):
         self.lib.orc_set_solver(SOLVER_IDS[self.solver], _p(self.pv), len(self.pv))
+        self.lib.orc_set_source(self.src, self.src_ndim, float(self.cd.lower[0]))
 
     def _interior(self):
         b = self.mbc
@@ -249,10 +258,11 @@ class OracleGrid:
         return cfl.value
 
 
-def run_oracle(rundata, solver, params, q0, aux=None, variant="parity", flush_tiny=True):
+def run_oracle(rundata, solver, params, q0, aux=None, variant="parity", flush_tiny=True,
+               user_source=None):
     """claw{1,2}ez frame loop on the oracle; returns [(frame, t, q, stats)]."""
     cd = getattr(rundata, "clawdata", rundata)
-    g = OracleGrid(cd, solver, params, variant)
+    g = OracleGrid(cd, solver, params, variant, user_source)
     q = np.array(q0, dtype=np.float64, copy=True)
     if flush_tiny:
         q[np.abs(q) < 1e-99] = 0.0
