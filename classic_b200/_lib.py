@@ -61,7 +61,9 @@ class ClawConfig(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("source_id", ctypes.c_int),
         ("source_ndim", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("b4step_id", ctypes.c_int),
+        ("reserved", ctypes.c_int * 2),
+        ("b4step_param", ctypes.c_double),
     ]
 
 

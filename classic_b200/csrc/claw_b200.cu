@@ -244,6 +244,58 @@ std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
     return nullptr;
 }
 
+// ------------------------------------------------------- before-step hook ---
+// b4step2 (src/2d/claw2.f:626-631) as a device routine launched ahead of each
+// step kernel: CLAW_B4STEP_REVERSING writes the edge velocities (aux fields 1,
+// 2) = the unscaled ones times cos(pi t / T) at the step's start time t, read
+// from the control block, so the device-resident time loop needs no host
+// round trip per step.
+template <typename real>
+__global__ void b4step_reversing_kernel(const ClawCtl* ctl, const real* __restrict__ base,
+                                        real* __restrict__ aux, long long n, double period) {
+    if (*(const volatile int*)&ctl->done) return;
+    const double told = *(const volatile double*)&ctl->told;
+    const double sc = cos(3.141592653589793 * told / period);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        aux[i] = (real)((double)base[i] * sc);
+}
+
+template <typename real>
+struct B4StepRunner : Runner {
+    std::unique_ptr<Runner> inner;
+    const ClawCtl* ctl = nullptr;
+    const real* base = nullptr;
+    real* aux = nullptr;
+    long long n = 0;
+    double period = 1.0;
+    int grid = 1;
+
+    explicit B4StepRunner(std::unique_ptr<Runner> r) : inner(std::move(r)) {}
+
+    int prepare(const claw_config& cfg, const Geometry& g) override {
+        int rc = inner->prepare(cfg, g);
+        if (rc) return rc;
+        ctl = g.ctl;
+        base = static_cast<const real*>(g.aux_base);
+        aux = static_cast<real*>(g.aux);
+        n = 2 * g.afstride;  // fields 1 and 2 are contiguous
+        period = cfg.b4step_param;
+        int dev = 0, nsm = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        grid = (int)std::min<long long>((n + 255) / 256, (long long)nsm * 8);
+        return 0;
+    }
+    cudaError_t launch(cudaStream_t s) override {
+        b4step_reversing_kernel<real><<<grid, 256, 0, s>>>(ctl, base, aux, n, period);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return inner->launch(s);
+    }
+    int launches_per_step() const override { return inner->launches_per_step() + 1; }
+};
+
 struct SolverShape { int dim, meqn, mwaves, maux; };
 
 bool solver_shape(int id, SolverShape* sh) {
@@ -326,6 +378,12 @@ static int validate(const claw_config* c, SolverShape* sh) {
         return fail(CLAW_E_INVALID, "dimensional splitting needs 2 or 3 dimensions");
     if (c->source_split < 0 || c->source_split > 2)
         return fail(CLAW_E_INVALID, "source_split must be 0, 1 (Godunov) or 2 (Strang)");
+    if (c->b4step_id != CLAW_B4STEP_NONE) {
+        if (c->b4step_id != CLAW_B4STEP_REVERSING) return fail(CLAW_E_INVALID, "unknown b4step_id %d", c->b4step_id);
+        if (c->solver_id != CLAW_SOLVER_VC_ADVECTION_2D)
+            return fail(CLAW_E_UNSUPPORTED, "the reversing flow is built for the variable-velocity advection solver");
+        if (!(c->b4step_param > 0.0)) return fail(CLAW_E_INVALID, "b4step_param (the period) must be > 0");
+    }
     if (c->source_id != CLAW_SOURCE_NONE) {
         if (c->source_id != CLAW_SOURCE_RADIAL) return fail(CLAW_E_INVALID, "unknown source_id %d", c->source_id);
         if (c->solver_id != CLAW_SOLVER_ACOUSTICS_1D && c->solver_id != CLAW_SOLVER_ACOUSTICS_2D)
@@ -395,6 +453,12 @@ int claw_create(const claw_config* cfg, claw_handle** out) {
     }
     h->runner = g.es == 8 ? make_runner<double>(*cfg) : make_runner<float>(*cfg);
     if (!h->runner) return fail(CLAW_E_UNSUPPORTED, "no kernel for solver %d", cfg->solver_id);
+    if (cfg->b4step_id == CLAW_B4STEP_REVERSING) {
+        CUDA_TRY(cudaMalloc(&g.aux_base, (size_t)g.afstride * g.maux * g.es));
+        CUDA_TRY(cudaMemsetAsync(g.aux_base, 0, (size_t)g.afstride * g.maux * g.es, h->stream));
+        if (g.es == 8) h->runner.reset(new B4StepRunner<double>(std::move(h->runner)));
+        else h->runner.reset(new B4StepRunner<float>(std::move(h->runner)));
+    }
     rc = h->runner->prepare(*cfg, g);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -410,6 +474,7 @@ int claw_destroy(claw_handle* h) {
     for (int k = 0; k < 2; ++k)
         if (h->g.q[k]) cudaFree(h->g.q[k]);
     if (h->g.aux) cudaFree(h->g.aux);
+    if (h->g.aux_base) cudaFree(h->g.aux_base);
     if (h->g.ctl) cudaFree(h->g.ctl);
     if (h->stage) cudaFree(h->stage);
     if (h->ctl_h) cudaFreeHost(h->ctl_h);
@@ -490,6 +555,9 @@ int claw_set_aux(claw_handle* h, const double* aux) {
     const long long rows = (long long)(g.dim >= 2 ? g.my + 4 : 1) * (g.dim >= 3 ? g.mz + 4 : 1);
     int rc = copy_fields(h, g.aux, g.ald, g.afstride, aux, g.maux, g.mx + 4, rows, true);
     if (rc) return rc;
+    if (g.aux_base)  // the before-step routine scales from this copy
+        CUDA_TRY(cudaMemcpyAsync(g.aux_base, g.aux, (size_t)g.afstride * g.maux * g.es,
+                                 cudaMemcpyDeviceToDevice, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (h->cfg.capa_index > 0) {
         // the reference stops on a non-positive capacity (src/1d/step1.f90:67-70)

@@ -17,6 +17,7 @@ struct Geometry {
     long long ld, fstride, ald, afstride;  // pitches in elements
     void* q[2];
     void* aux;
+    void* aux_base;  // the aux claw_set_aux received, when a before-step routine rewrites aux
     ClawCtl* ctl;
     double dx, dy, dz;
 };

@@ -35,16 +35,20 @@ USER_BCS = {"piston": 10}  # examples/acoustics_3d_heterogeneous/bc3.f:282-312, 
 # Built-in source terms (the example's src1 / src2), by name; their parameters
 # come from the problem parameters ("ndim").
 USER_SOURCES = {"radial": 1}  # examples/acoustics_2d_radial/1drad/src1.f:18-23
+# Built-in before-step routines (the example's b4step2), by name; parameter
+# "period" of the problem parameters.
+USER_B4STEPS = {"reversing": 1}  # edge velocities of vc_advection_2d times cos(pi t / T)
 
 
 def make_config(cd: ClawInputData, solver: str, params: dict | None = None,
                 precision: str = "fp64", user_bc: str | None = None,
-                user_source: str | None = None) -> ClawConfig:
+                user_source: str | None = None, user_b4step: str | None = None) -> ClawConfig:
     """Map clawdata + solver choice onto the C ``claw_config``.  ``user_bc``
     names the built-in routine that stands for the example's own bc code
     wherever clawdata says 'user'; ``user_source`` the built-in routine that
     stands for the example's src1 / src2 (applied as clawdata.source_split
-    says; without one the source step is the reference's default no-op)."""
+    says; without one the source step is the reference's default no-op);
+    ``user_b4step`` the one that stands for its b4step2 (default: nothing)."""
     if solver not in SOLVER_IDS:
         raise ValueError(f"unknown solver {solver!r}; built: {sorted(SOLVER_IDS)}")
     params = params or {}
@@ -70,6 +74,11 @@ def make_config(cd: ClawInputData, solver: str, params: dict | None = None,
             raise ValueError(f"unknown user_source {user_source!r}; built: {sorted(USER_SOURCES)}")
         c.source_id = USER_SOURCES[user_source]
         c.source_ndim = int(params.get("ndim", 2))
+    if user_b4step is not None:
+        if user_b4step not in USER_B4STEPS:
+            raise ValueError(f"unknown user_b4step {user_b4step!r}; built: {sorted(USER_B4STEPS)}")
+        c.b4step_id = USER_B4STEPS[user_b4step]
+        c.b4step_param = float(params.get("period", 1.0))
     c.use_fwaves = 1 if cd.use_fwaves else 0
     lim = cd.limiter_codes()
     if len(lim) != c.num_waves:
@@ -111,14 +120,15 @@ class Solver:
 
     def __init__(self, clawdata, solver: str, params: dict | None = None,
                  precision: str = "fp64", user_bc: str | None = None,
-                 user_source: str | None = None):
+                 user_source: str | None = None, user_b4step: str | None = None):
         if isinstance(clawdata, ClawRunData):
             clawdata = clawdata.clawdata
         self.lib = _lib.load()
         self.clawdata = clawdata
         self.solver = solver
         self.precision = precision
-        self.cfg = make_config(clawdata, solver, params, precision, user_bc, user_source)
+        self.cfg = make_config(clawdata, solver, params, precision, user_bc, user_source,
+                               user_b4step)
         self.ndim = self.cfg.num_dim
         self.meqn = self.cfg.num_eqn
         self.maux = self.cfg.num_aux
@@ -217,7 +227,8 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray | None,
         aux: np.ndarray | None = None, precision: str = "fp64",
         on_frame: Callable[[Frame], None] | None = None, keep_frames: bool = True,
         flush_tiny: bool = True, solver_obj: Solver | None = None, user_bc: str | None = None,
-        outdir: str | None = None, user_source: str | None = None):
+        outdir: str | None = None, user_source: str | None = None,
+        user_b4step: str | None = None):
     """claw{1,2,3}ez's frame loop on the GPU.  Returns the list of frames
     (frame 0 included when output_t0); raises on a nonzero info.
 
@@ -228,7 +239,7 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray | None,
     (src/2d/claw2ez.f:236-271; dtout keeps the data's t0)."""
     from . import frames as _frames
     cd = rundata.clawdata if isinstance(rundata, ClawRunData) else rundata
-    s = solver_obj or Solver(cd, solver, params, precision, user_bc, user_source)
+    s = solver_obj or Solver(cd, solver, params, precision, user_bc, user_source, user_b4step)
     nd = int(cd.num_dim)
     lower = [float(cd.lower[d]) for d in range(nd)]
     dxs = [(float(cd.upper[d]) - float(cd.lower[d])) / float(np.float32(int(cd.num_cells[d])))

@@ -63,6 +63,16 @@ enum claw_bc { CLAW_BC_PISTON = 10 };
  * axisymmetric (r, z) form (every row, u the radial velocity). */
 enum claw_source_id { CLAW_SOURCE_NONE = 0, CLAW_SOURCE_RADIAL = 1 };
 
+/* Built-in before-step routines: the b4step2 hook of src/2d/claw2.f:626-631,
+ * called after bc2 and before each step (retries included) with the step's
+ * start time, to set time-dependent aux arrays.  CLAW_B4STEP_NONE is the
+ * reference's default (src/2d/b4step2.f90, nothing).  CLAW_B4STEP_REVERSING
+ * scales the edge velocities of CLAW_SOLVER_VC_ADVECTION_2D (aux fields 1
+ * and 2) by cos(pi t / T), T = b4step_param: the flow runs forward until
+ * T/2 and backward to T, where an exact solution is back at its start.  The
+ * aux given to claw_set_aux is kept as the unscaled field. */
+enum claw_b4step_id { CLAW_B4STEP_NONE = 0, CLAW_B4STEP_REVERSING = 1 };
+
 /* Arithmetic of the Riemann/limiter/update path. */
 enum claw_precision {
     CLAW_FP64 = 0,      /* every multiply and add rounded separately: same
@@ -113,7 +123,9 @@ typedef struct claw_config {
     int precision;            /* enum claw_precision                               */
     int source_id;            /* enum claw_source_id (the src1 / src2 routine)     */
     int source_ndim;          /* CLAW_SOURCE_RADIAL: 2 cylindrical, 3 spherical    */
-    int reserved[5];
+    int b4step_id;            /* enum claw_b4step_id (the b4step2 routine)         */
+    int reserved[2];
+    double b4step_param;      /* CLAW_B4STEP_REVERSING: the period T               */
 } claw_config;
 
 /* What claw2 returns through dtv / cflv / nv (src/2d/claw2.f:776-781). */

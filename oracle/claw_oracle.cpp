@@ -75,6 +75,30 @@ int orc_set_source(int id, int ndim, double xlower) {
     return 0;
 }
 
+// Before-step routine (the example's b4step2; 0 = the reference's default
+// no-op).  1: the edge velocities (aux fields 1, 2) of the variable-velocity
+// advection solver scaled by cos(pi t / T), from an unscaled copy.
+static int g_b4 = 0;
+static double g_b4_period = 1.0;
+
+int orc_set_b4step(int id, double period) {
+    g_b4 = id;
+    g_b4_period = period;
+    return 0;
+}
+
+// b4step2 at time t: aux_out = aux_base with the velocity fields scaled
+// (aux in the reference layout aux(maux, cells)); a no-op copy for id 0.
+int orc_b4step2(int maux, long long ncells, const double* aux_base, double* aux_out, double t) {
+    const double sc = std::cos(3.141592653589793 * t / g_b4_period);
+    for (long long k = 0; k < ncells; ++k)
+        for (int ma = 0; ma < maux; ++ma) {
+            const double v = aux_base[ma + (long long)maux * k];
+            aux_out[ma + (long long)maux * k] = (g_b4 == 1 && ma < 2) ? v * sc : v;
+        }
+    return 0;
+}
+
 int orc_set_solver(int solver_id, const double* params, int nparams) {
     g_solver = solver_id;
     if (solver_id == ORC_ACOUSTICS_2D || solver_id == ORC_ACOUSTICS_1D) {
@@ -867,6 +891,10 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
     nv[1] = 0;
     const size_t nq = (size_t)meqn * (mx + 2 * mbc) * (my + 2 * mbc);
     std::vector<double> qwork(nq), qwork2(method[4] == 2 ? nq : 0);
+    // b4step2 (src/2d/claw2.f:626-631) writes a working aux from the caller's
+    const long long ncell = (long long)(mx + 2 * mbc) * (my + 2 * mbc);
+    std::vector<double> auxw(g_b4 != 0 ? (size_t)maux * ncell : 0);
+    const double* aux_step = g_b4 != 0 ? auxw.data() : aux;
     // the source routine over every row j = 1-mbc..my+mbc (0 = default no-op)
     auto src2 = [&](double* qq, double dts) {
         if (g_src != 1) return;
@@ -892,6 +920,7 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
         if (told + dt > tend && tstart < tend) dt = tend - told;
         for (;;) {
             if (orc_bc2(meqn, mbc, mx, my, q, mthbc) != 0) { info = -2; goto done; }
+            if (g_b4 != 0) orc_b4step2(maux, ncell, aux, auxw.data(), told);
             if (method[4] == 2) {
                 // src/2d/claw2.f:635-647: keep q for a retry, then dt/2 of source
                 std::memcpy(qwork2.data(), q, nq * sizeof(double));
@@ -899,10 +928,11 @@ int orc_claw2(int meqn, int mwaves, int maux, int mbc, int mx, int my, double* q
             }
             std::memcpy(qwork.data(), q, nq * sizeof(double));
             const int rc = method[2] >= 0
-                               ? orc_step2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q, aux,
-                                           dx, dy, dt, method, mthlim, use_fwaves, &cfl)
-                               : orc_dimsp2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q, aux,
-                                            dx, dy, dt, method, mthlim, cflv, use_fwaves, &cfl);
+                               ? orc_step2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q,
+                                           aux_step, dx, dy, dt, method, mthlim, use_fwaves, &cfl)
+                               : orc_dimsp2(meqn, mwaves, maux, mbc, mx, my, qwork.data(), q,
+                                            aux_step, dx, dy, dt, method, mthlim, cflv, use_fwaves,
+                                            &cfl);
             if (rc != 0) {
                 info = -1;
                 goto done;

@@ -38,6 +38,8 @@ SOLVER_PARAMS = {
 PISTON_BC = 10
 # restated source routines (examples/acoustics_2d_radial/1drad/src1.f:18-23)
 SOURCE_IDS = {"radial": 1}
+# restated before-step routines (edge velocities times cos(pi t / T))
+B4STEP_IDS = {"reversing": 1}
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -59,6 +61,10 @@ def _load(variant: str):
     lib.orc_set_solver.restype = ctypes.c_int
     lib.orc_set_source.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
     lib.orc_set_source.restype = ctypes.c_int
+    lib.orc_set_b4step.argtypes = [ctypes.c_int, ctypes.c_double]
+    lib.orc_set_b4step.restype = ctypes.c_int
+    lib.orc_b4step2.argtypes = [ctypes.c_int, ctypes.c_longlong, _D, _D, ctypes.c_double]
+    lib.orc_b4step2.restype = ctypes.c_int
     lib.orc_claw2.argtypes = [ctypes.c_int] * 6 + [_D, _D, ctypes.c_double, ctypes.c_double,
                                                    ctypes.c_double, _D, _D, _D, _I, _I, _I, _I,
                                                    ctypes.c_int]
@@ -130,7 +136,7 @@ class OracleGrid:
     """Reference-layout state of one grid driven by the CPU restatement."""
 
     def __init__(self, cd, solver: str, params: dict | None = None, variant: str = "parity",
-                 user_source: str | None = None):
+                 user_source: str | None = None, user_b4step: str | None = None):
         self.lib = _load(variant)
         self.cd = cd
         self.nd = int(cd.num_dim)
@@ -151,6 +157,8 @@ class OracleGrid:
         # the example's src routine (0 = the reference's default no-op)
         self.src = SOURCE_IDS[user_source] if user_source is not None else 0
         self.src_ndim = int(params.get("ndim", 2))
+        self.b4 = B4STEP_IDS[user_b4step] if user_b4step is not None else 0
+        self.b4_period = float(params.get("period", 1.0))
         g = tuple(n + 2 * self.mbc for n in reversed(self.cells))  # (my+4, mx+4) C order
         self.qf = np.zeros(g + (self.meqn,), dtype=np.float64)
         self.af = np.zeros(g + (max(self.maux, 1),), dtype=np.float64)
@@ -159,6 +167,7 @@ class OracleGrid:
     def _set_solver(self):
         self.lib.orc_set_solver(SOLVER_IDS[self.solver], _p(self.pv), len(self.pv))
         self.lib.orc_set_source(self.src, self.src_ndim, float(self.cd.lower[0]))
+        self.lib.orc_set_b4step(self.b4, self.b4_period)
 
     def _interior(self):
         b = self.mbc
@@ -219,14 +228,19 @@ class OracleGrid:
             mx, my = self.cells
             self.lib.orc_bc2(self.meqn, self.mbc, mx, my, _p(self.qf), _p(self.mthbc, _I))
             qold = self.qf.copy()
+            af = self.af
+            if self.b4:  # b4step2 at the step's start time, from the unscaled aux
+                af = np.empty_like(self.af)
+                self.lib.orc_b4step2(self.maux, self.af.size // max(self.maux, 1), _p(self.af),
+                                     _p(af), float(t))
             if self.method[2] >= 0:
                 rc = self.lib.orc_step2(self.meqn, self.mwaves, self.maux, self.mbc, mx, my,
-                                        _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                        _p(qold), _p(self.qf), _p(af), self.dxs[0],
                                         self.dxs[1], float(dt), _p(self.method, _I),
                                         _p(self.mthlim, _I), self.use_fwaves, ctypes.byref(cfl))
             else:
                 rc = self.lib.orc_dimsp2(self.meqn, self.mwaves, self.maux, self.mbc, mx, my,
-                                         _p(qold), _p(self.qf), _p(self.af), self.dxs[0],
+                                         _p(qold), _p(self.qf), _p(af), self.dxs[0],
                                          self.dxs[1], float(dt), _p(self.method, _I),
                                          _p(self.mthlim, _I), _p(self._cflv()), self.use_fwaves,
                                          ctypes.byref(cfl))
@@ -259,10 +273,10 @@ class OracleGrid:
 
 
 def run_oracle(rundata, solver, params, q0, aux=None, variant="parity", flush_tiny=True,
-               user_source=None):
+               user_source=None, user_b4step=None):
     """claw{1,2}ez frame loop on the oracle; returns [(frame, t, q, stats)]."""
     cd = getattr(rundata, "clawdata", rundata)
-    g = OracleGrid(cd, solver, params, variant, user_source)
+    g = OracleGrid(cd, solver, params, variant, user_source, user_b4step)
     q = np.array(q0, dtype=np.float64, copy=True)
     if flush_tiny:
         q[np.abs(q) < 1e-99] = 0.0

@@ -73,3 +73,15 @@ def test_axisymmetric_rows_follow_the_1d_radial_run(split):
         assert np.abs(q2[0, j] - f1[0]).max() < 1e-11
         assert np.abs(q2[1, j] - f1[1]).max() < 1e-11
     assert np.abs(q2[2]).max() == 0.0
+
+
+def test_b4step_reversing_flow_returns_the_annulus_data():
+    """A before-step routine (b4step2 hook, src/2d/claw2.f:626-631) that scales
+    the annulus velocities by cos(pi t / T): the data rotate forward until T/2
+    and back to their start at T, apart from the scheme's diffusion and the
+    per-step freezing of the velocity."""
+    rd, solver, _, q0, aux = problems.advection_2d_annulus(mx=40, my=120, nout=2, tfinal=1.0)
+    rd.clawdata.dt_max = 0.005
+    fr = run_oracle(rd, solver, {"period": 1.0}, q0, aux, user_b4step="reversing")
+    half, end = np.abs(fr[1][2] - q0).max(), np.abs(fr[2][2] - q0).max()
+    assert half > 0.9 and end < 0.15
