@@ -296,6 +296,83 @@ struct B4StepRunner : Runner {
     int launches_per_step() const override { return inner->launches_per_step() + 1; }
 };
 
+// --------------------------------------------------------- conserved totals ---
+// Sum over interior cells of capa * q_m (capa = 1 without a capacity
+// function) in FP64 with Neumaier's compensated summation, whatever the
+// storage precision.  Each block forms (sum, compensation) pairs over a fixed
+// range of cells; one final block adds the block pairs in order, so the result
+// does not depend on scheduling.
+constexpr int TOT_THREADS = 256, TOT_BLOCKS_MAX = 1184;
+
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+}
+
+template <typename real>
+__global__ void totals_partial_kernel(const real* __restrict__ q, const real* __restrict__ aux,
+                                      int capa, long long ld, long long fstride, long long ald,
+                                      long long afstride, int mx, int my, int mz, int dim,
+                                      int meqn, double* __restrict__ part) {
+    __shared__ double sh[2][TOT_THREADS / 32];
+    const long long rows = (long long)my * mz;
+    const long long ncell = rows * mx;
+    const long long per = (ncell + gridDim.x - 1) / gridDim.x;
+    const long long c0 = blockIdx.x * per, c1 = min(ncell, c0 + per);
+    for (int m = 0; m < meqn; ++m) {
+        double s = 0.0, c = 0.0;
+        for (long long k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+            const long long row = k / mx, i = k - row * mx;
+            double v = (double)q[m * fstride + row * ld + i];
+            if (capa > 0) {
+                // aux has two ghost layers per axis: cell (i, j, l) at (i+2, j+2, l+2)
+                const long long j = dim >= 2 ? row % my : 0, l = dim >= 3 ? row / my : 0;
+                const long long ao = (capa - 1) * afstride + (i + 2) +
+                                     (dim >= 2 ? (j + 2) * ald : 0) +
+                                     (dim >= 3 ? (l + 2) * ald * (my + 4) : 0);
+                v = (double)aux[ao] * v;
+            }
+            neumaier_add(s, c, v);
+        }
+        // fold the lanes' pairs (sum part exact by TwoSum, errors added)
+        for (int off = 16; off > 0; off >>= 1) {
+            const double s2 = __shfl_down_sync(0xffffffffu, s, off);
+            const double c2 = __shfl_down_sync(0xffffffffu, c, off);
+            const double t = s + s2;
+            const double bp = t - s;
+            const double e = (s - (t - bp)) + (s2 - bp);
+            s = t;
+            c = c + c2 + e;
+        }
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) { sh[0][w] = s; sh[1][w] = c; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double S = 0.0, C = 0.0;
+            for (int k = 0; k < TOT_THREADS / 32; ++k) {
+                neumaier_add(S, C, sh[0][k]);
+                C += sh[1][k];
+            }
+            part[(blockIdx.x * meqn + m) * 2] = S;
+            part[(blockIdx.x * meqn + m) * 2 + 1] = C;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void totals_final_kernel(const double* __restrict__ part, int nblocks, int meqn,
+                                    double* __restrict__ out) {
+    const int m = threadIdx.x;
+    if (m >= meqn) return;
+    double S = 0.0, C = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        neumaier_add(S, C, part[(b * meqn + m) * 2]);
+        C += part[(b * meqn + m) * 2 + 1];
+    }
+    out[m] = S + C;
+}
+
 struct SolverShape { int dim, meqn, mwaves, maux; };
 
 bool solver_shape(int id, SolverShape* sh) {
@@ -337,6 +414,7 @@ struct claw_handle {
     long long launches = 0;
     int device = 0;
     double t_now = 0.0;  // time of the current q (time-dependent boundary conditions)
+    double* totals_scratch = nullptr;  // block partials + result of claw_totals
 };
 
 extern "C" {
@@ -475,6 +553,7 @@ int claw_destroy(claw_handle* h) {
         if (h->g.q[k]) cudaFree(h->g.q[k]);
     if (h->g.aux) cudaFree(h->g.aux);
     if (h->g.aux_base) cudaFree(h->g.aux_base);
+    if (h->totals_scratch) cudaFree(h->totals_scratch);
     if (h->g.ctl) cudaFree(h->g.ctl);
     if (h->stage) cudaFree(h->stage);
     if (h->ctl_h) cudaFreeHost(h->ctl_h);
@@ -743,5 +822,33 @@ int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld, lo
 }
 
 long long claw_launch_count(claw_handle* h) { return h ? h->launches : 0; }
+
+int claw_totals(claw_handle* h, double* totals) {
+    if (!h || !totals) return fail(CLAW_E_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const Geometry& g = h->g;
+    const int meqn = g.meqn;
+    if (!h->totals_scratch)
+        CUDA_TRY(cudaMalloc(&h->totals_scratch, ((size_t)TOT_BLOCKS_MAX * meqn * 2 + meqn) * sizeof(double)));
+    const long long ncell = (long long)g.mx * g.my * g.mz;
+    const int nb = (int)std::max(1LL, std::min((long long)TOT_BLOCKS_MAX, (ncell + 4095) / 4096));
+    double* part = h->totals_scratch;
+    double* out = part + (size_t)TOT_BLOCKS_MAX * meqn * 2;
+    const int capa = h->cfg.capa_index;
+    if (g.es == 8)
+        totals_partial_kernel<double><<<nb, TOT_THREADS, 0, h->stream>>>(
+            static_cast<const double*>(g.q[h->cur]), static_cast<const double*>(g.aux), capa, g.ld,
+            g.fstride, g.ald, g.afstride, g.mx, g.my, g.mz, g.dim, meqn, part);
+    else
+        totals_partial_kernel<float><<<nb, TOT_THREADS, 0, h->stream>>>(
+            static_cast<const float*>(g.q[h->cur]), static_cast<const float*>(g.aux), capa, g.ld,
+            g.fstride, g.ald, g.afstride, g.mx, g.my, g.mz, g.dim, meqn, part);
+    CUDA_TRY(cudaGetLastError());
+    totals_final_kernel<<<1, 32, 0, h->stream>>>(part, nb, meqn, out);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(totals, out, meqn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
 
 }  // extern "C"

@@ -46,6 +46,8 @@ std::unique_ptr<Runner> make_char_runner(const claw_config& cfg);
 // 2D dimensionally split step (step2ds.cuh, one fused launch per step);
 // nullptr if cfg is not served.
 std::unique_ptr<Runner> make_split_runner(const claw_config& cfg);
+// its fused-multiply-add / FP32 build (split2d_fast.cu)
+std::unique_ptr<Runner> make_fast_split_runner(const claw_config& cfg);
 
 // 3D step (step3d.cuh: one launch per sweep); nullptr if cfg is not served.
 std::unique_ptr<Runner> make_runner3d(const claw_config& cfg);

@@ -1,137 +1,14 @@
-// Runner of the fused 2D dimensionally split step (step2ds.cuh), built in the
-// reference's order of operations (--fmad=false): dimensional_split = 1
-// (Godunov, method(3) = -1) and 2 (Strang, method(3) = -2), src/2d/claw2ez.f:126.
-#include <algorithm>
-#include <cmath>
-#include <cstring>
-
-#include "host.h"
-#include "riemann.cuh"
-#include "step2ds.cuh"
+// The 2D dimensionally split step in the reference's order of operations
+// (--fmad=false): bit-identical to the oracle's dimsp2 / step2ds.  FP32 and
+// fused FP64 go to the contracted build (split2d_fast.cu).
+#include "split2d_runner.cuh"
 
 namespace clawb200 {
-namespace {
-
-template <class S, class M, bool STRANG, bool SRC = false>
-struct SplitRunner2D : Runner {
-    using L = SplitLayout<S, STRANG>;
-    Step2Args<S> args;
-    int grid = 1, smem = 0;
-
-    explicit SplitRunner2D(const S& s) { std::memset(&args, 0, sizeof(args)); args.solver = s; }
-
-    int prepare(const claw_config& cfg, const Geometry& g) override {
-        args.q[0] = static_cast<typename S::real*>(g.q[0]);
-        args.q[1] = static_cast<typename S::real*>(g.q[1]);
-        args.aux = static_cast<const typename S::real*>(g.aux);
-        args.ld = g.ld;
-        args.fstride = g.fstride;
-        args.ald = g.ald;
-        args.afstride = g.afstride;
-        args.mx = g.mx;
-        args.my = g.my;
-        args.nstrips = (g.mx + L::STRIPW - 1) / L::STRIPW;
-        args.bc[0] = cfg.bc_lower[0];
-        args.bc[1] = cfg.bc_upper[0];
-        args.bc[2] = cfg.bc_lower[1];
-        args.bc[3] = cfg.bc_upper[1];
-        for (int k = 0; k < 8; ++k) args.mthlim[k] = k < cfg.num_waves ? cfg.limiter[k] : 0;
-        args.order = cfg.order;
-        args.trans = -cfg.dimensional_split;
-        args.fwave = cfg.use_fwaves;
-        args.capa = cfg.capa_index;
-        args.dx = g.dx;
-        args.dy = g.dy;
-        args.ctl = g.ctl;
-        args.src_split = (SRC && cfg.source_id == CLAW_SOURCE_RADIAL) ? cfg.source_split : 0;
-        args.src_nd1 = (double)(cfg.source_ndim - 1);
-        args.src_bulk = cfg.solver_params[1];
-        args.xlower = cfg.lower[0];
-        for (int k = 0; k < 2; ++k) {
-            int rc = make_map3(&args.tmq[k], g.q[k], g.es, g.mx, g.my, S::meqn, g.ld, g.fstride,
-                               L::W, 1, S::meqn);
-            if (rc) return rc;
-        }
-        if (S::maux > 0) {
-            int rc = make_map3(&args.tmaux, g.aux, g.es, g.mx + 4, g.my + 4, S::maux, g.ald,
-                               g.afstride, L::W, 1, S::maux);
-            if (rc) return rc;
-        }
-        smem = L::SMEM;
-        auto kern = split2_kernel<S, M, STRANG, SRC>;
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        int dev = 0, nsm = 0, per_sm = 0;
-        CUDA_TRY(cudaGetDevice(&dev));
-        CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * WARPS2D, smem));
-        if (per_sm < 1) return fail(CLAW_E_CUDA, "split step kernel cannot be resident on an SM");
-        args.units = (long long)args.nstrips * g.my;
-        // at least ~48 rows of one strip per warp: the 4-row prologue of a
-        // chunk stays a small fraction of its work
-        const long long want = std::max(1LL, args.units / 48);
-        const long long full = (long long)nsm * per_sm * WARPS2D;
-        const long long nw = std::min(full, want);
-        grid = (int)((nw + WARPS2D - 1) / WARPS2D);
-        args.nwarps = (int)nw;
-        return 0;
-    }
-
-    cudaError_t launch(cudaStream_t s) override {
-        split2_kernel<S, M, STRANG, SRC><<<grid, 32 * WARPS2D, smem, s>>>(args);
-        return cudaGetLastError();
-    }
-};
-
-template <class S>
-std::unique_ptr<Runner> split_for(const claw_config& cfg, const S& s) {
-    if constexpr (std::is_same<S, Acoustics2D<typename S::real>>::value) {
-        if (cfg.source_id == CLAW_SOURCE_RADIAL && cfg.source_split != 0) {
-            if (cfg.dimensional_split == 2)
-                return std::unique_ptr<Runner>(new SplitRunner2D<S, MethodGeneric2D, true, true>(s));
-            return std::unique_ptr<Runner>(new SplitRunner2D<S, MethodGeneric2D, false, true>(s));
-        }
-    }
-    bool mc = cfg.order == 2 && cfg.capa_index == 0 && !cfg.use_fwaves;
-    for (int k = 0; k < cfg.num_waves; ++k) mc = mc && cfg.limiter[k] == 4;
-    // order 2, MC, no capacity, no f-waves: the specialised policy; the
-    // transverse code is unused by the split kernels
-    using MC = Method2D<2, -1, 4, 0, 0>;
-    if (cfg.dimensional_split == 2) {
-        if (mc) return std::unique_ptr<Runner>(new SplitRunner2D<S, MC, true>(s));
-        return std::unique_ptr<Runner>(new SplitRunner2D<S, MethodGeneric2D, true>(s));
-    }
-    if (mc) return std::unique_ptr<Runner>(new SplitRunner2D<S, MC, false>(s));
-    return std::unique_ptr<Runner>(new SplitRunner2D<S, MethodGeneric2D, false>(s));
-}
-
-template <typename real>
-std::unique_ptr<Runner> split_runner(const claw_config& cfg) {
-    switch (cfg.solver_id) {
-        case CLAW_SOLVER_ACOUSTICS_2D: {
-            const double rho = cfg.solver_params[0], bulk = cfg.solver_params[1];
-            const double cc = std::sqrt(bulk / rho), zz = rho * cc, hz = 0.5 / zz;
-            return split_for(cfg, Acoustics2D<real>{(real)cc, (real)zz, (real)hz});
-        }
-        case CLAW_SOLVER_EULER_ROE_2D: {
-            const double gamma = cfg.solver_params[0];
-            return split_for(cfg, EulerRoe2D<real>{(real)gamma, (real)(gamma - 1.0)});
-        }
-        case CLAW_SOLVER_VC_ADVECTION_2D:
-            return std::unique_ptr<Runner>(
-                cfg.dimensional_split == 2
-                    ? static_cast<Runner*>(new SplitRunner2D<VCAdvection2D<real>, MethodGeneric2D, true>({}))
-                    : static_cast<Runner*>(new SplitRunner2D<VCAdvection2D<real>, MethodGeneric2D, false>({})));
-        default:
-            return nullptr;
-    }
-}
-
-}  // namespace
 
 std::unique_ptr<Runner> make_split_runner(const claw_config& cfg) {
     if (cfg.num_dim != 2 || cfg.dimensional_split <= 0) return nullptr;
-    if (cfg.precision == CLAW_FP32) return split_runner<float>(cfg);
-    return split_runner<double>(cfg);
+    if (cfg.precision != CLAW_FP64) return make_fast_split_runner(cfg);
+    return split_runner_for<double, 0>(cfg);
 }
 
 }  // namespace clawb200

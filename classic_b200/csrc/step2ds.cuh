@@ -531,7 +531,9 @@ __device__ __forceinline__ void cta_split_cfl_and_control(ClawCtl* ctl, const do
     }
 }
 
-template <class S, class M, bool STRANG, bool SRC = false>
+// BUILD tells apart the instantiations of the reference-order unit (0) and the
+// contracted unit (1), which must not share a symbol.
+template <class S, class M, bool STRANG, bool SRC, int BUILD>
 __global__ void __launch_bounds__(32 * WARPS2D, step2_minb<S>::value)
 split2_kernel(const __grid_constant__ Step2Args<S> A) {
     using L = SplitLayout<S, STRANG>;

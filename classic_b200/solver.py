@@ -185,6 +185,12 @@ class Solver:
     def launch_count(self) -> int:
         return int(self.lib.claw_launch_count(self._h))
 
+    def totals(self) -> np.ndarray:
+        """Conserved totals sum(capa * q_m) per field, FP64 compensated sums."""
+        out = np.zeros(self.meqn)
+        check(self.lib.claw_totals(self._h, _dptr(out)), "claw_totals")
+        return out
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             self.lib.claw_destroy(self._h)

@@ -192,6 +192,14 @@ int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld,
 /* Number of step-kernel launches issued on this handle so far. */
 long long claw_launch_count(claw_handle* h);
 
+/* Conserved totals of the current q: totals[m] = sum over interior cells of
+ * capa * q_m (capa = 1 without a capacity function), formed in FP64 with
+ * Neumaier's compensated summation whatever the storage precision, in a fixed
+ * order (the same q gives the same bits).  No counterpart in the reference,
+ * whose regression checks sum frames on the host; the FP32 path keeps its
+ * conservation sums in FP64 this way. */
+int claw_totals(claw_handle* h, double* totals);
+
 /* One 2D step (bc2 + step2, FP64) from caller-owned device buffers, with no
  * device allocation.  No counterpart in the reference: it serves callers that
  * cannot call cudaMalloc -- codes whose device memory all comes from their own

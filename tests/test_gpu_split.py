@@ -261,3 +261,31 @@ def test_3d_fp32_tracks_fp64():
     assert abs(sg["t_reached"] - so["t_reached"]) < 1e-12
     assert np.all(rel_diff(g.get_q(), o.get_q()) <= 5e-5)
     g.close()
+
+
+@pytest.mark.parametrize("split", SPLITS)
+def test_fused_fp64_within_1e12(split):
+    """CLAW_FP64_FMA: the split kernels built with contraction."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=200, nout=1, tfinal=0.05)
+    rd.clawdata.dimensional_split = split
+    g, o = _pair(rd, solver, params, q0, precision="fp64_fma")
+    ig, sg = g.advance(0.0, 0.05, 0.004)
+    io, so = o.advance(0.0, 0.05, 0.004)
+    assert ig == io == 0
+    for key in ("t_reached", "dt_next", "steps_taken", "cfl_max_seen"):
+        assert sg[key] == so[key], key
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 1e-12)
+    g.close()
+
+
+def test_3d_fused_fp64_within_1e12():
+    rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=40)
+    rd.clawdata.dimensional_split = "godunov"
+    g, o = _pair(rd, solver, params, q0, aux, precision="fp64_fma")
+    ig, sg = g.advance(0.0, 0.1, 0.01)
+    io, so = o.advance(0.0, 0.1, 0.01)
+    assert ig == io == 0
+    for key in ("t_reached", "dt_next", "steps_taken"):
+        assert sg[key] == so[key], key
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 1e-12)
+    g.close()
