@@ -229,6 +229,7 @@ def other_configs(peaks):
         b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4})
         for k, inst in enumerate(insts):
             b.set_q(k, inst[3])
+        shape = b.autotune(repeats=2)  # launch shape chosen before the timed run
         info, st = b.advance(0.0, 0.25)
         b.close()
         upd = sum(nn * nn * (x["steps_taken"] + x["steps_rejected"]) for nn, x in zip(sizes, st))
@@ -236,7 +237,9 @@ def other_configs(peaks):
         out["euler_batch_256"] = {"cell_updates_per_s": upd / (ms * 1e-3), "cell_updates": upd,
                                   "device_ms": ms, "launches": st[0]["launches"],
                                   "steps_min_max": [min(x["steps_taken"] for x in st),
-                                                    max(x["steps_taken"] for x in st)]}
+                                                    max(x["steps_taken"] for x in st)],
+                                  "autotuned_shape": {"min_rows": shape["min_rows"],
+                                                      "ctas_per_sm": shape["ctas_per_sm"]}}
     except Exception as e:
         out["euler_batch_256"] = {"error": str(e)}
     return out

@@ -113,6 +113,10 @@ SIGNATURES = {
     "claw_batch_destroy": (ctypes.c_int, [_P]),
     "claw_batch_set_q": (ctypes.c_int, [_P, ctypes.c_int, _D]),
     "claw_batch_get_q": (ctypes.c_int, [_P, ctypes.c_int, _D]),
+    "claw_batch_autotune": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_double)]),
+    "claw_batch_set_shape": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "claw_batch_advance": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, _D,
                                           ctypes.POINTER(ClawStats)]),
     "claw_last_error": (ctypes.c_char_p, []),

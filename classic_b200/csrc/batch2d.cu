@@ -29,6 +29,10 @@ struct BatchRunner {
     virtual int prepare(const std::vector<Geometry>& g, const claw_config* cfgs, ClawCtl* ctls,
                         int* active, int* err) = 0;
     virtual cudaError_t launch(cudaStream_t s) = 0;
+    // launch shape: tile height (rows per warp at least) and CTAs per SM
+    virtual void set_shape(int min_rows, int ctas_per_sm) = 0;
+    virtual int max_ctas_per_sm() const = 0;
+    int min_rows = 48, ctas_per_sm = 0;
 };
 
 template <class S, class M>
@@ -105,16 +109,27 @@ struct BatchRunnerT : BatchRunner {
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_batch_kernel<S, M>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "batch kernel cannot be resident on an SM");
-        grid = nsm * per_sm;
+        nsm_ = nsm;
+        per_sm_ = per_sm;
         b.inst = inst_d;
         b.ctls = ctls;
         b.units = units_d;
         b.count = n;
-        b.nwarps = grid * WARPS2D;
         b.active = active;
         b.err = err;
+        set_shape(48, per_sm);
         return 0;
     }
+
+    void set_shape(int rows, int ctas) override {
+        min_rows = std::max(1, rows);
+        ctas_per_sm = std::max(1, std::min(ctas, per_sm_));
+        grid = nsm_ * ctas_per_sm;
+        b.nwarps = grid * WARPS2D;
+        b.min_rows = min_rows;
+    }
+    int max_ctas_per_sm() const override { return per_sm_; }
+    int nsm_ = 1, per_sm_ = 1;
 
     cudaError_t launch(cudaStream_t s) override {
         step2_batch_kernel<S, M><<<grid, 32 * WARPS2D, smem, s>>>(b);
@@ -426,6 +441,106 @@ int claw_batch_advance(claw_batch* b, double tstart, double tend, const double* 
     }
     if (first < 0) return fail(first, "device error in the batch");
     return first;
+}
+
+int claw_batch_autotune(claw_batch* b, const double* dt_trial, int repeats, int* min_rows,
+                        int* ctas_per_sm, double* ms_per_step) {
+    if (!b) return fail(CLAW_E_INVALID, "null batch");
+    if (repeats < 1) repeats = 1;
+    CUDA_TRY(cudaSetDevice(b->device));
+    const int n = (int)b->g.size();
+    // trial steps start every instance afresh from its current q: the kernel
+    // reads q[cur] and writes q[cur ^ 1], and the saved control blocks are
+    // put back before every trial and at the end, so the state is unchanged
+    std::vector<ClawCtl> saved(b->ctl_h, b->ctl_h + n), trial(n);
+    for (int k = 0; k < n; ++k) {
+        const claw_config& cfg = b->cfgs[k];
+        ClawCtl& c = trial[k];
+        std::memset(&c, 0, sizeof(ClawCtl));
+        c.cur = saved[k].cur;
+        c.tend = 1e300;
+        c.dt = dt_trial ? dt_trial[k] : cfg.dt_initial;
+        c.dt_max = cfg.dt_max;
+        c.cfl_max = cfg.cfl_max;
+        c.cfl_desired = cfg.cfl_desired;
+        c.dtmin = c.dtmax = c.dt;
+        c.mode = CTL_ADVANCE;
+        c.dt_variable = cfg.dt_variable ? 1 : 0;
+        c.maxn = 1;
+    }
+    // Two regimes: while many instances run, the launch is full whatever the
+    // tile height and the CTA count decides; once only the largest ones are
+    // left (the tail of an uneven ensemble) the tile height decides how many
+    // warps share them.  The CTA count is tuned on a step of every instance,
+    // the tile height on a step of the largest instance alone.
+    std::vector<ClawCtl> tail = trial;
+    int big = 0;
+    for (int k = 1; k < n; ++k)
+        if ((long long)b->g[k].mx * b->g[k].my > (long long)b->g[big].mx * b->g[big].my) big = k;
+    for (int k = 0; k < n; ++k) tail[k].done = k == big ? 0 : 1;
+    auto time_step = [&](const std::vector<ClawCtl>& st, int active, float* out) -> int {
+        float tmin = 1e30f;
+        for (int r = 0; r < repeats; ++r) {
+            std::memcpy(b->ctl_h, st.data(), sizeof(ClawCtl) * n);
+            CUDA_TRY(cudaMemcpyAsync(b->ctl_d, b->ctl_h, sizeof(ClawCtl) * n, cudaMemcpyHostToDevice,
+                                     b->stream));
+            b->flags_h[0] = active;
+            b->flags_h[1] = 0;
+            CUDA_TRY(cudaMemcpyAsync(b->flags_d, b->flags_h, 2 * sizeof(int), cudaMemcpyHostToDevice,
+                                     b->stream));
+            CUDA_TRY(cudaEventRecord(b->ev0, b->stream));
+            CUDA_TRY(b->runner->launch(b->stream));
+            CUDA_TRY(cudaEventRecord(b->ev1, b->stream));
+            CUDA_TRY(cudaEventSynchronize(b->ev1));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+            tmin = std::min(tmin, ms);
+        }
+        *out = tmin;
+        return 0;
+    };
+    const int maxc = b->runner->max_ctas_per_sm();
+    float best = 1e30f, best_tail = 1e30f;
+    int best_ctas = maxc, best_rows = 48;
+    for (int ctas = maxc; ctas >= 1 && ctas >= maxc / 2; --ctas) {
+        b->runner->set_shape(48, ctas);
+        float t = 0.f;
+        int rc = time_step(trial, n, &t);
+        if (rc) return rc;
+        if (t < best) { best = t; best_ctas = ctas; }
+    }
+    const int rows_cand[] = {16, 24, 32, 48, 96, 192};
+    for (int rows : rows_cand) {
+        b->runner->set_shape(rows, best_ctas);
+        float t = 0.f;
+        int rc = time_step(tail, 1, &t);
+        if (rc) return rc;
+        if (t < best_tail) { best_tail = t; best_rows = rows; }
+    }
+    b->runner->set_shape(best_rows, best_ctas);
+    if (b->gexec) {  // the captured time loop holds the old launch shape
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+        b->gsteps = 0;
+    }
+    std::memcpy(b->ctl_h, saved.data(), sizeof(ClawCtl) * n);
+    CUDA_TRY(cudaMemcpyAsync(b->ctl_d, b->ctl_h, sizeof(ClawCtl) * n, cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    if (min_rows) *min_rows = best_rows;
+    if (ctas_per_sm) *ctas_per_sm = best_ctas;
+    if (ms_per_step) *ms_per_step = best;
+    return 0;
+}
+
+int claw_batch_set_shape(claw_batch* b, int min_rows, int ctas_per_sm) {
+    if (!b || min_rows < 1 || ctas_per_sm < 1) return fail(CLAW_E_INVALID, "bad argument");
+    b->runner->set_shape(min_rows, ctas_per_sm);
+    if (b->gexec) {
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+        b->gsteps = 0;
+    }
+    return 0;
 }
 
 }  // extern "C"

@@ -736,6 +736,7 @@ struct Step2Batch {
     const int* units;          // [count] strips * my
     int count;
     int nwarps;                // warps of the launch
+    int min_rows;              // tile height: fewest rows a sharing warp takes
     int* active;               // instances still advancing (polled by the host)
     int* err;                  // device error flags of the batch
 };
@@ -768,8 +769,8 @@ step2_batch_kernel(const __grid_constant__ Step2Batch<S> B) {
     __syncthreads();
     const long long total = pre[B.count];
     if (total == 0) return;
-    // every sharing warp gets >= ~48 rows, as in the single-grid launch
-    const long long nw = min((long long)B.nwarps, max(1LL, total / 48));
+    // every sharing warp gets >= min_rows rows of a strip (tile height, tuned)
+    const long long nw = min((long long)B.nwarps, max(1LL, total / B.min_rows));
     const long long gw = (long long)blockIdx.x * WARPS2D + warp;
     if (gw >= nw) return;
 

@@ -348,6 +348,24 @@ class BatchSolver:
         check(self.lib.claw_batch_get_q(self._h, k, _dptr(out)), "claw_batch_get_q")
         return out
 
+    def autotune(self, dt_trial=None, repeats: int = 3) -> dict:
+        """Choose the batch launch shape (tile height in rows, CTAs per SM) by
+        timing one step of every instance per candidate; the state is left as
+        it was.  Returns the chosen shape and its time per step."""
+        dts = None
+        if dt_trial is not None:
+            dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt_trial, dtype=np.float64),
+                                                       (self.count,)))
+        rows, ctas, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(self.lib.claw_batch_autotune(self._h, _dptr(dts) if dts is not None else None,
+                                           int(repeats), ctypes.byref(rows), ctypes.byref(ctas),
+                                           ctypes.byref(ms)), "claw_batch_autotune")
+        return {"min_rows": rows.value, "ctas_per_sm": ctas.value, "ms_per_step": ms.value}
+
+    def set_shape(self, min_rows: int, ctas_per_sm: int):
+        check(self.lib.claw_batch_set_shape(self._h, int(min_rows), int(ctas_per_sm)),
+              "claw_batch_set_shape")
+
     def advance(self, tstart: float, tend: float, dt_initial=None):
         """Advance every instance; returns (first nonzero info or 0, [stats])."""
         st = (ClawStats * self.count)()

@@ -240,6 +240,19 @@ int claw_batch_get_q(claw_batch* b, int k, double* q);
 int claw_batch_advance(claw_batch* b, double tstart, double tend, const double* dt_initial,
                        claw_stats* stats);
 
+/* Autotuner of the batch launch shape.  It times trial steps from the
+ * instances' current q with dt_trial[k] (NULL: each config's dt_initial), min
+ * over `repeats`: the CTA count per SM (the resident maximum down to half) on
+ * a step of every instance, then the tile height (16 .. 192 rows of a
+ * 28-column strip per warp, at least) on a step of the largest instance alone,
+ * the regime that ends an uneven ensemble.  It keeps the fastest shape and
+ * returns it with the full step's time.  The trial steps leave q and the
+ * instances' state as they were.  No counterpart in the reference. */
+int claw_batch_autotune(claw_batch* b, const double* dt_trial, int repeats, int* min_rows,
+                        int* ctas_per_sm, double* ms_per_step);
+/* Set the launch shape directly (a shape kept from an earlier tuning run). */
+int claw_batch_set_shape(claw_batch* b, int min_rows, int ctas_per_sm);
+
 /* Last error message of the calling thread ("" if none). */
 const char* claw_last_error(void);
 

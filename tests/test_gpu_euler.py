@@ -118,3 +118,47 @@ def test_batch_rejects_mixed_methods():
     rd2 = problems.euler_quadrants(n=16, limiter="minmod")[0]
     with pytest.raises(Exception):
         BatchSolver([rd1, rd2], "euler_roe_2d", {"gamma": 1.4})
+
+
+def test_batch_autotune_keeps_state_and_results():
+    """The autotuner's trial steps leave every instance's q as it was, and the
+    tuned launch shape gives the same bits as the default one."""
+    sizes = [40, 23, 57, 64, 29, 45, 33, 50, 96, 120]
+    insts = _ensemble(sizes, seed0=500)
+    rds = [i[0] for i in insts]
+    runs = []
+    for tune in (False, True):
+        b = BatchSolver(rds, "euler_roe_2d", {"gamma": 1.4})
+        for k, inst in enumerate(insts):
+            b.set_q(k, inst[3])
+        if tune:
+            shape = b.autotune(repeats=2)
+            assert shape["min_rows"] in (16, 24, 32, 48, 96, 192)
+            assert shape["ctas_per_sm"] >= 1 and shape["ms_per_step"] > 0
+            for k, inst in enumerate(insts):
+                assert same(b.get_q(k), inst[3]), k
+        info, stats = b.advance(0.0, 0.1)
+        assert info == 0
+        runs.append(([b.get_q(k) for k in range(len(insts))], [s["steps_taken"] for s in stats]))
+        b.close()
+    assert runs[0][1] == runs[1][1]
+    for a, c in zip(runs[0][0], runs[1][0]):
+        assert same(a, c)
+
+
+@pytest.mark.parametrize("rows,ctas", [(16, 1), (384, 2)])
+def test_batch_shapes_agree(rows, ctas):
+    sizes = [33, 70, 41]
+    insts = _ensemble(sizes, seed0=700)
+    b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4})
+    b.set_shape(rows, ctas)
+    for k, inst in enumerate(insts):
+        b.set_q(k, inst[3])
+    info, stats = b.advance(0.0, 0.05)
+    assert info == 0
+    for k, (rd, solver, params, q0, _) in enumerate(insts):
+        o = OracleGrid(rd.clawdata, solver, params)
+        o.set_q(q0)
+        o.advance(0.0, 0.05, rd.clawdata.dt_initial)
+        assert same(b.get_q(k), o.get_q()), k
+    b.close()
