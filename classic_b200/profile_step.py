@@ -3,8 +3,10 @@
 
     python -m classic_b200.profile_step --n 3072 --steps 4 --precision fp64_fma
     python -m classic_b200.profile_step --dim 3 --n 128 --steps 2
+    python -m classic_b200.profile_step --n 2048 --split godunov --precision fp64
 
-Each step is one claw_step (bc + step2 / step3) of fixed dt = 0.9 dx / c_max.
+Each step is one claw_step (bc + step2 / step3, or the dimensionally split
+step with --split) of fixed dt = 0.9 dx / c_max.
 """
 import argparse
 
@@ -18,6 +20,7 @@ def main():
     ap.add_argument("--n", type=int, default=3072)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", default="fp64_fma", choices=["fp64", "fp64_fma", "fp32"])
+    ap.add_argument("--split", default="unsplit", choices=["unsplit", "godunov", "strang"])
     args = ap.parse_args()
     if args.dim == 2:
         rd, solver, params, q0, aux = problems.radial_acoustics_2d(n=args.n)
@@ -26,7 +29,8 @@ def main():
     else:
         rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=args.n)
         cmax = 1.0
-        prec = "fp64"
+        prec = "fp64" if args.split == "unsplit" else args.precision
+    rd.clawdata.dimensional_split = args.split
     s = Solver(rd.clawdata, solver, params, precision=prec)
     s.set_q(q0)
     if aux is not None:
@@ -34,7 +38,8 @@ def main():
     dt = 0.9 * (2.0 / args.n) / cmax
     for _ in range(args.steps):
         s.step(dt)
-    print(f"{args.steps} steps of {args.n}^{args.dim} ({prec}), sum p = {s.get_q()[0].sum():.12e}")
+    print(f"{args.steps} steps of {args.n}^{args.dim} ({prec}, {args.split}), "
+          f"sum p = {s.get_q()[0].sum():.12e}")
     s.close()
 
 
