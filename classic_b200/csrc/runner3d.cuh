@@ -137,14 +137,17 @@ struct SplitRunner3D : Runner {
         args.nstripx = (g.mx + DS3_STRIPX - 1) / DS3_STRIPX;
         args.nstrip32 = (int)((px + 31) / 32);
         args.ctl = g.ctl;
-        CUDA_TRY(cudaMalloc(&scratch, (size_t)args.pfstride * 4 * sizeof(real)));
+        // P: the four fields after the x-sweep; P2: p and v after the y-sweep
+        CUDA_TRY(cudaMalloc(&scratch, (size_t)args.pfstride * 6 * sizeof(real)));
         args.P = scratch;
+        args.P2 = scratch + (size_t)args.pfstride * 4;
+        for (int d = 0; d < 3; ++d) args.nchunk[d] = (args.m[d] + DS3_CHUNK - 1) / DS3_CHUNK;
         int dev = 0, nsm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         const long long ux = (long long)args.nstripx * py * pz;
-        const long long uy = (long long)args.nstrip32 * pz;
-        const long long uz = (long long)args.nstrip32 * py;
+        const long long uy = (long long)args.nstrip32 * pz * args.nchunk[1];
+        const long long uz = (long long)args.nstrip32 * py * args.nchunk[2];
         auto ctas = [&](long long units, long long cap) {
             return (int)std::max(1LL, std::min(cap, (units + DS3_WARPS - 1) / DS3_WARPS));
         };

@@ -8,17 +8,17 @@
 // The x-sweep updates the slices j = 0..my+1, k = 0..mz+1 (one ghost layer
 // across), the y-sweep i = 0..mx+1, k = 0..mz+1 and the z-sweep i = 0..mx+1,
 // j = 0..my+1; every other ghost cell keeps its bc3 value for the whole step.
-// The intermediate state lives in a scratch array P over cells 0..m+1 of each
+// The intermediate state lives in scratch arrays over cells 0..m+1 of each
 // axis:
 //   X  reads q (interior cells, ghost values from the boundary maps) and
 //      writes P: x-updated for i = 1..mx, bc3 values for i = 0, mx+1;
-//   Y  updates p and v of P in place along columns (a warp owns a column
-//      range for the whole march, so nothing else reads what it writes);
-//   Z  reads P (bc3 values beyond it) and writes the interior of the new q.
+//   Y  reads P and writes the y-updated p and v of cells j = 1..my to P2;
+//   Z  reads P / P2 (bc3 values beyond them) and writes the new q's interior.
 // Lanes of a warp hold consecutive x positions: X exchanges neighbours by
-// shuffle, Y and Z march along y or z with every lane on its own slice, so
-// all global accesses are coalesced.  Each sweep's Courant maximum is kept
-// apart and the z-sweep's last CTA combines them as dimsp3 does.
+// shuffle, Y and Z march chunks of 32 cells along y or z with every lane on
+// its own slice, so all global accesses are coalesced and no warp reads what
+// another writes.  Each sweep's Courant maximum is kept apart and the
+// z-sweep's last CTA combines them as dimsp3 does.
 //
 // Arithmetic per value is flux3's / step3ds's, so the FP64 result is
 // bit-identical to the reference order of operations (built with
@@ -32,12 +32,14 @@ namespace clawb200 {
 
 constexpr int DS3_WARPS = 8;      // warps per CTA of the split sweeps
 constexpr int DS3_STRIPX = 28;    // x-sweep output columns per warp (lanes 2..29)
+constexpr int DS3_CHUNK = 32;     // y- and z-sweep cells per warp march
 
 template <typename real>
 struct Split3Args {
     const real* q[2];    // interior cells (the handle's two buffers)
     real* qw[2];
-    real* P;             // scratch: cells 0..m+1 of every axis
+    real* P;             // scratch: cells 0..m+1 of every axis (after the x-sweep)
+    real* P2;            // p and v after the y-sweep (cells 1..my of each column)
     const real* aux;     // (Z, c), two ghost layers
     long long qs[3], fstride;
     long long ps[3], pfstride;
@@ -49,6 +51,7 @@ struct Split3Args {
     double d[3];
     double xlower, ylower;
     int nstripx, nstrip32;
+    int nchunk[3];       // march chunks along y and z
     ClawCtl* ctl;
 };
 
@@ -215,11 +218,13 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_x_kernel(const Split3Ar
 }
 
 // --------------------------------------------------------- y- and z-sweep ---
-// AX = 1: columns (i, k), march along j, update p and v of P in place.
+// AX = 1: columns (i, k), march along j, write p and v of cells 1..my to P2.
 // AX = 2: columns (i, j), march along k, write the new q's interior; the last
 // CTA combines the three sweeps' Courant numbers and runs claw3's controller.
+// A warp marches DS3_CHUNK cells of 32 columns (two cells of halo either side
+// are re-solved), so no warp reads what another writes.
 template <class S, int AX, int BUILD>
-__global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3Args<typename S::real> a) {
+__global__ void __launch_bounds__(32 * DS3_WARPS, 2) split3_yz_kernel(const Split3Args<typename S::real> a) {
     using real = typename S::real;
     __shared__ double red[DS3_WARPS];
     ClawCtl* ctl = a.ctl;
@@ -229,7 +234,8 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3A
     const double tbc = *(volatile double*)&ctl->told;
     const real* __restrict__ q = a.q[cur];
     real* __restrict__ qn = a.qw[cur ^ 1];
-    real* __restrict__ P = a.P;
+    const real* __restrict__ P = a.P;
+    real* __restrict__ P2 = a.P2;
     const double tn_d = dt / a.d[AX];
     const real tn = (real)tn_d;
     const real dtdxave = real(0.5) * (tn + tn);
@@ -237,14 +243,18 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3A
     const int mA = a.m[AX];                 // along the march
     const int mO = AX == 1 ? mz : my;       // the other transverse axis
     const int lane = threadIdx.x & 31;
-    const long long units = (long long)a.nstrip32 * (mO + 2);
+    const int nch = a.nchunk[AX];
+    const long long units = (long long)a.nstrip32 * (mO + 2) * nch;
     const long long nwarps = (long long)gridDim.x * DS3_WARPS;
     constexpr int CN = 1 + AX;              // normal velocity component
     double cfl = 0.0;
 
     for (long long u = (long long)blockIdx.x * DS3_WARPS + (threadIdx.x >> 5); u < units; u += nwarps) {
         const int sx = (int)(u % a.nstrip32);
-        const int o = (int)(u / a.nstrip32);
+        const long long rest = u / a.nstrip32;
+        const int ch = (int)(rest % nch);
+        const int o = (int)(rest / nch);
+        const int c_lo = 1 + ch * DS3_CHUNK, c_hi = min(mA, c_lo + DS3_CHUNK - 1);
         const int i = sx * 32 + lane;       // 0..mx+1 valid
         const bool live = i <= mx + 1;
         const int ic = min(i, mx + 1);
@@ -259,8 +269,13 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3A
             cell(t, ci, cj, ck);
             if (t >= 0 && t <= mA + 1) {
                 const long long po = ds3_p_off(a, ci, cj, ck);
-                v[0] = P[po];
-                v[1] = P[po + CN * a.pfstride];
+                if (AX == 2 && cj >= 1 && cj <= my) {
+                    v[0] = P2[po];                     // y-updated p
+                    v[1] = P[po + CN * a.pfstride];    // w, untouched by the y-sweep
+                } else {
+                    v[0] = P[po];
+                    v[1] = P[po + CN * a.pfstride];
+                }
             } else {
                 real r[4];
                 ds3_raw(a, q, ci, cj, ck, tbc, r);
@@ -275,18 +290,18 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3A
         real vp[2], vt[2], zp[2], zt[2];    // cells t-2, t-1
         real w[2][2], s[2], am[2], ap[2];   // interface t-2|t-1
         real dl0 = 0, dl1 = 0, P1[2] = {0, 0}, Fp[2] = {0, 0};
-        load(-1, vp, zp);
-        load(0, vt, zt);
+        load(c_lo - 2, vp, zp);
+        load(c_lo - 1, vt, zt);
         S::rpn(vp[0], vp[1], vt[0], vt[1], zp[0], zp[1], zt[0], zt[1], w, s, am, ap);
         real vn[2], zn[2];
-        load(1, vn, zn);
-        for (int t = 1; t <= mA + 2; ++t) {
+        load(c_lo, vn, zn);
+        for (int t = c_lo; t <= c_hi + 2; ++t) {
             // prefetch t+1 while working on t
             real vf[2] = {0, 0}, zf[2] = {0, 0};
-            if (t + 1 <= mA + 2) load(t + 1, vf, zf);
+            if (t + 1 <= c_hi + 2) load(t + 1, vf, zf);
             real wn[2][2], sn[2], amn[2], apn[2];
             S::rpn(vt[0], vt[1], vn[0], vn[1], zt[0], zt[1], zn[0], zn[1], wn, sn, amn, apn);
-            if (live && t <= mA + 1) {      // interface t-1|t, t = 1..m+1
+            if (live && t >= 1 && t <= mA + 1) {  // interface t-1|t, t = 1..m+1
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     const double c = tn_d * (double)sn[kk];
@@ -299,7 +314,7 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3A
             if (a.order == 2) ds3_flux(a, w, s, dl0, dl1, dr0, dr1, dtdxave, F);
             // cell c = t-2: step3ds.f90:220-226 / 304-310 / 388-394
             const int c = t - 2;
-            if (live && c >= 1 && c <= mA) {
+            if (live && c >= c_lo && c <= c_hi) {
                 const real qa0 = P1[0] - tn * am[0];
                 const real qa1 = P1[1] - tn * am[1];
                 const real np0 = (vp[0] + qa0) - tn * (F[0] - Fp[0]);
@@ -308,14 +323,14 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_yz_kernel(const Split3A
                 cell(c, ci, cj, ck);
                 const long long po = ds3_p_off(a, ci, cj, ck);
                 if (AX == 1) {
-                    P[po] = np0;
-                    P[po + CN * a.pfstride] = np1;
+                    P2[po] = np0;
+                    P2[po + a.pfstride] = np1;
                 } else if (ci >= 1 && ci <= mx && cj >= 1 && cj <= my) {
                     const long long qo = (long long)(ci - 1) * a.qs[0] + (long long)(cj - 1) * a.qs[1] +
                                          (long long)(ck - 1) * a.qs[2];
                     qn[qo] = np0;
                     qn[qo + a.fstride] = P[po + a.pfstride];
-                    qn[qo + 2 * a.fstride] = P[po + 2 * a.pfstride];
+                    qn[qo + 2 * a.fstride] = P2[po + a.pfstride];
                     qn[qo + 3 * a.fstride] = np1;
                 }
             }
