@@ -89,49 +89,55 @@ struct EulerRoe2D {
     __host__ __device__ static constexpr bool wave_zero(int, int) { return false; }
     __host__ __device__ static constexpr bool trans_zero(int, int) { return false; }
 
-    struct Roe { real u, v, enth, a, g1a2, euv, hu; };
+    struct Roe { real u, v, enth, a, g1a2, euv, hu, ha; };  // ha = 1/(2a)
 
     // Interface context: the Roe average of (qL, qR) that rpn and both rpt
     // calls of one interface share (computed once; the same values).
-    struct Ctx { real u, v, enth, a, g1a2; };
+    struct Ctx { real u, v, enth, a, g1a2, ha; };
     __device__ __forceinline__ Ctx context(int ixy, const real* qL, const real* qR) const {
         const int mu = ixy == 1 ? 1 : 2, mv = ixy == 1 ? 2 : 1;
         const Roe r = average(qL, qR, mu, mv);
-        return Ctx{r.u, r.v, r.enth, r.a, r.g1a2};
+        return Ctx{r.u, r.v, r.enth, r.a, r.g1a2, r.ha};
     }
     __device__ __forceinline__ static Roe expand(const Ctx& c) {
         Roe r;
-        r.u = c.u; r.v = c.v; r.enth = c.enth; r.a = c.a; r.g1a2 = c.g1a2;
+        r.u = c.u; r.v = c.v; r.enth = c.enth; r.a = c.a; r.g1a2 = c.g1a2; r.ha = c.ha;
         const real u2v2 = r.u * r.u + r.v * r.v;
         r.euv = r.enth - u2v2;
         r.hu = real(0.5) * u2v2;
         return r;
     }
 
+    // One reciprocal per square root and per sum (divisions are this solver's
+    // costly operations); 1/rho = (1/sqrt(rho))^2.
     __device__ __forceinline__ Roe average(const real* qL, const real* qR, int mu, int mv) const {
         const real rhsqrtl = sqrt(qL[0]);
         const real rhsqrtr = sqrt(qR[0]);
-        const real pl = gamma1 * (qL[3] - real(0.5) * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / qL[0]);
-        const real pr = gamma1 * (qR[3] - real(0.5) * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / qR[0]);
-        const real rhsq2 = rhsqrtl + rhsqrtr;
+        const real il = real(1) / rhsqrtl;
+        const real ir = real(1) / rhsqrtr;
+        const real pl = gamma1 * (qL[3] - real(0.5) * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) * (il * il));
+        const real pr = gamma1 * (qR[3] - real(0.5) * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) * (ir * ir));
+        const real i2 = real(1) / (rhsqrtl + rhsqrtr);
         Roe r;
-        r.u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
-        r.v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
-        r.enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+        r.u = (qL[mu] * il + qR[mu] * ir) * i2;
+        r.v = (qL[mv] * il + qR[mv] * ir) * i2;
+        r.enth = ((qL[3] + pl) * il + (qR[3] + pr) * ir) * i2;
         const real u2v2 = r.u * r.u + r.v * r.v;
         const real a2 = gamma1 * (r.enth - real(0.5) * u2v2);
         r.a = sqrt(a2);
         r.g1a2 = gamma1 / a2;
+        r.ha = real(0.5) / r.a;
         r.euv = r.enth - u2v2;
         r.hu = real(0.5) * u2v2;
         return r;
     }
 
-    // normal velocity and sound speed of a conserved state
+    // normal velocity and sound speed of a conserved state (one division)
     __device__ __forceinline__ void state(const real* q, int mu, int mv, real& un, real& c) const {
-        const real p = gamma1 * (q[3] - real(0.5) * (q[mu] * q[mu] + q[mv] * q[mv]) / q[0]);
-        c = sqrt(gamma * p / q[0]);
-        un = q[mu] / q[0];
+        const real ri = real(1) / q[0];
+        const real p = gamma1 * (q[3] - real(0.5) * (q[mu] * q[mu] + q[mv] * q[mv]) * ri);
+        c = sqrt(gamma * p * ri);
+        un = q[mu] * ri;
     }
 
     __device__ __forceinline__ void rpn(int ixy, const real* qL, const real* qR, const real*,
@@ -150,7 +156,7 @@ struct EulerRoe2D {
         for (int m = 0; m < 4; ++m) d[m] = qR[m] - qL[m];
         const real a3 = r.g1a2 * (r.euv * d[0] + r.u * d[mu] + r.v * d[mv] - d[3]);
         const real a2 = d[mv] - r.v * d[0];
-        const real a4 = (d[mu] + (r.a - r.u) * d[0] - r.a * a3) / (real(2) * r.a);
+        const real a4 = (d[mu] + (r.a - r.u) * d[0] - r.a * a3) * r.ha;
         const real a1 = d[0] - a3 - a4;
         w[0][0] = a1; w[0][mu] = a1 * (r.u - r.a); w[0][mv] = a1 * r.v; w[0][3] = a1 * (r.enth - r.u * r.a);
         s[0] = r.u - r.a;
@@ -215,7 +221,7 @@ struct EulerRoe2D {
         const Roe r = expand(c);
         const real a3 = r.g1a2 * (r.euv * asdq[0] + r.u * asdq[mu] + r.v * asdq[mv] - asdq[3]);
         const real a2 = asdq[mu] - r.u * asdq[0];
-        const real a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) / (real(2) * r.a);
+        const real a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) * r.ha;
         const real a1 = asdq[0] - a3 - a4;
         real w[3][4], sb[3];
         w[0][0] = a1; w[0][mu] = a1 * r.u; w[0][mv] = a1 * (r.v - r.a); w[0][3] = a1 * (r.enth - r.v * r.a);

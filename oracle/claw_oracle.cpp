@@ -227,35 +227,41 @@ void rpt2_vc_advection(int ixy, int imp, int, int meqn, int, int maux, int mbc, 
 // characteristic speed across the wave (Harten & Hyman, J. Comput. Phys. 50,
 // 1983).  This is the pointwise arithmetic, identical to the device functor.
 struct RoeAvg {
-    double u, v, enth, a, g1a2, euv, hu;
+    double u, v, enth, a, g1a2, euv, hu, ha;  // ha = 1/(2a)
 };
 
 inline RoeAvg roe_average(const double* qL, const double* qR, int mu, int mv) {
+    // one reciprocal per square root and per sum (divisions are the costly
+    // operations of this solver); 1/rho = (1/sqrt(rho))^2
     const double g1 = g_gamma - 1.0;
     const double rhsqrtl = std::sqrt(qL[0]);
     const double rhsqrtr = std::sqrt(qR[0]);
-    const double pl = g1 * (qL[3] - 0.5 * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / qL[0]);
-    const double pr = g1 * (qR[3] - 0.5 * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / qR[0]);
-    const double rhsq2 = rhsqrtl + rhsqrtr;
+    const double il = 1.0 / rhsqrtl;
+    const double ir = 1.0 / rhsqrtr;
+    const double pl = g1 * (qL[3] - 0.5 * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) * (il * il));
+    const double pr = g1 * (qR[3] - 0.5 * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) * (ir * ir));
+    const double i2 = 1.0 / (rhsqrtl + rhsqrtr);
     RoeAvg r;
-    r.u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
-    r.v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
-    r.enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+    r.u = (qL[mu] * il + qR[mu] * ir) * i2;
+    r.v = (qL[mv] * il + qR[mv] * ir) * i2;
+    r.enth = ((qL[3] + pl) * il + (qR[3] + pr) * ir) * i2;
     const double u2v2 = r.u * r.u + r.v * r.v;
     const double a2 = g1 * (r.enth - 0.5 * u2v2);
     r.a = std::sqrt(a2);
     r.g1a2 = g1 / a2;
+    r.ha = 0.5 / r.a;
     r.euv = r.enth - u2v2;
     r.hu = 0.5 * u2v2;
     return r;
 }
 
-// sound speed and normal velocity of a conserved state
+// sound speed and normal velocity of a conserved state (one division)
 inline void euler_state(const double* q, int mu, int mv, double* un, double* c) {
     const double g1 = g_gamma - 1.0;
-    const double p = g1 * (q[3] - 0.5 * (q[mu] * q[mu] + q[mv] * q[mv]) / q[0]);
-    *c = std::sqrt(g_gamma * p / q[0]);
-    *un = q[mu] / q[0];
+    const double ri = 1.0 / q[0];
+    const double p = g1 * (q[3] - 0.5 * (q[mu] * q[mu] + q[mv] * q[mv]) * ri);
+    *c = std::sqrt(g_gamma * p * ri);
+    *un = q[mu] * ri;
 }
 
 // pointwise normal solve: qL = q(i-1), qR = q(i); mu/mv 0-based
@@ -266,7 +272,7 @@ void euler_rpn(const double* qL, const double* qR, int mu, int mv, double w[3][4
     for (int m = 0; m < 4; ++m) d[m] = qR[m] - qL[m];
     const double a3 = r.g1a2 * (r.euv * d[0] + r.u * d[mu] + r.v * d[mv] - d[3]);
     const double a2 = d[mv] - r.v * d[0];
-    const double a4 = (d[mu] + (r.a - r.u) * d[0] - r.a * a3) / (2.0 * r.a);
+    const double a4 = (d[mu] + (r.a - r.u) * d[0] - r.a * a3) * r.ha;
     const double a1 = d[0] - a3 - a4;
     w[0][0] = a1;
     w[0][mu] = a1 * (r.u - r.a);
@@ -329,7 +335,7 @@ void euler_rpt(const double* qL, const double* qR, int mu, int mv, const double*
     const RoeAvg r = roe_average(qL, qR, mu, mv);
     const double a3 = r.g1a2 * (r.euv * asdq[0] + r.u * asdq[mu] + r.v * asdq[mv] - asdq[3]);
     const double a2 = asdq[mu] - r.u * asdq[0];
-    const double a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) / (2.0 * r.a);
+    const double a4 = (asdq[mv] + (r.a - r.v) * asdq[0] - r.a * a3) * r.ha;
     const double a1 = asdq[0] - a3 - a4;
     double w[3][4], sb[3];
     w[0][0] = a1; w[0][mu] = a1 * r.u; w[0][mv] = a1 * (r.v - r.a); w[0][3] = a1 * (r.enth - r.v * r.a);
