@@ -133,6 +133,26 @@ def dist_setup():
     return world, rank, local
 
 
+def reduce_over_ranks(x, op, world, device):
+    """max or sum of a float over the ranks (NCCL on the GPU run; any
+    initialised process group works, gloo with device 'cpu')."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def whole_job_rate(updates_local, ms_local, world, device):
+    """Replicas (weak scaling): the cell-updates of all ranks over the
+    slowest rank's device time.  Returns (rate, max ms, total updates)."""
+    ms_max = reduce_over_ranks(ms_local, "max", world, device)
+    total = reduce_over_ranks(updates_local, "sum", world, device)
+    return total / (ms_max * 1e-3), ms_max, total
+
+
 def cpu_reference_sample(n, nsteps):
     """Time the CPU restatement (oracle, speed build) on nsteps whole n^2
     steps of the workload; returns (cell-updates/s, seconds, cores)."""
@@ -275,18 +295,10 @@ def main():
             torch.distributed.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks(x, "max", world, "cuda")
 
     def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t)
-        return float(t.item())
+        return reduce_over_ranks(x, "sum", world, "cuda")
 
     from classic_b200 import problems
     from classic_b200.solver import Solver
@@ -337,9 +349,7 @@ def main():
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     barrier()
-    ms_max = max_over_ranks(ms)
-    total_updates = sum_over_ranks(float(cells) * steps)
-    value = total_updates / (ms_max * 1e-3)
+    value, ms_max, total_updates = whole_job_rate(float(cells) * steps, ms, world, "cuda")
 
     # ---- e2e: same frames with host q in / out per frame (pinned)
     e2e = None
