@@ -242,15 +242,17 @@ class PairGenerator:
         self.lib = _lib.load()
 
     def run(self, seed, norm: Norm, keep_steps, x_out, t_out, slot0, cfl_desired=0.9,
-            net=None, alpha=1.0, gamma_tol=1e-10):
-        """Advance one instance to tfinal; for the coarse steps whose index is
-        in keep_steps write features / targets into x_out[slot] / t_out[slot].
-        Without `net` every coarse step starts from the block-averaged fine
-        state (teacher forcing).  With `net` the coarse grid runs its own
-        corrected trajectory (alpha times the network after each step), so
-        the pairs cover the states the corrector meets at inference, with
-        targets from the fine run at the same times.  Returns (steps, slots
-        used)."""
+            net=None, alpha=1.0, gamma_tol=1e-10, interval=1):
+        """Advance one instance to tfinal in windows of `interval` coarse
+        steps; for the windows whose index is in keep_steps write features
+        (the window's start state and increment) / targets (the block-averaged
+        fine state minus the coarse state at the window's end) into
+        x_out[slot] / t_out[slot].  Without `net` every window starts from the
+        block-averaged fine state (teacher forcing).  With `net` the coarse
+        grid runs its own corrected trajectory (alpha times the network at
+        the end of each window), so the pairs cover the states the corrector
+        meets at inference, with targets from the fine run at the same times.
+        Returns (windows, slots used)."""
         torch = _torch()
         n, r = self.n, self.r
         rdf, solver, params, qf0, _ = problems.euler_quadrants(n=n * r, seed=seed, gamma=self.gamma)
@@ -262,6 +264,7 @@ class PairGenerator:
         st = _stream()
         t, dt, dtf = 0.0, 1e-3, 1e-3 / r
         qold = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
+        qwin = torch.empty((4, n, n), dtype=torch.float64, device="cuda")  # window start
         qfa = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
         step, slot = 0, slot0
         keep = set(keep_steps)
@@ -279,10 +282,13 @@ class PairGenerator:
             dt = min(dt, self.tfinal - t)
             qf, ldf, fsf = q_view(fine)
             qc, ldc, fsc = q_view(coarse)
-            if net is None:
+            first = step % interval == 0
+            if net is None and first:
                 check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qc), ldc, fsc, n, n, r, 4, st),
                       "nn_block_average")
             qold.copy_(qc)
+            if first:
+                qwin.copy_(qc)
             cfl = coarse.step(dt)
             if cfl > 1.0:  # rejected: retry from the same state with a smaller dt
                 qn, _, _ = q_view(coarse)
@@ -295,17 +301,19 @@ class PairGenerator:
                 raise RuntimeError(f"fine run info {info}")
             dtf = sf["dt_next"]
             qsc = qs.contiguous()
-            if step in keep:
+            last = step % interval == interval - 1
+            win = step // interval
+            if last and win in keep:
                 qf, _, _ = q_view(fine)
                 check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qfa), n, n * n, n, n, r, 4, st),
                       "nn_block_average")
-                check(self.lib.nn_features(_p(qold), _p(qsc), n, n * n, n, n, slot, _p(nd), _p(x_out),
+                check(self.lib.nn_features(_p(qwin), _p(qsc), n, n * n, n, n, slot, _p(nd), _p(x_out),
                                            st), "nn_features")
                 check(self.lib.nn_residual_target(_p(qfa), _p(qsc), n, n * n, n, n, slot, _p(nd),
                                                   _p(t_out), st), "nn_residual_target")
                 slot += 1
-            if net is not None:
-                check(self.lib.nn_features(_p(qold), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(xin), st),
+            if net is not None and last:
+                check(self.lib.nn_features(_p(qwin), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(xin), st),
                       "nn_features")
                 out = net.forward(xin)
                 check(self.lib.nn_apply_correction(_p(qs), ldc, fsc, n, n, _p(out), 16, _p(nda),
@@ -316,7 +324,7 @@ class PairGenerator:
             step += 1
         fine.close()
         coarse.close()
-        return step, slot - slot0
+        return step // interval, slot - slot0
 
 
 def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=0, log=None,
@@ -364,10 +372,11 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
 
 
 def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25, tol=1e-10,
-                  cfl_desired=0.9, cfl_max=1.0, alpha=1.0):
+                  cfl_desired=0.9, cfl_max=1.0, alpha=1.0, interval=1):
     """The corrected coarse run of one instance (claw2's dt control on the
-    host, alpha times the corrector after every accepted step).  Returns
-    (q, steps, corrected tile fraction, device seconds)."""
+    host, alpha times the corrector after every `interval` accepted steps,
+    fed the window's start state and increment).  Returns (q, steps,
+    corrected tile fraction, device seconds)."""
     if alpha != 1.0:
         v = norm.values.copy()
         v[12:16] = v[12:16] / max(alpha, 1e-30)
@@ -381,6 +390,7 @@ def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25,
     st = _stream()
     x = torch.empty((1, n, n, 16), dtype=torch.bfloat16, device="cuda")
     qold = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
+    qwin = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
     flags = torch.empty(((n + 15) // 16) ** 2, dtype=torch.int32, device="cuda")
     good = torch.zeros((), dtype=torch.int64, device="cuda")
     t, dt, steps, tiles = 0.0, float(rd.clawdata.dt_initial), 0, 0
@@ -391,20 +401,24 @@ def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25,
         dt = min(dt, tfinal - t)
         qc, ld, fs = q_view(s)
         qold.copy_(qc)
+        if steps % interval == 0:
+            qwin.copy_(qc)
         cfl = s.step(dt)
         if cfl > cfl_max:
             qn, _, _ = q_view(s)
             qn.copy_(qold)
             dt = dt * cfl_desired / cfl
             continue
-        qs, ld, fs = q_view(s)
-        qsc = qs.contiguous() if ld != n else qs
-        check(lib.nn_features(_p(qold), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(x), st), "nn_features")
-        out = net.forward(x)
-        check(lib.nn_apply_correction(_p(qs), ld, fs, n, n, _p(out), 16, _p(nd), gamma, tol,
-                                      _p(flags), st), "nn_apply_correction")
-        good += flags.sum()
-        tiles += flags.numel()
+        if steps % interval == interval - 1:
+            qs, ld, fs = q_view(s)
+            qsc = qs.contiguous() if ld != n else qs
+            check(lib.nn_features(_p(qwin), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(x), st),
+                  "nn_features")
+            out = net.forward(x)
+            check(lib.nn_apply_correction(_p(qs), ld, fs, n, n, _p(out), 16, _p(nd), gamma, tol,
+                                          _p(flags), st), "nn_apply_correction")
+            good += flags.sum()
+            tiles += flags.numel()
         t += dt
         dt = dt * cfl_desired / cfl if cfl > 0 else dt
         steps += 1

@@ -30,7 +30,7 @@ def _log(*a):
     print(*a, flush=True)
 
 
-def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0):
+def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0, interval=1):
     torch = C._torch()
     total = len(seeds) * keep
     x = torch.empty((total, n, n, 16), dtype=torch.bfloat16, device="cuda")
@@ -40,9 +40,10 @@ def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0):
     steps_all = []
     for seed in seeds:
         # the steps kept: spread over the run (90..250 coarse steps to t_final at 256^2)
-        est = int(0.6 * n)
-        kept = sorted(rng.choice(np.arange(2, est), size=keep, replace=False).tolist())
-        steps, k = gen.run(seed, norm, kept, x, t, used, net=net, alpha=alpha)
+        est = int(0.6 * n) // interval  # windows of `interval` coarse steps
+        kept = sorted(rng.choice(np.arange(1 if interval > 1 else 2, est),
+                                 size=min(keep, est - 2), replace=False).tolist())
+        steps, k = gen.run(seed, norm, kept, x, t, used, net=net, alpha=alpha, interval=interval)
         if k and not (torch.isfinite(x[used:used + k].float()).all() and
                       torch.isfinite(t[used:used + k]).all()):
             k = 0  # a run that left the physical states: drop its pairs
@@ -69,7 +70,7 @@ def recalibrate(x, t, norm):
     return C.Norm(v)
 
 
-def choose_alpha(net, norm, seeds, n, alphas=(0.0, 0.25, 0.5, 0.75, 1.0)):
+def choose_alpha(net, norm, seeds, n, alphas=(0.0, 0.25, 0.5, 0.75, 1.0), interval=1):
     """The corrector's gain alpha with the smallest mean L1 error against the
     block-averaged fine run on validation seeds (alpha = 0 is the plain
     step, so the chosen corrector is never worse than plain there)."""
@@ -81,7 +82,7 @@ def choose_alpha(net, norm, seeds, n, alphas=(0.0, 0.25, 0.5, 0.75, 1.0)):
             if a == 0.0:
                 q = C.plain_run(s, n)[0]
             else:
-                q = C.corrected_run(net, norm, s, n=n, alpha=a)[0]
+                q = C.corrected_run(net, norm, s, n=n, alpha=a, interval=interval)[0]
             e = C.l1_error(q, refs[s])
             errs.append(e if np.isfinite(e) else np.inf)
         table.append((a, float(np.mean(errs))))
@@ -90,11 +91,11 @@ def choose_alpha(net, norm, seeds, n, alphas=(0.0, 0.25, 0.5, 0.75, 1.0)):
     return best, table
 
 
-def evaluate(net, norm, seeds, n, truth_count, alpha=1.0):
+def evaluate(net, norm, seeds, n, truth_count, alpha=1.0, interval=1):
     out = []
     for k, seed in enumerate(seeds):
         qc, sc, tc = C.plain_run(seed, n)
-        qk, sk, frac, tk = C.corrected_run(net, norm, seed, n=n, alpha=alpha)
+        qk, sk, frac, tk = C.corrected_run(net, norm, seed, n=n, alpha=alpha, interval=interval)
         qf, sf, tf = C.plain_run(seed, 4 * n)
         ref = C.block_average(qf, 4)
         row = dict(seed=seed, alpha=alpha, coarse_steps=sc, fine_steps=sf, corrected_steps=sk,
@@ -130,6 +131,8 @@ def main(argv=None):
     ap.add_argument("--round-seeds", type=int, default=128)
     ap.add_argument("--round-iters", type=int, default=6000)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--interval", type=int, default=1,
+                    help="coarse steps between corrections (windows of the pairs)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     torch = C._torch()
@@ -137,11 +140,12 @@ def main(argv=None):
     train_seeds = list(range(10000, 10000 + args.train))
     held_seeds = list(range(20000, 20000 + args.heldout))
     t0 = time.perf_counter()
-    x, t, steps = generate(train_seeds, C.default_norm(), args.n, args.keep, rng)
+    K = args.interval
+    x, t, steps = generate(train_seeds, C.default_norm(), args.n, args.keep, rng, interval=K)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t0
     _log(f"pairs: {x.shape[0]} from {len(train_seeds)} seeds in {t_gen:.1f} s "
-         f"(coarse steps per run {min(steps)}..{max(steps)})")
+         f"(windows of {K} coarse steps per run {min(steps)}..{max(steps)})")
     norm = recalibrate(x, t, C.default_norm())
     if args.clip > 0:
         t.clamp_(-args.clip, args.clip)  # shock residuals are heavy-tailed
@@ -158,7 +162,8 @@ def main(argv=None):
     # all pairs (DAgger)
     for rnd in range(args.rounds):
         seeds_r = list(range(50000 + 1000 * rnd, 50000 + 1000 * rnd + args.round_seeds))
-        xr, tr_, _ = generate(seeds_r, norm, args.n, args.keep, rng, net=net, alpha=0.5)
+        xr, tr_, _ = generate(seeds_r, norm, args.n, args.keep, rng, net=net, alpha=0.5,
+                              interval=K)
         if args.clip > 0:
             tr_.clamp_(-args.clip, args.clip)
         C.project_tiles(tr_)
@@ -174,7 +179,8 @@ def main(argv=None):
         t_train += time.perf_counter() - t1
     del x, t
     # one-step skill on pairs of unseen seeds (same scaling and projection)
-    xv, tv, _ = generate(list(range(40000, 40004)), C.Norm(C.default_norm().values), args.n, 4, rng)
+    xv, tv, _ = generate(list(range(40000, 40004)), C.Norm(C.default_norm().values), args.n, 4, rng,
+                         interval=K)
     if xv.shape[0]:
         sc = C.default_norm().values
         for c in range(8):
@@ -190,11 +196,12 @@ def main(argv=None):
         gain = float("nan")
     del xv, tv
     val_seeds = list(range(30000, 30000 + args.validation))
-    alpha, table = choose_alpha(net, norm, val_seeds, args.n) if val_seeds else (1.0, [])
-    rows = evaluate(net, norm, held_seeds, args.n, args.truth, alpha=alpha)
+    alpha, table = (choose_alpha(net, norm, val_seeds, args.n, interval=K) if val_seeds
+                    else (1.0, []))
+    rows = evaluate(net, norm, held_seeds, args.n, args.truth, alpha=alpha, interval=K)
     good = [r for r in rows if r["finite"]]
     summary = dict(
-        alpha=alpha, alpha_table=table, one_step_relative_error=gain,
+        alpha=alpha, alpha_table=table, one_step_relative_error=gain, interval=K,
         pairs_seconds=t_gen, train_seconds=t_train, iters=args.iters, batch=args.batch,
         train_seeds=len(train_seeds), heldout_seeds=len(held_seeds), loss_first=losses[0][1],
         loss_last=losses[-1][1],
