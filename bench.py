@@ -204,9 +204,10 @@ def other_configs(peaks):
     """The other workloads of the suite, measured once each after the
     headline (device time from CUDA events inside the library): 1D acoustics
     (800 cells, 10 frames to t=1), 3D heterogeneous acoustics (256^3, the
-    first frame t=0..0.1, FP64 reference order and FP32) and the batched 2D
-    Euler ensemble (256 instances, sides log-uniform in 128..1024, to
-    t=0.25)."""
+    first frame t=0..0.1, FP64 reference order and FP32), the dimensionally
+    split steps (2D radial 4096^2 to t=0.03, Godunov and Strang; 3D 256^3
+    Godunov, first frame) and the batched 2D Euler ensemble (256 instances,
+    sides log-uniform in 128..1024, to t=0.25)."""
     from classic_b200 import problems
     from classic_b200.solver import BatchSolver, Solver
     out = {}
@@ -241,6 +242,30 @@ def other_configs(peaks):
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
                         "hbm_frac_algorithmic": rate * 10 * es / 1e9 / peaks["hbm_gbs"]}
+        except Exception as e:
+            out[key] = {"error": str(e)}
+    # dimensionally split steps (dimsp2 / dimsp3), FP64 reference order
+    for key, dim, split in (("radial_2d_4096_godunov_split_fp64", 2, "godunov"),
+                            ("radial_2d_4096_strang_split_fp64", 2, "strang"),
+                            ("hetero_acoustics_3d_256_split_fp64", 3, "godunov")):
+        try:
+            if dim == 2:
+                rd, solver, params, q0, aux = problems.radial_acoustics_2d(n=4096)
+                t1, dt0, cells, nbytes = 0.03, 0.01, 4096 ** 2, 48
+            else:
+                rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=256)
+                t1, dt0, cells, nbytes = 0.1, 0.01, 256 ** 3, 80
+            rd.clawdata.dimensional_split = split
+            s = Solver(rd.clawdata, solver, params, precision="fp64")
+            s.set_q(q0)
+            if aux is not None:
+                s.set_aux(aux)
+            info, st = s.advance(0.0, t1, dt0)
+            s.close()
+            rate = cells * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
+            out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
+                        "device_ms": st["device_ms"],
+                        "hbm_frac_algorithmic": rate * nbytes / 1e9 / peaks["hbm_gbs"]}
         except Exception as e:
             out[key] = {"error": str(e)}
     try:
