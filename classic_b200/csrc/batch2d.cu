@@ -190,6 +190,27 @@ struct claw_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     long long launches = 0;
     int device = 0;
+
+    // Frees everything the batch holds, so an error part-way through
+    // claw_batch_create leaks nothing.
+    ~claw_batch() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        runner.reset();
+        for (auto& gg : g) {
+            for (int s = 0; s < 2; ++s)
+                if (gg.q[s]) cudaFree(gg.q[s]);
+            if (gg.aux) cudaFree(gg.aux);
+        }
+        if (ctl_d) cudaFree(ctl_d);
+        if (ctl_h) cudaFreeHost(ctl_h);
+        if (flags_d) cudaFree(flags_d);
+        if (flags_h) cudaFreeHost(flags_h);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 extern "C" {
@@ -270,24 +291,7 @@ int claw_batch_create(const claw_config* cfgs, int count, claw_batch** out) {
 }
 
 int claw_batch_destroy(claw_batch* b) {
-    if (!b) return 0;
-    cudaSetDevice(b->device);
-    if (b->stream) cudaStreamSynchronize(b->stream);
-    if (b->gexec) cudaGraphExecDestroy(b->gexec);
-    b->runner.reset();
-    for (auto& g : b->g) {
-        for (int s = 0; s < 2; ++s)
-            if (g.q[s]) cudaFree(g.q[s]);
-        if (g.aux) cudaFree(g.aux);
-    }
-    if (b->ctl_d) cudaFree(b->ctl_d);
-    if (b->ctl_h) cudaFreeHost(b->ctl_h);
-    if (b->flags_d) cudaFree(b->flags_d);
-    if (b->flags_h) cudaFreeHost(b->flags_h);
-    if (b->ev0) cudaEventDestroy(b->ev0);
-    if (b->ev1) cudaEventDestroy(b->ev1);
-    if (b->stream) cudaStreamDestroy(b->stream);
-    delete b;
+    delete b;  // ~claw_batch frees the device state
     return 0;
 }
 

@@ -415,6 +415,26 @@ struct claw_handle {
     int device = 0;
     double t_now = 0.0;  // time of the current q (time-dependent boundary conditions)
     double* totals_scratch = nullptr;  // block partials + result of claw_totals
+
+    // Frees everything the handle holds, so an error part-way through
+    // claw_create (the handle lives in a unique_ptr there) leaks nothing.
+    ~claw_handle() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        runner.reset();
+        for (int k = 0; k < 2; ++k)
+            if (g.q[k]) cudaFree(g.q[k]);
+        if (g.aux) cudaFree(g.aux);
+        if (g.aux_base) cudaFree(g.aux_base);
+        if (totals_scratch) cudaFree(totals_scratch);
+        if (g.ctl) cudaFree(g.ctl);
+        if (stage) cudaFree(stage);
+        if (ctl_h) cudaFreeHost(ctl_h);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 extern "C" {
@@ -545,22 +565,7 @@ int claw_create(const claw_config* cfg, claw_handle** out) {
 }
 
 int claw_destroy(claw_handle* h) {
-    if (!h) return 0;
-    cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
-    if (h->gexec) cudaGraphExecDestroy(h->gexec);
-    for (int k = 0; k < 2; ++k)
-        if (h->g.q[k]) cudaFree(h->g.q[k]);
-    if (h->g.aux) cudaFree(h->g.aux);
-    if (h->g.aux_base) cudaFree(h->g.aux_base);
-    if (h->totals_scratch) cudaFree(h->totals_scratch);
-    if (h->g.ctl) cudaFree(h->g.ctl);
-    if (h->stage) cudaFree(h->stage);
-    if (h->ctl_h) cudaFreeHost(h->ctl_h);
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->stream) cudaStreamDestroy(h->stream);
-    delete h;
+    delete h;  // ~claw_handle frees the device state
     return 0;
 }
 
