@@ -123,6 +123,7 @@ SIGNATURES = {
     # learned corrector kernels (include/claw_nn.h)
     "nn_conv3x3_forward": (ctypes.c_int, [_P, _P, _P, _P, _P] + [ctypes.c_int] * 7 + [_P]),
     "nn_conv3x3_wgrad": (ctypes.c_int, [_P] * 6 + [ctypes.c_int] * 5 + [_P]),
+    "nn_device_error": (ctypes.c_int, [ctypes.c_int]),
     "nn_flip_weights": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
     "nn_gelu_backward": (ctypes.c_int, [_P, _P, _P, ctypes.c_longlong, _P]),
     "nn_mse_grad": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,

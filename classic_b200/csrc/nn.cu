@@ -2,13 +2,15 @@
 // device pointers, declared in include/claw_nn.h).
 //
 // The corrector is a stack of 3x3 "same" convolutions over NHWC BF16
-// activations with FP32 accumulation on the tensor cores (mma.sync m16n8k16
-// BF16 -> FP32), GELU between layers.  Training runs on the device with the
-// kernels below: the forward convolution (optionally saving the FP32
-// pre-activation), the data gradient (the same convolution with flipped and
-// transposed weights), the weight/bias gradient (a pixel-reduction GEMM per
-// tile plus a reduction over tiles), GELU's derivative, the MSE loss
-// gradient and Adam.  Glue kernels move between the solver's FP64 SoA q and
+// activations with FP32 accumulation on the tensor cores, GELU between
+// layers.  The forward convolution (and the data gradient, the same
+// convolution with flipped and transposed weights) runs on the 5th-generation
+// tensor cores: tcgen05.mma of shared-memory operands into a TMEM
+// accumulator, read back with tcgen05.ld for the epilogue.  Training runs on
+// the device with the kernels below: the forward convolution (optionally
+// saving the FP32 pre-activation), the data gradient, the weight/bias
+// gradient (a pixel-reduction GEMM per tile with mma.sync, plus a reduction
+// over tiles), GELU's derivative, the MSE loss gradient and Adam.  Glue kernels move between the solver's FP64 SoA q and
 // the network: block averages of a fine grid, input features, residual
 // targets, and the corrector's application with a per-tile conservative
 // projection and a positivity fallback to the plain step.
@@ -17,6 +19,11 @@
 #include <stdint.h>
 
 #include "../../include/claw_nn.h"
+#include "common.cuh"
+
+// Device-side error flags of the network kernels (bit 0: a tensor-core
+// accumulator wait gave up); read and cleared by nn_device_error().
+__device__ int g_nn_err;
 
 namespace {
 
@@ -65,93 +72,191 @@ __device__ __forceinline__ void load_halo(__nv_bfloat16* xs, const __nv_bfloat16
     }
 }
 
-// ------------------------------------------------------------ forward conv ---
-// out[p, co] = act(b[co] + sum_{tap, ci} W[co][tap][ci] x[p + off(tap), ci]).
-// Warp w computes output rows 2w and 2w+1 of the tile (two m16 tiles of 16
-// pixels) for all COUT channels (COUT/8 n8 tiles); K runs over 9 taps x CIN.
-template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
-__global__ void __launch_bounds__(NTHREADS) conv3x3_fwd(const __nv_bfloat16* __restrict__ x,
-                                                         const __nv_bfloat16* __restrict__ wt,
-                                                         const float* __restrict__ bias, void* out,
-                                                         float* __restrict__ zsave, int h, int w) {
-    constexpr int XP = CIN + 8, WP = 9 * CIN + 8, NT = COUT / 8;
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem);
-    __nv_bfloat16* ws = xs + HALO * HALO * XP;
-    float* bs = reinterpret_cast<float*>(ws + COUT * WP);
-    const int n = blockIdx.z, y0 = blockIdx.y * TILE, x0 = blockIdx.x * TILE;
-    load_halo<CIN>(xs, x, n, h, w, y0, x0);
-    constexpr int WCH = 9 * CIN / 8;
-    for (int e = threadIdx.x; e < COUT * WCH; e += NTHREADS) {
-        const int co = e / WCH, ck = e % WCH;
-        *reinterpret_cast<uint4*>(ws + co * WP + ck * 8) =
-            *reinterpret_cast<const uint4*>(wt + (long long)co * 9 * CIN + ck * 8);
-    }
-    for (int e = threadIdx.x; e < COUT; e += NTHREADS) bs[e] = bias[e];
-    __syncthreads();
+// ------------------------------------------------- forward conv, tcgen05 ---
+// The same convolution as an implicit GEMM on the 5th-generation tensor
+// cores.  A CTA (4 warps) owns an output tile of 16 rows x 8 columns: M = 128
+// pixels, N = COUT, K = 9 taps x CIN.  The halo tile (18 x 10 pixels) and the
+// weights sit in shared memory in the UMMA no-swizzle K-major layout (core
+// matrices of 8 rows x 16 bytes: 8 pixels or 8 output channels, 8 input
+// channels), so each tap's operand A is the halo tile itself with the start
+// address moved by the tap's offset: 8-row groups (tile rows) are HW*16
+// bytes apart, 8-channel chunks one halo plane apart.  One thread issues the
+// 9 x CIN/16 tcgen05.mma (M128 N=COUT K16, BF16 -> FP32) into a TMEM
+// accumulator of COUT columns and commits them to an mbarrier; each warp
+// then reads its 32 pixels (TMEM lanes) with tcgen05.ld and applies bias,
+// GELU and the stores.
+namespace tc {
+constexpr int TW = 8, TH = 16, HW = TW + 2, HH = TH + 2, NPX = HW * HH;
+constexpr int NTH = 128;
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, t = lane & 3;
-    float acc[2][NT][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) acc[mt][nt][k] = 0.f;
-
-#pragma unroll 1
-    for (int tap = 0; tap < 9; ++tap) {
-        const int ky = tap / 3, kx = tap % 3;
-#pragma unroll
-        for (int kc = 0; kc < CIN / 16; ++kc) {
-            uint32_t b[NT][2];
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const __nv_bfloat16* wp = ws + (nt * 8 + g) * WP + tap * CIN + kc * 16 + 2 * t;
-                b[nt][0] = ld32(wp);
-                b[nt][1] = ld32(wp + 8);
-            }
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                const int row = 2 * warp + mt + ky;
-                const __nv_bfloat16* p0 = xs + (row * HALO + g + kx) * XP + kc * 16 + 2 * t;
-                const __nv_bfloat16* p1 = p0 + 8 * XP;
-                const uint32_t a[4] = {ld32(p0), ld32(p1), ld32(p0 + 8), ld32(p1 + 8)};
-#pragma unroll
-                for (int nt = 0; nt < NT; ++nt) mma_bf16(acc[mt][nt], a, b[nt]);
-            }
-        }
-    }
-    // epilogue: bias, activation, store (two channels per value pair)
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-        const int py = y0 + 2 * warp + mt;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int px = x0 + g + 8 * half;
-            const long long pix = ((long long)n * h + py) * w + px;
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const int co = nt * 8 + 2 * t;
-                const float z0 = acc[mt][nt][2 * half] + bs[co];
-                const float z1 = acc[mt][nt][2 * half + 1] + bs[co + 1];
-                if (SAVEZ) *reinterpret_cast<float2*>(zsave + pix * COUT + co) = make_float2(z0, z1);
-                const float y0v = ACT ? gelu(z0) : z0, y1v = ACT ? gelu(z1) : z1;
-                if (OUTF32)
-                    *reinterpret_cast<float2*>(static_cast<float*>(out) + pix * COUT + co) = make_float2(y0v, y1v);
-                else
-                    *reinterpret_cast<uint32_t*>(static_cast<__nv_bfloat16*>(out) + pix * COUT + co) =
-                        pack2(__float2bfloat16_rn(y0v), __float2bfloat16_rn(y1v));
-            }
-        }
-    }
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n) {
+    // c_format F32 (bits 4-5), a/b format BF16 (bits 7-9, 10-12), both K-major,
+    // N >> 3 (bits 17-22), M >> 4 (bits 24-28)
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
+// shared-memory matrix descriptor: no swizzle, lbo = bytes between core
+// matrices adjacent in K, sbo = bytes between 8-row groups; version 1
+__device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                    uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(clawb200::smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void alloc(uint32_t* slot, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(clawb200::smem_u32(slot)), "r"(cols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void dealloc(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+// 32 lanes x 16 columns of 32-bit values (this warp's lane quarter)
+__device__ __forceinline__ void ld16(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 template <int CIN, int COUT>
-constexpr int fwd_smem() {
-    return HALO * HALO * (CIN + 8) * 2 + COUT * (9 * CIN + 8) * 2 + COUT * 4;
+__host__ __device__ constexpr int a_bytes() { return (CIN / 8) * NPX * 16; }
+template <int CIN, int COUT>
+__host__ __device__ constexpr int smem_bytes() {
+    return ((a_bytes<CIN, COUT>() + 127) / 128) * 128 + 9 * (CIN / 8) * COUT * 16 + COUT * 4;
 }
+}  // namespace tc
+
+template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
+__global__ void __launch_bounds__(tc::NTH) conv3x3_fwd_tc(const __nv_bfloat16* __restrict__ x,
+                                                           const __nv_bfloat16* __restrict__ wt,
+                                                           const float* __restrict__ bias, void* out,
+                                                           float* __restrict__ zsave, int h, int w) {
+    using namespace tc;
+    static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "UMMA M128: N in {16, 32}, K in steps of 16");
+    constexpr int KC = CIN / 8;                 // 16-byte chunks per pixel
+    constexpr int APLANE = NPX * 16;            // bytes of one chunk plane of the halo tile
+    constexpr int AOFF = ((a_bytes<CIN, COUT>() + 127) / 128) * 128;
+    constexpr int BPLANE = COUT * 16;           // bytes of one (tap, chunk) plane of the weights
+    extern __shared__ __align__(16) unsigned char smem[];  // 16-byte alignment is all UMMA needs without swizzle
+    unsigned char* As = smem;                   // [KC][NPX][8 channels]
+    unsigned char* Bs = smem + AOFF;            // [9][KC][COUT][8 channels]
+    float* bs = reinterpret_cast<float*>(Bs + 9 * KC * BPLANE);
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tslot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nimg = blockIdx.z, y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
+
+    for (int e = tid; e < NPX * KC; e += NTH) {
+        const int pix = e / KC, kc = e % KC;
+        const int gy = y0 + pix / HW - 1, gx = x0 + pix % HW - 1;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (gy >= 0 && gy < h && gx >= 0 && gx < w)
+            v = *reinterpret_cast<const uint4*>(x + (((long long)nimg * h + gy) * w + gx) * CIN + kc * 8);
+        *reinterpret_cast<uint4*>(As + kc * APLANE + pix * 16) = v;
+    }
+    for (int e = tid; e < COUT * 9 * KC; e += NTH) {  // wt[co][tap][ci] -> [tap][kc][co]
+        const int co = e / (9 * KC), r = e % (9 * KC), tap = r / KC, kc = r % KC;
+        *reinterpret_cast<uint4*>(Bs + (tap * KC + kc) * BPLANE + co * 16) =
+            *reinterpret_cast<const uint4*>(wt + ((long long)co * 9 + tap) * CIN + kc * 8);
+    }
+    for (int e = tid; e < COUT; e += NTH) bs[e] = bias[e];
+    if (warp == 0) alloc(&tslot, 32);
+    if (tid == 0) {
+        clawb200::mbar_init(&bar, 1);
+        clawb200::fence_barrier_init();
+    }
+    clawb200::fence_proxy_async_smem();  // the tensor core reads what the threads wrote
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tslot;
+
+    if (tid == 0) {
+        constexpr uint32_t idesc = idesc_bf16_f32(128, COUT);
+        const uint32_t a0 = clawb200::smem_u32(As), b0 = clawb200::smem_u32(Bs);
+        uint32_t acc = 0;
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) {
+            const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+            for (int kk = 0; kk < CIN / 16; ++kk) {
+                const uint64_t da = desc(a0 + (ky * HW + kx) * 16 + 2 * kk * APLANE, APLANE, HW * 16);
+                const uint64_t db = desc(b0 + (tap * KC + 2 * kk) * BPLANE, BPLANE, 128);
+                mma(tmem, da, db, idesc, acc);
+                acc = 1;
+            }
+        }
+        commit(&bar);
+    }
+    bool ok = clawb200::mbar_wait_bounded(&bar, 0);
+    if (!ok) {  // never expected: record it, give the MMAs a second bound, skip the stores
+        if (lane == 0) atomicOr(&g_nn_err, 1);
+        ok = false;
+        (void)clawb200::mbar_wait_bounded(&bar, 0);
+    }
+    fence_after();
+
+    // epilogue: warp w holds TMEM lanes 32w..32w+31 = pixels 32w..32w+31
+    const int m = warp * 32 + lane;
+    const int py = y0 + m / TW, px = x0 + m % TW;
+    const long long pix = ((long long)nimg * h + py) * w + px;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 16) {
+        uint32_t r[16];
+        ld16(trow + c0, r);
+        wait_ld();
+        if (!ok) continue;
+        float z[16], yv[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            z[j] = __uint_as_float(r[j]) + bs[c0 + j];
+            yv[j] = ACT ? gelu(z[j]) : z[j];
+        }
+        if (SAVEZ) {
+#pragma unroll
+            for (int j = 0; j < 16; j += 4)
+                *reinterpret_cast<float4*>(zsave + pix * COUT + c0 + j) = make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
+        }
+        if (OUTF32) {
+#pragma unroll
+            for (int j = 0; j < 16; j += 4)
+                *reinterpret_cast<float4*>(static_cast<float*>(out) + pix * COUT + c0 + j) =
+                    make_float4(yv[j], yv[j + 1], yv[j + 2], yv[j + 3]);
+        } else {
+            uint32_t pk[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                pk[j] = pack2(__float2bfloat16_rn(yv[2 * j]), __float2bfloat16_rn(yv[2 * j + 1]));
+            uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * COUT + c0);
+            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        dealloc(tmem, 32);
+    }
+}
+
 
 // ------------------------------------------------------- weight gradient ---
 // partial[blk][co][tap*CIN + ci] = sum over the tile's pixels p of
@@ -450,11 +555,11 @@ int grid_for(long long n) {
 template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
 int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, int n, int h,
                int wd, cudaStream_t s) {
-    constexpr int SM = fwd_smem<CIN, COUT>();
-    auto k = conv3x3_fwd<CIN, COUT, ACT, OUTF32, SAVEZ>;
+    constexpr int SM = tc::smem_bytes<CIN, COUT>();
+    auto k = conv3x3_fwd_tc<CIN, COUT, ACT, OUTF32, SAVEZ>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess)
         return NN_E_CUDA;
-    k<<<dim3(wd / TILE, h / TILE, n), NTHREADS, SM, s>>>(
+    k<<<dim3(wd / tc::TW, h / tc::TH, n), tc::NTH, SM, s>>>(
         static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), b, y, z, h, wd);
     return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
 }
@@ -514,6 +619,16 @@ int nn_conv3x3_wgrad(const void* x, const void* dz, float* partial, float* pdb, 
     reduce_tiles<<<(len + 255) / 256, 256, 0, s>>>(partial, dw, nblk, len);
     reduce_tiles<<<1, 256, 0, s>>>(pdb, db, nblk, cout);
     return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+}
+
+int nn_device_error(int clear) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_nn_err, sizeof(int)) != cudaSuccess) return NN_E_CUDA;
+    if (clear) {
+        const int zero = 0;
+        if (cudaMemcpyToSymbol(g_nn_err, &zero, sizeof(int)) != cudaSuccess) return NN_E_CUDA;
+    }
+    return v;
 }
 
 int nn_flip_weights(const void* w, void* wt, int cout, int cin, void* stream) {

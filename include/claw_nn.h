@@ -24,13 +24,18 @@ enum nn_error { NN_E_INVALID = -1, NN_E_CUDA = -2, NN_E_UNSUPPORTED = -3 };
 /* y = act(conv3x3(x, w) + b); act 0 = identity, 1 = GELU.  z (optional) keeps
  * the FP32 pre-activation for the backward pass.  (cin, cout, act, out_f32):
  * (16,32,1,0) (32,32,1,0) (32,16,0,1), and the data-gradient shapes
- * (32,32,0,0) (16,32,0,0). */
+ * (32,32,0,0) (16,32,0,0).  Runs as tcgen05.mma (M128 x N=cout x K16 BF16
+ * products, FP32 accumulator in tensor memory) on 16 x 8 pixel tiles. */
 int nn_conv3x3_forward(const void* x, const void* w, const float* b, void* y, float* z, int n,
                        int h, int wd, int cin, int cout, int act, int out_f32, void* stream);
 /* dw[cout][9][cin] = sum_p dz[p][co] x[p + off][ci], db[co] = sum_p dz[p][co];
  * partial / pdb: scratch of n*(h/16)*(wd/16) blocks x (cout*9*cin) / cout floats. */
 int nn_conv3x3_wgrad(const void* x, const void* dz, float* partial, float* pdb, float* dw,
                      float* db, int n, int h, int wd, int cin, int cout, void* stream);
+/* Device-side error flags of these kernels (bit 0: a wait on the tensor-core
+ * accumulator gave up, and that launch left its output unwritten); clear != 0
+ * resets them.  Synchronises with the device. */
+int nn_device_error(int clear);
 /* wt[ci][tap][co] = w[co][8-tap][ci]: the data gradient dx = conv3x3(dz, wt). */
 int nn_flip_weights(const void* w, void* wt, int cout, int cin, void* stream);
 /* dz = dy * GELU'(z), n elements. */
