@@ -4,6 +4,10 @@
     python -m classic_b200.profile_step --n 3072 --steps 4 --precision fp64_fma
     python -m classic_b200.profile_step --dim 3 --n 128 --steps 2
     python -m classic_b200.profile_step --n 2048 --split godunov --precision fp64
+    python -m classic_b200.profile_step --nn --n 256 --steps 3
+
+With --nn each step is one forward pass of the corrector network (five
+tcgen05 convolutions) on a batch of 8 random n x n inputs.
 
 Each step is one claw_step (bc + step2 / step3, or the dimensionally split
 step with --split) of fixed dt = 0.9 dx / c_max.
@@ -21,7 +25,19 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", default="fp64_fma", choices=["fp64", "fp64_fma", "fp32"])
     ap.add_argument("--split", default="unsplit", choices=["unsplit", "godunov", "strang"])
+    ap.add_argument("--nn", action="store_true", help="the corrector network's forward pass")
     args = ap.parse_args()
+    if args.nn:
+        import torch
+
+        from .corrector import ConvNet
+        net = ConvNet(seed=0)
+        x = torch.randn((8, args.n, args.n, 16), device="cuda").to(torch.bfloat16)
+        for _ in range(args.steps):
+            y = net.forward(x)
+        torch.cuda.synchronize()
+        print(f"{args.steps} forward passes of 8 x {args.n}^2, sum = {float(y.float().sum()):.6e}")
+        return
     if args.dim == 2:
         rd, solver, params, q0, aux = problems.radial_acoustics_2d(n=args.n)
         cmax = 2.0
