@@ -21,6 +21,8 @@ SOLVER_IDS = {
     "euler_roe_2d": 3,
     "acoustics_1d": 11,
     "vc_acoustics_1d": 12,
+    "advection_1d": 13,
+    "euler_roe_1d": 14,
     "vc_acoustics_3d": 21,
 }
 

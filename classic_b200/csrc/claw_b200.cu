@@ -149,8 +149,12 @@ template <class S>
 struct Runner1D : Runner {
     Step1Args<S> args;
     int smem = 0;
+    typename S::real* iface = nullptr;
 
     explicit Runner1D(const S& s) { std::memset(&args, 0, sizeof(args)); args.solver = s; }
+    ~Runner1D() override {
+        if (iface) cudaFree(iface);
+    }
 
     int prepare(const claw_config& cfg, const Geometry& g) override {
         args.q[0] = static_cast<typename S::real*>(g.q[0]);
@@ -171,12 +175,19 @@ struct Runner1D : Runner {
         args.src_nd1 = (double)(cfg.source_ndim - 1);
         args.src_bulk = cfg.solver_params[1];
         args.xlower = cfg.lower[0];
-        smem = step1_smem_bytes<S>(g.mx);
         int dev = 0, optin = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        if (smem + 1024 > optin)
-            return fail(CLAW_E_UNSUPPORTED, "1D grid of %d cells exceeds the single-CTA kernel", g.mx);
+        long long bytes = step1_smem_bytes<S>(g.mx, true);
+        if (bytes + 1024 > optin) {
+            // the interface arrays move to an L2-resident global buffer
+            bytes = step1_smem_bytes<S>(g.mx, false);
+            if (bytes + 1024 > optin)
+                return fail(CLAW_E_UNSUPPORTED, "1D grid of %d cells exceeds the single-CTA kernel", g.mx);
+            CUDA_TRY(cudaMalloc(&iface, (size_t)step1_iface_doubles<S>(g.mx) * sizeof(typename S::real)));
+        }
+        args.iface = iface;
+        smem = (int)bytes;
         CUDA_TRY(cudaFuncSetAttribute(step1_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
         return 0;
@@ -241,6 +252,14 @@ std::unique_ptr<Runner> make_runner(const claw_config& cfg) {
         return std::unique_ptr<Runner>(new Runner2D<VCAdvection2D<real>, MethodGeneric2D>(VCAdvection2D<real>{}));
     if (id == CLAW_SOLVER_VC_ACOUSTICS_1D)
         return std::unique_ptr<Runner>(new Runner1D<VCAcoustics1D<real>>(VCAcoustics1D<real>{}));
+    if (id == CLAW_SOLVER_ADVECTION_1D)
+        return std::unique_ptr<Runner>(
+            new Runner1D<Advection1D<real>>(Advection1D<real>{(real)cfg.solver_params[0]}));
+    if (id == CLAW_SOLVER_EULER_ROE_1D) {
+        const double gamma = cfg.solver_params[0];
+        return std::unique_ptr<Runner>(
+            new Runner1D<EulerRoe1D<real>>(EulerRoe1D<real>{(real)gamma, (real)(gamma - 1.0)}));
+    }
     return nullptr;
 }
 
@@ -382,6 +401,8 @@ bool solver_shape(int id, SolverShape* sh) {
         case CLAW_SOLVER_EULER_ROE_2D: *sh = {2, 4, 3, 0}; return true;
         case CLAW_SOLVER_ACOUSTICS_1D: *sh = {1, 2, 2, 0}; return true;
         case CLAW_SOLVER_VC_ACOUSTICS_1D: *sh = {1, 2, 2, 2}; return true;
+        case CLAW_SOLVER_ADVECTION_1D: *sh = {1, 1, 1, 0}; return true;
+        case CLAW_SOLVER_EULER_ROE_1D: *sh = {1, 3, 3, 0}; return true;
         case CLAW_SOLVER_VC_ACOUSTICS_3D: *sh = {3, 4, 2, 2}; return true;
         default: return false;
     }

@@ -298,6 +298,120 @@ struct Acoustics1D {
     }
 };
 
+// 1D advection q_t + u q_x = 0 with constant u (examples/advection_1d_example1,
+// the rp1_advection plugin of clawpack/riemann, restated): one wave, the jump,
+// with speed u; A-dq = min(u, 0) dq, A+dq = max(u, 0) dq.
+template <typename real_>
+struct Advection1D {
+    using real = real_;
+    static constexpr int meqn = 1, mwaves = 1, maux = 0;
+    real u;
+
+    __device__ __forceinline__ void rp1(const real* qL, const real* qR, const real*, const real*,
+                                        real wave[mwaves][meqn], real s[mwaves], real amdq[meqn],
+                                        real apdq[meqn]) const {
+        const real d = qR[0] - qL[0];
+        wave[0][0] = d;
+        s[0] = u;
+        amdq[0] = fmin(u, real(0)) * d;
+        apdq[0] = fmax(u, real(0)) * d;
+    }
+};
+
+// 1D Euler, q = (rho, rho u, E), gamma-law gas (examples/euler_1d_wcblast, the
+// rp1_euler_with_efix plugin of clawpack/riemann): Roe averages, three waves
+// (u-a, u, u+a), A-dq with the Harten-Hyman entropy fix in the 1- and 3-waves
+// and A+dq = sum s w - A-dq; one reciprocal per square root and per sum, as
+// in the 2D solver above.
+template <typename real_>
+struct EulerRoe1D {
+    using real = real_;
+    static constexpr int meqn = 3, mwaves = 3, maux = 0;
+    real gamma, gamma1;
+
+    // velocity and sound speed of a conserved state (one division)
+    __device__ __forceinline__ void state(const real* q, real& u, real& c) const {
+        const real ri = real(1) / q[0];
+        const real p = gamma1 * (q[2] - real(0.5) * (q[1] * q[1]) * ri);
+        c = sqrt(gamma * p * ri);
+        u = q[1] * ri;
+    }
+
+    __device__ __forceinline__ void rp1(const real* qL, const real* qR, const real*, const real*,
+                                        real w[mwaves][meqn], real s[mwaves], real amdq[meqn],
+                                        real apdq[meqn]) const {
+        const real rhsqrtl = sqrt(qL[0]);
+        const real rhsqrtr = sqrt(qR[0]);
+        const real il = real(1) / rhsqrtl;
+        const real ir = real(1) / rhsqrtr;
+        const real pl = gamma1 * (qL[2] - real(0.5) * (qL[1] * qL[1]) * (il * il));
+        const real pr = gamma1 * (qR[2] - real(0.5) * (qR[1] * qR[1]) * (ir * ir));
+        const real i2 = real(1) / (rhsqrtl + rhsqrtr);
+        const real u = (qL[1] * il + qR[1] * ir) * i2;
+        const real enth = ((qL[2] + pl) * il + (qR[2] + pr) * ir) * i2;
+        const real u2 = u * u;
+        const real a2 = gamma1 * (enth - real(0.5) * u2);
+        const real a = sqrt(a2);
+        const real g1a2 = gamma1 / a2;
+        const real ha = real(0.5) / a;
+        real d[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) d[m] = qR[m] - qL[m];
+        const real b2 = g1a2 * ((enth - u2) * d[0] + u * d[1] - d[2]);
+        const real b3 = (d[1] + (a - u) * d[0] - a * b2) * ha;
+        const real b1 = d[0] - b2 - b3;
+        w[0][0] = b1; w[0][1] = b1 * (u - a); w[0][2] = b1 * (enth - u * a);
+        s[0] = u - a;
+        w[1][0] = b2; w[1][1] = b2 * u;       w[1][2] = b2 * (real(0.5) * u2);
+        s[1] = u;
+        w[2][0] = b3; w[2][1] = b3 * (u + a); w[2][2] = b3 * (enth + u * a);
+        s[2] = u + a;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) amdq[m] = real(0);
+        real ul, cl;
+        state(qL, ul, cl);
+        const real s0 = ul - cl;
+        real q1[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) q1[m] = qL[m] + w[0][m];
+        real u1, c1;
+        state(q1, u1, c1);
+        const real s1 = u1 - c1;
+        if (!(s0 >= real(0) && s[0] > real(0))) {
+            real sfract;
+            if (s0 < real(0) && s1 > real(0)) sfract = s0 * (s1 - s[0]) / (s1 - s0);
+            else if (s[0] < real(0)) sfract = s[0];
+            else sfract = real(0);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) amdq[m] = sfract * w[0][m];
+            if (s[1] < real(0)) {
+#pragma unroll
+                for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+                real ur, cr;
+                state(qR, ur, cr);
+                const real s3 = ur + cr;
+                real q2[3];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) q2[m] = qR[m] - w[2][m];
+                real u2s, c2;
+                state(q2, u2s, c2);
+                const real s2 = u2s + c2;
+                real sf3;
+                if (s2 < real(0) && s3 > real(0)) sf3 = s2 * (s3 - s[2]) / (s3 - s2);
+                else if (s[2] < real(0)) sf3 = s[2];
+                else sf3 = real(0);
+#pragma unroll
+                for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + sf3 * w[2][m];
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const real df = (s[0] * w[0][m] + s[1] * w[1][m]) + s[2] * w[2][m];
+            apdq[m] = df - amdq[m];
+        }
+    }
+};
+
 // 1D variable-coefficient acoustics, aux = (Z, c) per cell: the left-going
 // wave lies on the eigenvector of the left cell, the right-going on the
 // right cell's: jump = a1*(-Z_l, 1) + a2*(Z_r, 1), speeds -c_l, +c_r.

@@ -30,6 +30,11 @@ struct Step1Args {
     // Strang; the radial term of examples/acoustics_2d_radial/1drad/src1.f
     int src_split;
     double src_nd1, src_bulk, xlower;  // ndim - 1, bulk, xlower
+    // per-interface waves, speeds and fluctuations: in shared memory when
+    // null, else this global buffer of step1_iface_doubles(mx) reals (grids
+    // whose interface arrays do not fit the CTA's shared memory; the buffer
+    // stays in L2, and __syncthreads orders the CTA's global accesses too)
+    typename S::real* iface;
     ClawCtl* ctl;
     S solver;
 };
@@ -47,17 +52,23 @@ __device__ __forceinline__ void step1_source(const Step1Args<S>& A, typename S::
     }
 }
 
+// per-interface wave/s/amdq/apdq (f reuses amdq)
 template <class S>
-__host__ __device__ constexpr int step1_smem_doubles(int mx) {
-    // q, aux, dtdx, per-interface wave/s/amdq/apdq (f reuses amdq), reduction;
-    // the copy kept for a rejected step lives in the output buffer
-    return (S::meqn + S::maux + 1) * (mx + 4) +
-           (S::mwaves * S::meqn + S::mwaves + 2 * S::meqn) * (mx + 4) + 32;
+__host__ __device__ constexpr long long step1_iface_doubles(int mx) {
+    return (long long)(S::mwaves * S::meqn + S::mwaves + 2 * S::meqn) * (mx + 4);
 }
 
 template <class S>
-int step1_smem_bytes(int mx) {
-    return step1_smem_doubles<S>(mx) * (int)sizeof(typename S::real) + 64 * 8;
+__host__ __device__ constexpr long long step1_smem_doubles(int mx, bool iface_in_smem) {
+    // q, aux, dtdx (+ the interface arrays), reduction; the copy kept for a
+    // rejected step lives in the output buffer
+    return (long long)(S::meqn + S::maux + 1) * (mx + 4) + (iface_in_smem ? step1_iface_doubles<S>(mx) : 0) +
+           32;
+}
+
+template <class S>
+long long step1_smem_bytes(int mx, bool iface_in_smem) {
+    return step1_smem_doubles<S>(mx, iface_in_smem) * (long long)sizeof(typename S::real) + 64 * 8;
 }
 
 template <class S>
@@ -72,7 +83,7 @@ __global__ void __launch_bounds__(STEP1_THREADS, 1) step1_kernel(const __grid_co
     real* qs = reinterpret_cast<real*>(smem_raw);
     real* as = qs + ME * n;
     real* dtdx = as + MA * n;
-    real* wv = dtdx + n;            // [MW][ME][ne]
+    real* wv = A.iface ? A.iface : dtdx + n;  // [MW][ME][ne]
     real* sv = wv + MW * ME * ne;   // [MW][ne]
     real* amd = sv + MW * ne;       // [ME][ne]
     real* apd = amd + ME * ne;

@@ -57,6 +57,55 @@ def acoustics_1d_config(mx=800, nout=10, tfinal=1.0):
     return rd, solver, params, q0, None
 
 
+def advection_1d_example1(mx=200, nout=20, tfinal=4.0):
+    """examples/advection_1d_example1 (setrun.py, qinit.f90, setprob.f90):
+    q_t + u q_x = 0 with u = 1 on [0, 1], periodic, 200 cells, MC, cfl 0.9,
+    q0 = exp(-beta (x - 0.75)^2) (beta = 400) plus 1 on 0.1 < x < 0.4; 20
+    outputs to t = 4 (four periods)."""
+    rd = ClawRunData("classic", 1)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("u", 1.0)
+    pd.add_param("beta", 400.0)
+    cd = rd.clawdata
+    cd.lower[0], cd.upper[0], cd.num_cells[0] = 0.0, 1.0, mx
+    cd.num_eqn, cd.num_aux, cd.capa_index = 1, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 0.1, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 500
+    cd.order, cd.num_waves, cd.limiter = 2, 1, ["mc"]
+    cd.bc_lower[0], cd.bc_upper[0] = "periodic", "periodic"
+    x, _ = _centres(0.0, 1.0, mx)
+    q0 = np.zeros((1, mx))
+    q0[0] = np.exp(-400.0 * (x - 0.75) ** 2) + np.where((x > 0.1) & (x < 0.4), 1.0, 0.0)
+    return rd, "advection_1d", {"u": 1.0}, q0, None
+
+
+def euler_1d_wcblast(mx=2000, nout=20, tfinal=0.038, gamma=1.4):
+    """examples/euler_1d_wcblast (setrun.py, qinit.f90, setprob.f90): the
+    Woodward-Colella blast waves on 2000 cells, rho = 1, u = 0,
+    p = 1000 / 0.01 / 100 on x < 0.1 / 0.1..0.9 / x > 0.9, solid walls, MC on
+    3 waves, cfl 0.9, dt_initial 1e-6, 20 outputs to t = 0.038."""
+    rd = ClawRunData("classic", 1)
+    pd = rd.new_UserData("probdata", "setprob.data")
+    pd.add_param("gamma", gamma)
+    cd = rd.clawdata
+    cd.lower[0], cd.upper[0], cd.num_cells[0] = 0.0, 1.0, mx
+    cd.num_eqn, cd.num_aux, cd.capa_index = 3, 0, 0
+    cd.t0, cd.output_style, cd.num_output_times, cd.tfinal = 0.0, 1, nout, tfinal
+    cd.output_t0 = True
+    cd.dt_variable, cd.dt_initial, cd.dt_max = True, 1e-6, 1e99
+    cd.cfl_desired, cd.cfl_max, cd.steps_max = 0.9, 1.0, 5000
+    cd.order, cd.num_waves, cd.limiter = 2, 3, ["mc"] * 3
+    cd.bc_lower[0], cd.bc_upper[0] = "wall", "wall"
+    x, _ = _centres(0.0, 1.0, mx)
+    g1 = gamma - 1.0
+    q0 = np.zeros((3, mx))
+    q0[0] = 1.0
+    q0[2] = np.where(x < 0.1, 1e3 / g1, np.where(x < 0.9, 1e-2 / g1, 1e2 / g1))
+    return rd, "euler_roe_1d", {"gamma": gamma}, q0, None
+
+
 def radial_pulse(r, width=0.2):
     """qinit of examples/acoustics_2d_radial (qinit.f:17-28) and of its 1drad
     companion (1drad/qinit.f): p = 1 + cos(pi (r-0.5)/width) for

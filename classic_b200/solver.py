@@ -26,6 +26,8 @@ SOLVER_PARAMS = {
     "euler_roe_2d": ("gamma",),
     "vc_advection_2d": (),
     "vc_acoustics_1d": (),
+    "advection_1d": ("u",),
+    "euler_roe_1d": ("gamma",),
     "vc_acoustics_3d": (),
 }
 

@@ -41,6 +41,8 @@ enum claw_solver_id {
     CLAW_SOLVER_EULER_ROE_2D = 3,    /* q=(rho,rhou,rhov,E); params: gamma      */
     CLAW_SOLVER_ACOUSTICS_1D = 11,   /* q=(p,u); params: rho, bulk              */
     CLAW_SOLVER_VC_ACOUSTICS_1D = 12,/* q=(p,u); aux=(Z,c)                      */
+    CLAW_SOLVER_ADVECTION_1D = 13,   /* q=(q); params: u                        */
+    CLAW_SOLVER_EULER_ROE_1D = 14,   /* q=(rho,rhou,E); params: gamma           */
     CLAW_SOLVER_VC_ACOUSTICS_3D = 21 /* q=(p,u,v,w); aux=(Z,c)                  */
 };
 

@@ -53,6 +53,8 @@ enum {
     ORC_EULER_ROE_2D = 3,      // q = (rho, rho u, rho v, E);  params: gamma
     ORC_ACOUSTICS_1D = 11,     // q = (p, u);  params: rho, bulk
     ORC_VC_ACOUSTICS_1D = 12,  // q = (p, u);  aux = (Z, c)
+    ORC_ADVECTION_1D = 13,     // q = (q);  params: u
+    ORC_EULER_ROE_1D = 14,     // q = (rho, rho u, E);  params: gamma
     ORC_VC_ACOUSTICS_3D = 21,  // q = (p, u, v, w);  aux = (Z, c)
 };
 
@@ -61,6 +63,7 @@ enum {
 static int g_solver = 0;
 static double g_rho = 1.0, g_bulk = 1.0, g_cc = 1.0, g_zz = 1.0, g_hz = 0.5;
 static double g_gamma = 1.4;
+static double g_u = 1.0;  // 1D advection velocity
 
 // Source term (the example's src1 / src2; 0 = the reference's default no-op).
 // 1: examples/acoustics_2d_radial/1drad/src1.f:18-23, radial symmetry with x
@@ -108,9 +111,12 @@ int orc_set_solver(int solver_id, const double* params, int nparams) {
         g_cc = std::sqrt(g_bulk / g_rho);
         g_zz = g_rho * g_cc;
         g_hz = 0.5 / g_zz;
-    } else if (solver_id == ORC_EULER_ROE_2D) {
+    } else if (solver_id == ORC_EULER_ROE_2D || solver_id == ORC_EULER_ROE_1D) {
         if (nparams < 1) return -1;
         g_gamma = params[0];
+    } else if (solver_id == ORC_ADVECTION_1D) {
+        if (nparams < 1) return -1;
+        g_u = params[0];
     }
     return 0;
 }
@@ -404,6 +410,112 @@ void rp1_acoustics(int, int meqn, int mwaves, int, int mbc, int mx, const double
         amdq[q.at(2, i)] = -(cc * a1);
         apdq[q.at(1, i)] = cc * (a2 * zz);
         apdq[q.at(2, i)] = cc * a2;
+    }
+}
+
+// rp1_advection (clawpack/riemann, restated): wave = jump, s = u,
+// A-dq = min(u, 0) wave, A+dq = max(u, 0) wave
+void rp1_advection(int, int meqn, int mwaves, int, int mbc, int mx, const double* ql,
+                   const double* qr, const double*, const double*, double* wave, double* s,
+                   double* amdq, double* apdq) {
+    const Slice q{meqn, 1 - mbc}, w{meqn * mwaves, 1 - mbc}, sv{mwaves, 1 - mbc};
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const double d = ql[q.at(1, i)] - qr[q.at(1, i - 1)];
+        wave[w.at(1, i)] = d;
+        s[sv.at(1, i)] = g_u;
+        amdq[q.at(1, i)] = std::fmin(g_u, 0.0) * d;
+        apdq[q.at(1, i)] = std::fmax(g_u, 0.0) * d;
+    }
+}
+
+// 1D Euler Roe solver with the Harten-Hyman entropy fix (rp1_euler_with_efix
+// of clawpack/riemann, restated from the mathematics; the same operations as
+// the 2D solver above with the transverse velocity absent)
+inline void euler1d_state(const double* q, double* u, double* c) {
+    const double g1 = g_gamma - 1.0;
+    const double ri = 1.0 / q[0];
+    const double p = g1 * (q[2] - 0.5 * (q[1] * q[1]) * ri);
+    *c = std::sqrt(g_gamma * p * ri);
+    *u = q[1] * ri;
+}
+
+void euler1d_rp(const double* qL, const double* qR, double w[3][3], double s[3], double* amdq,
+                double* apdq) {
+    const double g1 = g_gamma - 1.0;
+    const double rhsqrtl = std::sqrt(qL[0]);
+    const double rhsqrtr = std::sqrt(qR[0]);
+    const double il = 1.0 / rhsqrtl;
+    const double ir = 1.0 / rhsqrtr;
+    const double pl = g1 * (qL[2] - 0.5 * (qL[1] * qL[1]) * (il * il));
+    const double pr = g1 * (qR[2] - 0.5 * (qR[1] * qR[1]) * (ir * ir));
+    const double i2 = 1.0 / (rhsqrtl + rhsqrtr);
+    const double u = (qL[1] * il + qR[1] * ir) * i2;
+    const double enth = ((qL[2] + pl) * il + (qR[2] + pr) * ir) * i2;
+    const double u2 = u * u;
+    const double a2 = g1 * (enth - 0.5 * u2);
+    const double a = std::sqrt(a2);
+    const double g1a2 = g1 / a2;
+    const double ha = 0.5 / a;
+    double d[3];
+    for (int m = 0; m < 3; ++m) d[m] = qR[m] - qL[m];
+    const double b2 = g1a2 * ((enth - u2) * d[0] + u * d[1] - d[2]);
+    const double b3 = (d[1] + (a - u) * d[0] - a * b2) * ha;
+    const double b1 = d[0] - b2 - b3;
+    w[0][0] = b1; w[0][1] = b1 * (u - a); w[0][2] = b1 * (enth - u * a);
+    s[0] = u - a;
+    w[1][0] = b2; w[1][1] = b2 * u;       w[1][2] = b2 * (0.5 * u2);
+    s[1] = u;
+    w[2][0] = b3; w[2][1] = b3 * (u + a); w[2][2] = b3 * (enth + u * a);
+    s[2] = u + a;
+    for (int m = 0; m < 3; ++m) amdq[m] = 0.0;
+    double ul, cl;
+    euler1d_state(qL, &ul, &cl);
+    const double s0 = ul - cl;
+    double q1[3];
+    for (int m = 0; m < 3; ++m) q1[m] = qL[m] + w[0][m];
+    double u1, c1;
+    euler1d_state(q1, &u1, &c1);
+    const double s1 = u1 - c1;
+    if (!(s0 >= 0.0 && s[0] > 0.0)) {
+        double sfract;
+        if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) / (s1 - s0);
+        else if (s[0] < 0.0) sfract = s[0];
+        else sfract = 0.0;
+        for (int m = 0; m < 3; ++m) amdq[m] = sfract * w[0][m];
+        if (s[1] < 0.0) {
+            for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+            double ur, cr;
+            euler1d_state(qR, &ur, &cr);
+            const double s3 = ur + cr;
+            double q2[3];
+            for (int m = 0; m < 3; ++m) q2[m] = qR[m] - w[2][m];
+            double u2s, c2;
+            euler1d_state(q2, &u2s, &c2);
+            const double s2 = u2s + c2;
+            double sf3;
+            if (s2 < 0.0 && s3 > 0.0) sf3 = s2 * (s3 - s[2]) / (s3 - s2);
+            else if (s[2] < 0.0) sf3 = s[2];
+            else sf3 = 0.0;
+            for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + sf3 * w[2][m];
+        }
+    }
+    for (int m = 0; m < 3; ++m) {
+        const double df = (s[0] * w[0][m] + s[1] * w[1][m]) + s[2] * w[2][m];
+        apdq[m] = df - amdq[m];
+    }
+}
+
+void rp1_euler_roe(int, int meqn, int mwaves, int, int mbc, int mx, const double* ql,
+                   const double* qr, const double*, const double*, double* wave, double* s,
+                   double* amdq, double* apdq) {
+    const Slice q{meqn, 1 - mbc}, w{meqn * mwaves, 1 - mbc}, sv{mwaves, 1 - mbc};
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double wl[3][3], sl[3];
+        euler1d_rp(&qr[q.at(1, i - 1)], &ql[q.at(1, i)], wl, sl, &amdq[q.at(1, i)], &apdq[q.at(1, i)]);
+        for (int k = 0; k < 3; ++k) {
+            for (int m = 0; m < 3; ++m) wave[w.at(1, i) + k * meqn + m] = wl[k][m];
+            s[sv.at(k + 1, i)] = sl[k];
+        }
     }
 }
 
@@ -1604,6 +1716,8 @@ int orc_step1(int meqn, int mwaves, int mbc, int maux, int mx, double* q, const 
     rp1_t rp1;
     if (g_solver == ORC_ACOUSTICS_1D) rp1 = rp1_acoustics;
     else if (g_solver == ORC_VC_ACOUSTICS_1D) rp1 = rp1_vc_acoustics;
+    else if (g_solver == ORC_ADVECTION_1D) rp1 = rp1_advection;
+    else if (g_solver == ORC_EULER_ROE_1D) rp1 = rp1_euler_roe;
     else return -1;
     const int n = mx + 2 * mbc;
     const Slice sl{meqn, 1 - mbc}, sv{mwaves, 1 - mbc}, w{meqn * mwaves, 1 - mbc};

@@ -26,12 +26,16 @@ SOLVER_IDS = {
     "euler_roe_2d": 3,
     "acoustics_1d": 11,
     "vc_acoustics_1d": 12,
+    "advection_1d": 13,
+    "euler_roe_1d": 14,
     "vc_acoustics_3d": 21,
 }
 SOLVER_PARAMS = {
     "acoustics_2d": ("rho", "bulk"),
     "acoustics_1d": ("rho", "bulk"),
     "euler_roe_2d": ("gamma",),
+    "advection_1d": ("u",),
+    "euler_roe_1d": ("gamma",),
 }
 
 # bc code of the restated user BC (examples/acoustics_3d_heterogeneous/bc3.f:282-312)
@@ -178,7 +182,8 @@ class OracleGrid:
         self.qf[self._interior()] = np.moveaxis(q, 0, -1)
 
     def get_q(self):
-        return np.ascontiguousarray(np.moveaxis(self.qf[self._interior()], -1, 0))
+        # a copy: with one field the moved view already counts as contiguous
+        return np.array(np.moveaxis(self.qf[self._interior()], -1, 0), order="C", copy=True)
 
     def set_aux(self, aux):
         if self.maux:

@@ -65,3 +65,32 @@ def test_reference_setrun_runs_unchanged(example, tmp_path):
     back = data.read_claw_data(str(tmp_path / "claw.data"))
     assert back.num_cells == list(rd.clawdata.num_cells)
     assert back.limiter == rd.clawdata.limiter_codes()
+
+
+def _cfg_fields(cfg):
+    out = {}
+    for name, _ in cfg._fields_:
+        v = getattr(cfg, name)
+        out[name] = list(v) if hasattr(v, "__len__") else v
+    return out
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.parametrize("example,solver,params", [
+    ("advection_1d_example1", "advection_1d", {"u": 1.0}),
+    ("euler_1d_wcblast", "euler_roe_1d", {"gamma": 1.4}),
+])
+def test_builtin_problem_matches_reference_setrun(example, solver, params):
+    """The problem builders restate the examples' setrun.py: the unchanged
+    setrun.py and the builder give the same claw_config."""
+    from classic_b200 import problems
+    data.install_clawutil_alias()
+    path = os.path.join(REF, example, "setrun.py")
+    spec = importlib.util.spec_from_file_location(f"setrun_{example}_cfg", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    ref = _cfg_fields(make_config(mod.setrun("classic").clawdata, solver, params))
+    rd, s, p, _, _ = getattr(problems, example)()
+    assert s == solver and p == params
+    ours = _cfg_fields(make_config(rd.clawdata, s, p))
+    assert ours == ref
