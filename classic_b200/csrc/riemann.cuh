@@ -480,6 +480,32 @@ struct VCAcoustics3D {
         const real c1 = cb * b1, c2 = ca * b2;
         return Split{c1 * zb, -c1, c2 * za, c2};
     }
+    // The same split given the face reciprocals rb = 1 / (Z_b + Z_m) and
+    // ra = 1 / (Z_m + Z_a): multiplications only (the contracted and FP32
+    // builds; the quotients round differently from the divisions above).
+    __device__ __forceinline__ static Split split_r(real xp, real rb, real zb, real cb, real ra,
+                                                    real za, real ca) {
+        const real b1 = -(xp * rb);
+        const real b2 = xp * ra;
+        const real c1 = cb * b1, c2 = ca * b2;
+        return Split{c1 * zb, -c1, c2 * za, c2};
+    }
+    // rpn with one reciprocal of the impedance sum instead of two divisions
+    __device__ __forceinline__ static void rpn_r(real pL, real uL, real pR, real uR, real zl,
+                                                 real cl, real zr, real cr, real w[2][2],
+                                                 real s[2], real am[2], real ap[2]) {
+        const real dp = pR - pL;
+        const real du = uR - uL;
+        const real r = real(1) / (zl + zr);
+        const real a1 = (zr * du - dp) * r;
+        const real a2 = (zl * du + dp) * r;
+        w[0][0] = -(a1 * zl); w[0][1] = a1;
+        w[1][0] = a2 * zr;    w[1][1] = a2;
+        s[0] = -cl;
+        s[1] = cr;
+        am[0] = cl * (a1 * zl); am[1] = -(cl * a1);
+        ap[0] = cr * (a2 * zr); ap[1] = cr * a2;
+    }
 };
 
 }  // namespace clawb200

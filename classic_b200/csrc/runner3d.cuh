@@ -1,7 +1,7 @@
 // Runner of the 3D step (one launch per sweep: x, y, z; the z-sweep's last
 // CTA runs claw3's dt controller, src/3d/claw3.f:738-904), shared by the
-// reference-order unit (claw3d.cu, --fmad=false) and the fused / FP32 unit
-// (fast3d.cu).
+// reference-order unit (claw3d.cu, --fmad=false, sweep3p_kernel) and the
+// fused / FP32 unit (fast3d.cu, sweep3f_kernel).
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -13,6 +13,7 @@
 #include "host.h"
 #include "riemann.cuh"
 #include "step3d.cuh"
+#include "step3d_fast.cuh"
 #include "step3ds.cuh"
 
 namespace clawb200 {
@@ -22,7 +23,7 @@ struct Runner3D : Runner {
     using real = typename S::real;
     Sweep3Args<real> args[3];
     int grid[3] = {1, 1, 1};
-    static constexpr int SMEM = sweep3_smem_bytes<real>();
+    static constexpr int SMEM = BUILD == 1 ? sweep3f_smem_bytes<real>() : sweep3_smem_bytes<real>();
 
     int prepare(const claw_config& cfg, const Geometry& g) override {
         Sweep3Args<real> b;
@@ -67,19 +68,23 @@ struct Runner3D : Runner {
             if (n > 0x7fffffffLL) return fail(CLAW_E_UNSUPPORTED, "3D grid too large");
             grid[dir] = (int)n;
         }
-        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 0, M, false, BUILD>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 1, M, false, BUILD>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-        CUDA_TRY(cudaFuncSetAttribute(sweep3p_kernel<S, 2, M, true, BUILD>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        CUDA_TRY(cudaFuncSetAttribute(kernel<0, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        CUDA_TRY(cudaFuncSetAttribute(kernel<1, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        CUDA_TRY(cudaFuncSetAttribute(kernel<2, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
         return 0;
     }
 
+    // the sweep kernel of direction DIR for this unit
+    template <int DIR, bool LAST>
+    static auto kernel() {
+        if constexpr (BUILD == 1) return &sweep3f_kernel<S, DIR, M, LAST>;
+        else return &sweep3p_kernel<S, DIR, M, LAST, BUILD>;
+    }
+
     cudaError_t launch(cudaStream_t s) override {
-        sweep3p_kernel<S, 0, M, false, BUILD><<<grid[0], NT3P, SMEM, s>>>(args[0]);
-        sweep3p_kernel<S, 1, M, false, BUILD><<<grid[1], NT3P, SMEM, s>>>(args[1]);
-        sweep3p_kernel<S, 2, M, true, BUILD><<<grid[2], NT3P, SMEM, s>>>(args[2]);
+        kernel<0, false>()<<<grid[0], NT3P, SMEM, s>>>(args[0]);
+        kernel<1, false>()<<<grid[1], NT3P, SMEM, s>>>(args[1]);
+        kernel<2, true>()<<<grid[2], NT3P, SMEM, s>>>(args[2]);
         return cudaGetLastError();
     }
     int launches_per_step() const override { return 3; }
