@@ -204,7 +204,7 @@ def other_configs(peaks):
     """The other workloads of the suite, measured once each after the
     headline (device time from CUDA events inside the library): 1D acoustics
     (800 cells, 10 frames to t=1), 3D heterogeneous acoustics (256^3, the
-    first frame t=0..0.1, FP64 reference order and FP32), the dimensionally
+    first frame t=0..0.1, FP64 reference order, FP64 contracted and FP32), the dimensionally
     split steps (2D radial 4096^2 to t=0.03, Godunov and Strang; 3D 256^3
     Godunov, first frame) and the batched 2D Euler ensemble (256 instances,
     sides log-uniform in 128..1024, to t=0.25)."""
@@ -226,7 +226,7 @@ def other_configs(peaks):
                                    "device_ms": ms, "note": "one CTA runs the whole claw1 loop per frame"}
     except Exception as e:  # a failed side measurement must not hide the headline
         out["acoustics_1d_800"] = {"error": str(e)}
-    for prec in ("fp64", "fp32"):
+    for prec in ("fp64", "fp64_fma", "fp32"):
         key = f"hetero_acoustics_3d_256_{prec}"
         try:
             rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=256)

@@ -191,3 +191,52 @@ def test_fp32_tracks_fp64():
     assert abs(sg["t_reached"] - so["t_reached"]) < 1e-12
     assert np.all(rel_diff(g.get_q(), o.get_q()) <= 5e-5)
     g.close()
+
+
+def _fast_pair(rd, solver, params, q0, aux, precision):
+    g = Solver(rd.clawdata, solver, params, precision=precision)
+    o = OracleGrid(rd.clawdata, solver, params)
+    for s in (g, o):
+        s.set_q(q0)
+        s.set_aux(aux)
+    return g, o
+
+
+@pytest.mark.parametrize("lim", [0, 1, 3, 4])
+@pytest.mark.parametrize("order,trans", [(1, 0), (1, 11), (2, 0), (2, 10), (2, 11),
+                                         (2, 20), (2, 21), (2, 22)])
+@pytest.mark.parametrize("precision,tol", [("fp64_fma", 1e-12), ("fp32", 5e-5)])
+def test_fast_kernel_methods(lim, order, trans, precision, tol):
+    """The contracted / FP32 sweep kernel over every transverse code (codes
+    without double-transverse splits take its extra pair barrier) and ragged
+    tiles: the same Courant numbers (to FP32 speeds), q within the build's
+    tolerance."""
+    rd, solver, params, q0, aux = problems.random_acoustics_3d(
+        37, 19, 23, seed=5, limiter=lim, order=order, trans=trans,
+        bc=("wall", "extrap", "periodic", "periodic", "wall", "extrap"))
+    g, o = _fast_pair(rd, solver, params, q0, aux, precision)
+    t = 0.0
+    for _ in range(3):
+        cg, co = g.step(0.01), o.step(0.01, t)
+        t += 0.01
+        if precision == "fp64_fma":
+            assert cg == co
+        assert abs(cg - co) <= 1e-6 * abs(co)
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= tol)
+    g.close()
+
+
+@pytest.mark.parametrize("shape", [(2, 3, 4), (70, 9, 8), (8, 70, 9), (9, 8, 70), (33, 18, 15)])
+def test_fast_kernel_ragged_sizes(shape):
+    mx, my, mz = shape
+    rd, solver, params, q0, aux = problems.random_acoustics_3d(mx, my, mz, seed=mx + my + mz,
+                                                               bc=("extrap",) * 6)
+    for precision, tol in (("fp64_fma", 1e-12), ("fp32", 5e-5)):
+        g, o = _fast_pair(rd, solver, params, q0, aux, precision)
+        t = 0.0
+        for dt in (0.004, 0.006):
+            g.step(dt)
+            o.step(dt, t)
+            t += dt
+        assert np.all(rel_diff(g.get_q(), o.get_q()) <= tol)
+        g.close()
