@@ -14,12 +14,10 @@
 //   * the aux ring holds the face reciprocals 1 / (Z + Z_next) along the
 //     tile's two axes, so the 16 transverse splits of a slice position
 //     multiply instead of dividing (rounding differs from the divisions);
-//   * in FP32, Z, c and the next position's q values are copied by cp.async
-//     issued at the top of a position and awaited just before its CTA
-//     barrier, so their latency overlaps the position's arithmetic, and the
-//     reciprocals of a ring position are formed from the landed Z one
-//     position later (in FP64 that measured 3 % slower than loading through
-//     registers just before the barrier, which FP64 keeps);
+//   * Z, c and the next position's q values are copied by cp.async issued at
+//     the top of a position and awaited just before its CTA barrier, so their
+//     latency overlaps the position's arithmetic, and the reciprocals of a
+//     ring position are formed from the landed Z one position later;
 //   * a cell adds its nine neighbour terms in a fixed order instead of
 //     step3's 2x2-block colour order.
 // The Courant number is the same FP64 product as the exact build's, so the
@@ -34,15 +32,10 @@ constexpr int NPL3F = 4;  // aux planes: Z, c, 1/(Z+Z_e1), 1/(Z+Z_e2)
 
 // Shared memory is sized to the carveout steps (100, 132, 164, 196, 228 KB):
 // what the carveout leaves is L1, which serves the x-sweep's strided loads.
-// Staged q planes of NT3 values, [position & 1][p, normal velocity], exist in
-// the FP32 build only.
-template <typename real>
-__host__ __device__ constexpr int qst3_planes() {
-    return sizeof(real) == 4 ? 4 : 0;
-}
-// buffers of neighbour terms: two (by position parity) in FP32; one in FP64,
-// with a second CTA barrier per position, which keeps the CTA under the
-// 132 KB carveout
+constexpr int QST3 = 4;  // staged q planes of NT3 values: [position & 1][p, normal velocity]
+// buffers of neighbour terms: two (by position parity) in FP32 (98 KB, the
+// 100 KB step); one in FP64, with a second CTA barrier per position (133 KB,
+// the 164 KB step, instead of 197 KB and the 228 KB step)
 template <typename real>
 __host__ __device__ constexpr int term3_bufs() {
     return sizeof(real) == 4 ? 2 : 1;
@@ -51,7 +44,7 @@ __host__ __device__ constexpr int term3_bufs() {
 template <typename real>
 __host__ __device__ constexpr int sweep3f_smem_bytes() {
     return (RING3 * NPL3F * NS3 + term3_bufs<real>() * NTERM3 * NT3 +
-            (XCH3 + qst3_planes<real>()) * NT3) *
+            (XCH3 + QST3) * NT3) *
                (int)sizeof(real) +
            16 * (int)sizeof(double);
 }
@@ -80,7 +73,6 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
     constexpr bool E1A = DIR != 1;
     constexpr int CN = 1 + AXN, CE1 = 1 + (E1A ? AXA : AXB), CE2 = 1 + (E1A ? AXB : AXA);
     constexpr int NPL = NPL3F;
-    constexpr bool ASYNC = sizeof(real) == 4;  // cp.async refills (FP32)
     constexpr int NTB = term3_bufs<real>();
     // shared-memory steps of this role's own split direction and the other
     constexpr int E1S = E1A ? 1 : S3A, E2S = E1A ? S3A : 1;
@@ -90,7 +82,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
     real* saux = reinterpret_cast<real*>(smem_raw);  // [RING3][NPL][NS3]
     real* sterm = saux + RING3 * NPL * NS3;          // [NTB][NTERM3][NT3]
     real* sxch = sterm + NTB * NTERM3 * NT3;         // [XCH3][NT3]
-    real* sq = sxch + XCH3 * NT3;                    // [qst3_planes][NT3]
+    real* sq = sxch + XCH3 * NT3;                    // [QST3][NT3]
 
     ClawCtl* ctl = a.ctl;
     const int cur = ctl->cur;
@@ -153,8 +145,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
             }
         }
     };
-    // Z and c of ring position pos: copied asynchronously (FP32), or loaded
-    // with the reciprocals formed at once (FP64)
+    // Z and c of ring position pos, copied asynchronously
     auto load_aux = [&](int pos) {
         real* dst = saux + (pos & (RING3 - 1)) * NPL * NS3;
         const long long pofs = (long long)(pos + 1) * a.as[AXN];
@@ -162,25 +153,13 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
             const int sa = e % S3A, sb = e / S3A;
             const int Ai = min(A0 - 2 + sa, mA + 2), Bi = min(B0 - 2 + sb, mB + 2);
             const long long o = pofs + (long long)(Ai + 1) * a.as[AXA] + (long long)(Bi + 1) * a.as[AXB];
-            if constexpr (ASYNC) {
-                cp_async_el(dst + e, aux + o);
-                cp_async_el(dst + NS3 + e, aux + o + a.afstride);
-            } else {
-                const real z = aux[o];
-                dst[e] = z;
-                dst[NS3 + e] = aux[o + a.afstride];
-                // faces to the next cell along A and B (clamped as the tile is)
-                const real zA = aux[o + (Ai < mA + 2 ? a.as[AXA] : 0)];
-                const real zB = aux[o + (Bi < mB + 2 ? a.as[AXB] : 0)];
-                dst[(E1A ? 2 : 3) * NS3 + e] = real(1) / (z + zA);
-                dst[(E1A ? 3 : 2) * NS3 + e] = real(1) / (z + zB);
-            }
+            cp_async_el(dst + e, aux + o);
+            cp_async_el(dst + NS3 + e, aux + o + a.afstride);
         }
     };
-    // 1 / (Z + Z_next) along A and B of ring position pos, from its landed Z
-    // (FP32).  The next tile element is the next cell, or the same clamped
-    // cell past the grid's last ghost, as in the FP64 load; the tile's last
-    // row and column are never read.
+    // 1 / (Z + Z_next) along A and B of ring position pos, from its landed Z.
+    // The next tile element is the next cell, or the same clamped cell past
+    // the grid's last ghost; the tile's last row and column are never read.
     auto make_rcp = [&](int pos) {
         real* dst = saux + (pos & (RING3 - 1)) * NPL * NS3;
         for (int e = tid; e < NS3; e += NT3P) {
@@ -193,8 +172,8 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
             dst[(E1A ? 3 : 2) * NS3 + e] = rB;
         }
     };
-    // q of this slice at position pos (FP32): role 0 stages p, role 1 the
-    // normal velocity; boundary conditions are applied when the pair takes them
+    // q of this slice at position pos: role 0 stages p, role 1 the normal
+    // velocity; boundary conditions are applied when the pair takes them
     auto issue_q = [&](int pos) {
         if (!active) return;
         bool fN;
@@ -248,13 +227,11 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
     load_aux(p0 - 1);
     load_aux(p0);
     load_aux(p0 + 1);
-    if constexpr (ASYNC) {
-        issue_q(p0 + 1);
-        cp_async_wait_all();
-        __syncthreads();
-        make_rcp(p0 - 1);
-        make_rcp(p0);
-    }
+    issue_q(p0 + 1);
+    cp_async_wait_all();
+    __syncthreads();
+    make_rcp(p0 - 1);
+    make_rcp(p0);
     __syncthreads();
 
     real wA[2][2], wB[2][2];
@@ -285,16 +262,14 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
 
     for (int p = p0 - 1; p < p1; ++p) {
         const bool emit = p >= p0;
-        if constexpr (ASYNC) {
-            // position p+3: its ring slot and staged q were last read before
-            // the previous position's barrier
-            if (p + 3 <= p1 + 1) {
-                load_aux(p + 3);
-                issue_q(p + 3);
-            }
-            // the reciprocals of position p+2 (its Z landed before the last barrier)
-            if (p + 2 <= p1 + 1) make_rcp(p + 2);
+        // position p+3: its ring slot and staged q were last read before the
+        // previous position's barrier
+        if (p + 3 <= p1 + 1) {
+            load_aux(p + 3);
+            issue_q(p + 3);
         }
+        // the reciprocals of position p+2 (its Z landed before the last barrier)
+        if (p + 2 <= p1 + 1) make_rcp(p + 2);
         real vA = 0, vB = 0;
         if (emit && apply) {
             const long long off = qoffAB + (long long)(p - 1) * a.qs[AXN];
@@ -310,8 +285,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
         Split qm = {0, 0, 0, 0};
         const int L = p, R = p + 1;
         if (active) {
-            if constexpr (ASYNC) take_q(p + 2, qRp, qRn);
-            else load_pn(p + 2, qRp, qRn);
+            take_q(p + 2, qRp, qRn);
             solve(p + 2, qLp, qLn, qRp, qRn, wC, amC, apC);
             real wl[2][2];
             const real sB[2] = {-*plane(p, 1), *plane(p + 1, 1)};
@@ -473,8 +447,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
         // no split exchange).
         if (!xch) pair_sync(pair_id);
         sxch[(8 + H) * NT3 + sl] = cterm;
-        if constexpr (ASYNC) cp_async_wait_all();
-        else if (p + 3 <= p1 + 1) load_aux(p + 3);
+        cp_async_wait_all();
         __syncthreads();
         if (emit && apply) {
             const real crecv = sxch[(8 + 1 - H) * NT3 + sl];
@@ -528,7 +501,7 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3f_kernel(const Sweep3Args<typen
     using real = typename S::real;
     double* red = reinterpret_cast<double*>(reinterpret_cast<real*>(smem_raw) +
                                             RING3 * NPL3F * NS3 + term3_bufs<real>() * NTERM3 * NT3 +
-                                            (XCH3 + qst3_planes<real>()) * NT3);
+                                            (XCH3 + QST3) * NT3);
     ClawCtl* ctl = a.ctl;
     if (ctl->done) return;
     // warps 2k (role 0) and 2k+1 (role 1) share 32 slices
