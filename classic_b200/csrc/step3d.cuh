@@ -49,10 +49,24 @@ struct Sweep3Args {
     ClawCtl* ctl;
 };
 
+constexpr int QST3 = 4;  // staged q planes of NT3 values: [position & 1][p, normal velocity]
+
+// aux ring, two neighbour-term buffers, staged q: 160 KB in FP64, inside the
+// 164 KB shared-memory carveout (the rest of the SM's 256 KB is L1)
 template <typename real>
-constexpr int sweep3_smem_bytes() {
-    return (RING3 * 2 * NS3 + 2 * NTERM3 * NT3) * (int)sizeof(real) + 16 * (int)sizeof(double);
+__host__ __device__ constexpr int sweep3_smem_bytes() {
+    return (RING3 * 2 * NS3 + 2 * NTERM3 * NT3 + QST3 * NT3) * (int)sizeof(real) +
+           16 * (int)sizeof(double);
 }
+
+// one element global -> shared, asynchronously (cp.async, 4 or 8 bytes)
+template <typename real>
+__device__ __forceinline__ void cp_async_el(real* dst, const real* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "n"((int)sizeof(real))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Source index of (possibly ghost) cell idx along an axis of n cells, and
 // whether a solid wall negates the normal velocity (src/3d/bc3.f).
@@ -128,7 +142,8 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
     extern __shared__ __align__(16) unsigned char smem_raw[];
     real* saux = reinterpret_cast<real*>(smem_raw);  // [RING3][2][NS3]
     real* sterm = saux + RING3 * 2 * NS3;            // [2][NTERM3][NT3]
-    double* red = reinterpret_cast<double*>(sterm + 2 * NTERM3 * NT3);
+    real* sq = sterm + 2 * NTERM3 * NT3;             // [QST3][NT3]
+    double* red = reinterpret_cast<double*>(sq + QST3 * NT3);
 
     ClawCtl* ctl = a.ctl;
     if (ctl->done) return;
@@ -207,6 +222,8 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
             }
         }
     };
+    // Z and c of ring position pos, copied asynchronously: issued at the top
+    // of a position, awaited just before its CTA barrier
     auto load_aux = [&](int pos) {
         real* dst = saux + (pos & (RING3 - 1)) * 2 * NS3;
         const long long pofs = (long long)(pos + 1) * a.as[AXN];
@@ -214,8 +231,32 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
             const int sa = e % S3A, sb = e / S3A;
             const int Ai = min(A0 - 2 + sa, mA + 2), Bi = min(B0 - 2 + sb, mB + 2);
             const long long o = pofs + (long long)(Ai + 1) * a.as[AXA] + (long long)(Bi + 1) * a.as[AXB];
-            dst[e] = aux[o];
-            dst[NS3 + e] = aux[o + a.afstride];
+            cp_async_el(dst + e, aux + o);
+            cp_async_el(dst + NS3 + e, aux + o + a.afstride);
+        }
+    };
+    // q of this slice at position pos, staged the same way: h = 0 copies p,
+    // h = 1 the normal velocity; boundary conditions apply when the pair takes them
+    auto issue_q = [&](int pos) {
+        if (!active) return;
+        bool fN;
+        const int pm = bc3_src(pos, mN, a.bc[2 * AXN], a.bc[2 * AXN + 1], fN);
+        const long long off = qoffAB + (long long)(pm - 1) * a.qs[AXN] + (h ? CN * a.fstride : 0);
+        cp_async_el(sq + ((pos & 1) * 2 + h) * NT3 + sl, qold + off);
+    };
+    auto take_q = [&](int pos, real& qp, real& qn) {
+        qp = sq[((pos & 1) * 2) * NT3 + sl];
+        qn = sq[((pos & 1) * 2 + 1) * NT3 + sl];
+        bool fN;
+        (void)bc3_src(pos, mN, a.bc[2 * AXN], a.bc[2 * AXN + 1], fN);
+        if (fN) qn = -qn;
+        if (CN == 3) {
+            const bool pist = (AXN == 2 && pos > mN && a.bc[5] == BC_PISTON) || pistonB;
+            if (pist) {
+                const int ci = AXN == 0 ? pos : A;
+                const int cj = AXN == 1 ? pos : (AXA == 1 ? A : B);
+                qn = (real)(2.0 * piston_speed(a, ci, cj, tbc)) - qn;
+            }
         }
     };
     // shared-memory steps of this thread's own split direction and the other
@@ -251,6 +292,8 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
     load_aux(p0 - 1);
     load_aux(p0);
     load_aux(p0 + 1);
+    issue_q(p0 + 1);
+    cp_async_wait_all();
     __syncthreads();
 
     real wA[2][2], wB[2][2];
@@ -275,6 +318,12 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
 
     for (int p = p0 - 1; p < p1; ++p) {
         const bool emit = p >= p0;
+        // position p+3: its ring slot and staged q were last read before the
+        // previous position's barrier
+        if (p + 3 <= p1 + 1) {
+            load_aux(p + 3);
+            issue_q(p + 3);
+        }
         const int cA = h ? CE1 : 0, cB = h ? CE2 : CN;  // components this thread updates
         real vA = 0, vB = 0;
         if (emit && apply) {
@@ -288,7 +337,7 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
         real wC[2][2], amC[2], apC[2], qRp = 0, qRn = 0;
         real cterm = 0, own_c = 0;  // centre terms: sent to the partner / kept
         if (active) {
-            load_pn(p + 2, qRp, qRn);
+            take_q(p + 2, qRp, qRn);
             solve(p + 2, qLp, qLn, qRp, qRn, wC, amC, apC);
             real wl[2][2];
             const real sB[2] = {-Co(p, 0, 0), Co(p + 1, 0, 0)};
@@ -430,7 +479,7 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
             }
         }
         const real crecv = __shfl_xor_sync(FULL, cterm, 1);
-        if (p + 3 <= p1 + 1) load_aux(p + 3);
+        cp_async_wait_all();
         __syncthreads();
         if (emit && apply) {
             const real* in = sterm + (p & 1) * NTERM3 * NT3;

@@ -32,7 +32,6 @@ constexpr int NPL3F = 4;  // aux planes: Z, c, 1/(Z+Z_e1), 1/(Z+Z_e2)
 
 // Shared memory is sized to the carveout steps (100, 132, 164, 196, 228 KB):
 // what the carveout leaves is L1, which serves the x-sweep's strided loads.
-constexpr int QST3 = 4;  // staged q planes of NT3 values: [position & 1][p, normal velocity]
 // buffers of neighbour terms: two (by position parity) in FP32 (98 KB, the
 // 100 KB step); one in FP64, with a second CTA barrier per position (133 KB,
 // the 164 KB step, instead of 197 KB and the 228 KB step)
@@ -48,15 +47,6 @@ __host__ __device__ constexpr int sweep3f_smem_bytes() {
                (int)sizeof(real) +
            16 * (int)sizeof(double);
 }
-
-// one element global -> shared, asynchronously (cp.async, 4 or 8 bytes)
-template <typename real>
-__device__ __forceinline__ void cp_async_el(real* dst, const real* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
-                 "n"((int)sizeof(real))
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void pair_sync(int id) {
     asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");
