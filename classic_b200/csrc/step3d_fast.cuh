@@ -32,25 +32,20 @@ constexpr int NPL3F = 4;  // aux planes: Z, c, 1/(Z+Z_e1), 1/(Z+Z_e2)
 
 // Shared memory is sized to the carveout steps (100, 132, 164, 196, 228 KB):
 // what the carveout leaves is L1, which serves the x-sweep's strided loads.
-// buffers of neighbour terms: two (by position parity) in FP32 (98 KB, the
-// 100 KB step); one in FP64, with a second CTA barrier per position (149 KB
-// with the staged cell values, the 164 KB step, instead of the 228 KB step)
+// buffers of neighbour terms: two (by position parity) in FP32 (106 KB, the
+// 132 KB step); one in FP64, with a second CTA barrier per position (149 KB,
+// the 164 KB step, instead of the 228 KB step)
 template <typename real>
 __host__ __device__ constexpr int term3_bufs() {
     return sizeof(real) == 4 ? 2 : 1;
 }
 
-// staged planes of the cell values each role updates, [position & 1][role][2]
-// of NT3 values: in FP64, where they fit the same carveout step
-template <typename real>
-__host__ __device__ constexpr int vst3_planes() {
-    return sizeof(real) == 8 ? 8 : 0;
-}
+constexpr int VST3 = 8;  // staged values of the cells each role updates: [position & 1][role][2]
 
 template <typename real>
 __host__ __device__ constexpr int sweep3f_smem_bytes() {
     return (RING3 * NPL3F * NS3 + term3_bufs<real>() * NTERM3 * NT3 +
-            (XCH3 + QST3 + vst3_planes<real>()) * NT3) *
+            (XCH3 + QST3 + VST3) * NT3) *
                (int)sizeof(real) +
            16 * (int)sizeof(double);
 }
@@ -80,8 +75,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
     real* sterm = saux + RING3 * NPL * NS3;          // [NTB][NTERM3][NT3]
     real* sxch = sterm + NTB * NTERM3 * NT3;         // [XCH3][NT3]
     real* sq = sxch + XCH3 * NT3;                    // [QST3][NT3]
-    real* sv = sq + QST3 * NT3;                      // [vst3_planes][NT3]
-    constexpr bool STAGE_V = vst3_planes<real>() > 0;
+    real* sv = sq + QST3 * NT3;                      // [VST3][NT3]
 
     ClawCtl* ctl = a.ctl;
     const int cur = ctl->cur;
@@ -271,19 +265,13 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
         if (p + 2 <= p1 + 1) make_rcp(p + 2);
         const real* vsrc = DIR == 0 ? qold : qnew;
         real vA = 0, vB = 0;
-        if constexpr (STAGE_V) {
-            // the cell values of position p+1, staged for the next position
-            // (only this thread writes that cell, at that position)
-            if (apply && p + 1 >= p0 && p + 1 < p1) {
-                const long long off = qoffAB + (long long)p * a.qs[AXN];
-                real* dv = sv + (((p + 1) & 1) * 2 + H) * 2 * NT3 + sl;
-                cp_async_el(dv, vsrc + off + CA * a.fstride);
-                cp_async_el(dv + NT3, vsrc + off + CB * a.fstride);
-            }
-        } else if (emit && apply) {
-            const long long off = qoffAB + (long long)(p - 1) * a.qs[AXN];
-            vA = vsrc[off + CA * a.fstride];
-            vB = vsrc[off + CB * a.fstride];
+        // the cell values of position p+1, staged for the next position (only
+        // this thread writes that cell, at that position)
+        if (apply && p + 1 >= p0 && p + 1 < p1) {
+            const long long off = qoffAB + (long long)p * a.qs[AXN];
+            real* dv = sv + (((p + 1) & 1) * 2 + H) * 2 * NT3 + sl;
+            cp_async_el(dv, vsrc + off + CA * a.fstride);
+            cp_async_el(dv + NT3, vsrc + off + CB * a.fstride);
         }
         real F1[2] = {0, 0};
         real Qp[2] = {0, 0};
@@ -459,7 +447,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
         __syncthreads();
         if (emit && apply) {
             const real crecv = sxch[(8 + 1 - H) * NT3 + sl];
-            if constexpr (STAGE_V) {
+            {
                 const real* vv = sv + ((p & 1) * 2 + H) * 2 * NT3 + sl;
                 vA = vv[0];
                 vB = vv[NT3];
@@ -514,7 +502,7 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3f_kernel(const Sweep3Args<typen
     using real = typename S::real;
     double* red = reinterpret_cast<double*>(reinterpret_cast<real*>(smem_raw) +
                                             RING3 * NPL3F * NS3 + term3_bufs<real>() * NTERM3 * NT3 +
-                                            (XCH3 + QST3 + vst3_planes<real>()) * NT3);
+                                            (XCH3 + QST3 + VST3) * NT3);
     ClawCtl* ctl = a.ctl;
     if (ctl->done) return;
     // warps 2k (role 0) and 2k+1 (role 1) share 32 slices
