@@ -178,6 +178,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     }
     __syncwarp();
     const int mx = A.mx, my = A.my;
+    const unsigned long long wait_ns = ctl_wait_ns(ctl);
     bool failed = false;
     uint32_t seq_base = 0;
     bool any_work = false;
@@ -210,7 +211,9 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
         const bool out0 = out_lane && c0 < mx, out1 = out_lane && c1 < mx;
 
         auto seq_of = [&](int r) -> uint32_t { return seq_base + (uint32_t)(r - rfirst); };
+        const int skip1 = strip == 0 ? *(volatile const int*)&ctl->skip_row : 0;  // test hook
         auto issue = [&](int r) {
+            if (skip1 != 0 && r == skip1 - 1) return;
             const uint32_t sq = seq_of(r);
             const int sl = (int)(sq & (RING - 1));
             bool nyneg;
@@ -225,7 +228,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
         __syncwarp();
         auto wait_row = [&](int r) -> bool {
             const uint32_t sq = seq_of(r);
-            return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u);
+            return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u, wait_ns);
         };
         // field m of column cs at row r (boundary conditions applied)
         auto fetch = [&](const real* sq, int sr, bool nyneg, const ColSrc& cs, int m) -> real {

@@ -436,6 +436,8 @@ struct claw_handle {
     int device = 0;
     double t_now = 0.0;  // time of the current q (time-dependent boundary conditions)
     double* totals_scratch = nullptr;  // block partials + result of claw_totals
+    unsigned long long wait_ns = 0;    // device wait limit (0: the 2 s default)
+    int skip_row = 0;                  // test hook: 1 + row whose copy is skipped
 
     // Frees everything the handle holds, so an error part-way through
     // claw_create (the handle lives in a unique_ptr there) leaks nothing.
@@ -689,6 +691,8 @@ int claw_step(claw_handle* h, double dt, double* cfl) {
     CUDA_TRY(cudaSetDevice(h->device));
     ClawCtl* c = h->ctl_h;
     std::memset(c, 0, sizeof(ClawCtl));
+    c->wait_ns = h->wait_ns;
+    c->skip_row = h->skip_row;
     c->mode = CTL_SINGLE;
     c->dt = dt;
     c->cur = h->cur;
@@ -701,10 +705,10 @@ int claw_step(claw_handle* h, double dt, double* cfl) {
     h->launches += h->runner->launches_per_step();
     rc = pull_ctl(h);
     if (rc) return rc;
-    h->cur = c->cur;
-    h->t_now += dt;
+    h->cur = c->cur;  // unchanged when a device wait gave up (the step is not kept)
     if (cfl) *cfl = c->cfl_last;
     if (c->err & CTL_ERR_TMA_TIMEOUT) return fail(CLAW_E_DEVICE, "device wait timed out");
+    h->t_now += dt;
     return 0;
 }
 
@@ -737,6 +741,8 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
     const claw_config& cfg = h->cfg;
     ClawCtl* c = h->ctl_h;
     std::memset(c, 0, sizeof(ClawCtl));
+    c->wait_ns = h->wait_ns;
+    c->skip_row = h->skip_row;
     c->t = c->told = tstart;
     c->tstart = tstart;
     c->tend = tend;
@@ -785,17 +791,31 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
             rc = pull_ctl(h);
             if (rc) return rc;
         } else {
-            // steps per graph chunk: one host check per chunk
+            // Rounds: each launches the steps still needed as far as the host
+            // can tell from the control block (the steps left to tend at the
+            // current dt, or to steps_max), as graph chunks plus single
+            // launches for the remainder, then reads the control block once.
+            // A round that falls short (a rejected step, a smaller dt) is
+            // followed by another; launches past `done` return at once.
             const long long cells = (long long)h->g.mx * h->g.my * h->g.mz;
             const int chunk = cells >= (1LL << 22) ? 8 : 32;
             rc = ensure_graph(h, chunk);
             if (rc) return rc;
             for (;;) {
-                CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
-                h->launches += (long long)chunk * h->runner->launches_per_step();
+                long long want = (long long)c->maxn - c->n;
+                if (c->dt_variable && c->dt > 0.0) {
+                    const double left = (c->tend - c->told) / c->dt;
+                    if (left < (double)want) want = (long long)std::ceil(left - 1e-9);
+                }
+                want = std::max(1LL, std::min(want, 4096LL));
+                long long k = 0;
+                for (; k + chunk <= want; k += chunk)
+                    CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
+                for (; k < want; ++k) CUDA_TRY(h->runner->launch(h->stream));
+                h->launches += want * h->runner->launches_per_step();
                 rc = pull_ctl(h);
                 if (rc) return rc;
-                if (c->done) break;
+                if (c->done || c->err) break;
             }
         }
     }
@@ -848,6 +868,14 @@ int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld, lo
 }
 
 long long claw_launch_count(claw_handle* h) { return h ? h->launches : 0; }
+
+int claw_debug_fault(claw_handle* h, long long wait_ns, int skip_row) {
+    if (!h) return fail(CLAW_E_INVALID, "null handle");
+    if (wait_ns < 0) return fail(CLAW_E_INVALID, "wait_ns must be >= 0");
+    h->wait_ns = (unsigned long long)wait_ns;
+    h->skip_row = skip_row < -2 ? 0 : skip_row + 1;
+    return 0;
+}
 
 int claw_totals(claw_handle* h, double* totals) {
     if (!h || !totals) return fail(CLAW_E_INVALID, "null argument");

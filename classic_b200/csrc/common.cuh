@@ -25,10 +25,17 @@ struct ClawCtl {
     int mode;                      // CTL_ADVANCE or CTL_SINGLE
     int dt_variable;
     int err;                       // device error flags (CTL_ERR_*)
-    int pad;
+    int skip_row;                  // test hook: 1 + the row whose copy strip 0 skips (0: none)
     unsigned long long cfl_sweep[2];  // dimensional splitting: Courant maxima of the
                                       // y-sweep and of Strang's last x-sweep
+    unsigned long long wait_ns;    // limit of a device-side wait (0: the 2 s default)
 };
+
+constexpr unsigned long long WAIT_NS_DEFAULT = 2000000000ull;
+__device__ __forceinline__ unsigned long long ctl_wait_ns(const ClawCtl* c) {
+    const unsigned long long w = *(volatile const unsigned long long*)&c->wait_ns;
+    return w ? w : WAIT_NS_DEFAULT;
+}
 
 enum { CTL_ADVANCE = 0, CTL_SINGLE = 1 };
 
@@ -43,6 +50,10 @@ __device__ __forceinline__ void ctl_finish_step(ClawCtl* c) {
     c->cfl_bits = 0ull;
     c->ctas_done = 0u;
     c->cfl_last = cfl;
+    if (c->err) {  // a device wait gave up: the step's output is incomplete
+        c->done = 1;
+        return;
+    }
     if (c->mode == CTL_SINGLE) {
         c->cur ^= 1;
         return;
@@ -145,14 +156,16 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
-// Bounded wait on an mbarrier phase: gives up after ~2 s of wall time and
-// reports failure instead of hanging the GPU.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: gives up after limit_ns of wall time
+// (2 s unless the control block sets another limit) and reports failure
+// instead of hanging the GPU.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  unsigned long long limit_ns = 2000000000ull) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 0u && globaltimer_ns() - t0 > 2000000000ull) return false;
+        if ((it & 255u) == 0u && globaltimer_ns() - t0 > limit_ns) return false;
     }
 }
 

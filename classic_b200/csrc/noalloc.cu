@@ -43,7 +43,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
-void* g_scratch_dev[MAX_DEVICES] = {};  // device address of g_noalloc_scratch, per device
 
 int nofail(int code, const char* msg) {
     clawb200::set_last_error(msg);
@@ -52,23 +51,33 @@ int nofail(int code, const char* msg) {
 
 // Device address of the scratch array on the current device.  The host-side
 // name g_noalloc_scratch is only a stand-in; the kernel must be given this
-// address.  Looked up once per device (the first call on a device).
-int scratch_address(int dev, void** out) {
-    if (dev < 0 || dev >= MAX_DEVICES) return nofail(CLAW_E_INVALID, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_dev[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            char buf[256];
-            snprintf(buf, sizeof(buf), "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-            return nofail(CLAW_E_CUDA, buf);
-        }
-        g_scratch_dev[dev] = p;
+// address.  It is looked up on every call (a lookup allocates nothing), so a
+// context rebuilt after cudaDeviceReset is served from its own module.
+int scratch_address(void** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        char buf[256];
+        snprintf(buf, sizeof(buf), "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return nofail(CLAW_E_CUDA, buf);
     }
-    *out = g_scratch_dev[dev];
+    *out = p;
     return 0;
 }
+
+// Per device and kernel instantiation: the dynamic shared-memory attribute
+// has been set and the resident CTAs per SM are known.  A launch that fails
+// (a context rebuilt after cudaDeviceReset has lost the attribute) clears the
+// entry and is retried once after the set-up runs again.
+template <class S, class M>
+struct LaunchSetup {
+    static int per_sm[MAX_DEVICES];
+    static int nsm[MAX_DEVICES];
+};
+template <class S, class M>
+int LaunchSetup<S, M>::per_sm[MAX_DEVICES] = {};
+template <class S, class M>
+int LaunchSetup<S, M>::nsm[MAX_DEVICES] = {};
 
 PFN_cuTensorMapEncodeTiled_v12000 encode() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -137,24 +146,40 @@ int launch_step(const claw_config* c, const S& solver, const double* q_in, doubl
         if (rc) return rc;
     }
     const int smem = R::SMEM;
-    if (cudaFuncSetAttribute(step2_kernel<S, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-        cudaSuccess)
-        return nofail(CLAW_E_CUDA, "cudaFuncSetAttribute failed");
-    int dev = 0, nsm = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_kernel<S, M>, 32 * WARPS2D, smem) !=
-            cudaSuccess || per_sm < 1)
-        return nofail(CLAW_E_CUDA, "occupancy query failed");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
+        return nofail(CLAW_E_CUDA, "cudaGetDevice failed or device ordinal out of range");
     a.units = (long long)a.nstrips * my;
-    const long long want = a.units / 48 > 0 ? a.units / 48 : 1;
-    const long long full = (long long)nsm * per_sm * WARPS2D;
-    const long long nw = want < full ? want : full;
-    const int grid = (int)((nw + WARPS2D - 1) / WARPS2D);
-    a.nwarps = (int)nw;
-    step2_kernel<S, M><<<grid, 32 * WARPS2D, smem, st>>>(a);
-    if (cudaGetLastError() != cudaSuccess) return nofail(CLAW_E_CUDA, "step kernel launch failed");
-    return 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        int per_sm = 0, nsm = 0;
+        {
+            std::lock_guard<std::mutex> lock(g_mu);
+            if (!LaunchSetup<S, M>::per_sm[dev]) {
+                int n = 0, r = 0;
+                if (cudaFuncSetAttribute(step2_kernel<S, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem) != cudaSuccess)
+                    return nofail(CLAW_E_CUDA, "cudaFuncSetAttribute failed");
+                if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, step2_kernel<S, M>, 32 * WARPS2D,
+                                                                  smem) != cudaSuccess || r < 1)
+                    return nofail(CLAW_E_CUDA, "occupancy query failed");
+                LaunchSetup<S, M>::nsm[dev] = n;
+                LaunchSetup<S, M>::per_sm[dev] = r;
+            }
+            per_sm = LaunchSetup<S, M>::per_sm[dev];
+            nsm = LaunchSetup<S, M>::nsm[dev];
+        }
+        const long long want = a.units / 48 > 0 ? a.units / 48 : 1;
+        const long long full = (long long)nsm * per_sm * WARPS2D;
+        const long long nw = want < full ? want : full;
+        const int grid = (int)((nw + WARPS2D - 1) / WARPS2D);
+        a.nwarps = (int)nw;
+        step2_kernel<S, M><<<grid, 32 * WARPS2D, smem, st>>>(a);
+        if (cudaGetLastError() == cudaSuccess) return 0;
+        std::lock_guard<std::mutex> lock(g_mu);
+        LaunchSetup<S, M>::per_sm[dev] = 0;
+    }
+    return nofail(CLAW_E_CUDA, "step kernel launch failed");
 }
 
 }  // namespace
@@ -179,12 +204,21 @@ extern "C" int claw_step2d_noalloc(const claw_config* cfg, const double* q_in, d
             return nofail(CLAW_E_INVALID, "boundary conditions must be extrap, periodic or wall");
     if (cfg->order < 1 || cfg->order > 2 || cfg->dimensional_split != 0)
         return nofail(CLAW_E_INVALID, "unsupported method");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return nofail(CLAW_E_CUDA, "cudaGetDevice failed");
-    void* scratch = nullptr;
-    int rc = scratch_address(dev, &scratch);
-    if (rc) return rc;
+    // claw_step runs the before-step routine on a copy of the unscaled aux
+    // that it allocates; without an allocation there is no such copy.
+    if (cfg->b4step_id != CLAW_B4STEP_NONE)
+        return nofail(CLAW_E_UNSUPPORTED, "claw_step2d_noalloc runs no before-step routine");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Each call waits for the stream and uploads its control block from a
+    // host variable, neither of which a captured graph could replay.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess)
+        return nofail(CLAW_E_CUDA, "cudaStreamIsCapturing failed");
+    if (cap != cudaStreamCaptureStatusNone)
+        return nofail(CLAW_E_INVALID, "claw_step2d_noalloc must not be called during stream capture");
+    void* scratch = nullptr;
+    int rc = scratch_address(&scratch);
+    if (rc) return rc;
 
     // The array keeps the previous call's contents: reset the whole block.
     ClawCtl h;
@@ -224,5 +258,8 @@ extern "C" int claw_step2d_noalloc(const claw_config* cfg, const double* q_in, d
         return nofail(CLAW_E_CUDA, "step failed on the device");
     if (h.err & CTL_ERR_TMA_TIMEOUT) return nofail(CLAW_E_DEVICE, "device wait timed out");
     *cfl = h.cfl_last;
+    // A NaN Courant number means a NaN in the new state (for instance a
+    // capacity field that is not positive, which this path does not check).
+    if (h.cfl_last != h.cfl_last) return nofail(CLAW_E_NAN, "Courant number is NaN");
     return 0;
 }

@@ -236,8 +236,13 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
     const bool cx_ok = c >= 0 && c <= mx;
     const bool cy_ok = c >= -1 && c <= mx;
 
+    // wait limit; test hook: strip 0 skips the copy of one row (its wait then
+    // runs out, nothing faults)
+    const unsigned long long wait_ns = ctl_wait_ns(ctl);
+    const int skip1 = strip == 0 ? *(volatile const int*)&ctl->skip_row : 0;
     auto seq_of = [&](int r) -> uint32_t { return seq_base + (uint32_t)(r - rfirst); };
     auto issue = [&](int r) {
+        if (skip1 != 0 && r == skip1 - 1) return;
         const uint32_t sq = seq_of(r);
         const int sl = (int)(sq & (RING - 1));
         unsigned char* dst = ring + sl * R::SLOT;
@@ -255,7 +260,7 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
 
     auto wait_row = [&](int r) -> bool {
         const uint32_t sq = seq_of(r);
-        return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u);
+        return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u, wait_ns);
     };
     auto slot_ptr = [&](int r) -> const unsigned char* {
         return ring + (int)(seq_of(r) & (RING - 1)) * R::SLOT;

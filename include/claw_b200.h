@@ -194,6 +194,16 @@ int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld,
 /* Number of step-kernel launches issued on this handle so far. */
 long long claw_launch_count(claw_handle* h);
 
+/* Test hook for the device-wait failure path (no counterpart in the
+ * reference, whose steps have no device waits).  wait_ns limits every
+ * device-side wait of the handle's later steps (0: the 2 s default);
+ * skip_row >= -2 makes the 2D step kernels of strip 0 skip the copy of that
+ * row (-2 .. my+1, ghost rows included), so its wait runs out after wait_ns
+ * and nothing faults; skip_row < -2 turns the hook off.  A step whose wait
+ * ran out is not accepted: claw_advance / claw_step return CLAW_E_DEVICE and
+ * the current q stays that of the last accepted step. */
+int claw_debug_fault(claw_handle* h, long long wait_ns, int skip_row);
+
 /* Conserved totals of the current q: totals[m] = sum over interior cells of
  * capa * q_m (capa = 1 without a capacity function), formed in FP64 with
  * Neumaier's compensated summation whatever the storage precision, in a fixed
@@ -213,10 +223,18 @@ int claw_totals(claw_handle* h, double* totals);
  *   stream      : a cudaStream_t (NULL = the default stream); the call waits
  *                 for it and returns the Courant number in *cfl
  * The step kernel's scratch (its 256-byte control block) is a static device
- * array of the library: the first call on a device looks up its address (make
- * that first call before any stream capture); calls that overlap on the GPU
- * race on it; each call resets it.  Requests whose scratch would exceed the
- * 256-byte maximum are rejected with CLAW_E_INVALID. */
+ * array of the library; every call looks up its device address on the
+ * current device and resets it, and calls that overlap on the GPU race on
+ * it.  Requests whose scratch would exceed the 256-byte maximum are rejected
+ * with CLAW_E_INVALID.  Limits:
+ *   - it must not be called while the stream is being captured (each call
+ *     waits for the stream and uploads the control block from a host
+ *     variable): CLAW_E_INVALID;
+ *   - no before-step routine (b4step_id must be CLAW_B4STEP_NONE;
+ *     otherwise CLAW_E_UNSUPPORTED): the hook needs a copy of the unscaled
+ *     aux that this path cannot allocate;
+ *   - the caller guarantees a positive capacity field (claw_set_aux checks
+ *     it; this path does not): a NaN Courant number returns CLAW_E_NAN. */
 int claw_step2d_noalloc(const claw_config* cfg, const double* q_in, double* q_out,
                         long long q_ld, const double* aux, long long aux_ld, double dt,
                         double* cfl, void* stream);

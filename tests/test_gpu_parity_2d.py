@@ -197,6 +197,40 @@ def test_fast_fp64_full_run_4096_within_1e12():
     assert np.all(d <= 1e-12), d
 
 
+def test_config2_1024_against_oracle_50_steps():
+    """The 1024^2 size of the radial-acoustics workload, every arithmetic
+    against the CPU restatement itself (not through the reference-order GPU
+    kernel): claw2 from t = 0 to 0.045 (51 steps at Courant number 0.9).
+    Reference order: bit-identical q and dt/Courant returns.  Fused FP64 (the
+    benchmark's arithmetic): the same dt sequence and Courant numbers, max
+    relative difference per field <= 1e-12.  FP32 update: the same number of
+    steps, <= 1e-5."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=1024)
+    o = OracleGrid(rd.clawdata, solver, params)
+    o.set_q(q0)
+    info_o, so = o.advance(0.0, 0.045, 0.01)
+    assert info_o == 0 and so["steps_taken"] >= 50
+    qo = o.get_q()
+    for prec in ("fp64", "fp64_fma", "fp32"):
+        s = Solver(rd.clawdata, solver, params, precision=prec)
+        s.set_q(q0)
+        info, st = s.advance(0.0, 0.045, 0.01)
+        q = s.get_q()
+        s.close()
+        assert info == 0
+        assert st["steps_taken"] == so["steps_taken"], prec
+        if prec == "fp32":
+            assert np.all(rel_diff(q, qo) <= 1e-5)
+            continue
+        for key in ("t_reached", "dt_next", "cfl_max_seen", "cfl_last", "dt_min", "dt_max_taken"):
+            assert st[key] == so[key], (prec, key)
+        if prec == "fp64":
+            assert same(q, qo)
+        else:
+            d = rel_diff(q, qo)
+            assert np.all(d <= 1e-12), d
+
+
 def test_fast_fp32_tracks_fp64_all_bcs():
     for bc in BCS:
         rd, solver, params, q0, _ = problems.random_acoustics_2d(70, 33, seed=2, bc=bc)

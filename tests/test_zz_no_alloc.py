@@ -99,3 +99,34 @@ def test_noalloc_rejects_bad_requests():
     rc = lib.claw_step2d_noalloc(ctypes.byref(cfg), ctypes.c_void_p(16), ctypes.c_void_p(32), 63,
                                  None, 0, 0.001, ctypes.byref(cfl), None)
     assert rc == -1  # odd row pitch
+    # a before-step routine needs a copy of the unscaled aux this path cannot allocate
+    rd, solver, params, q0, aux = problems.advection_2d_annulus()
+    cfg = make_config(rd.clawdata, solver, params)
+    cfg.b4step_id = 1
+    cfg.b4step_param = 1.0
+    rc = lib.claw_step2d_noalloc(ctypes.byref(cfg), ctypes.c_void_p(16), ctypes.c_void_p(32), 64,
+                                 ctypes.c_void_p(64), 68, 0.001, ctypes.byref(cfl), None)
+    assert rc == -3
+
+
+def test_noalloc_refuses_stream_capture():
+    """A captured graph could not replay the call's stream wait and host upload:
+    the entry point refuses before touching the stream."""
+    import torch
+
+    lib = _lib.load()
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=64)
+    cfg = make_config(rd.clawdata, solver, params)
+    dev = torch.device("cuda", 0)
+    bufs = [torch.zeros((3, 64, 64), dtype=torch.float64, device=dev) for _ in range(2)]
+    cfl = ctypes.c_double(0.0)
+    side = torch.cuda.Stream(dev)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        rc = lib.claw_step2d_noalloc(ctypes.byref(cfg), ctypes.c_void_p(bufs[0].data_ptr()),
+                                     ctypes.c_void_p(bufs[1].data_ptr()), 64, None, 0, 0.001,
+                                     ctypes.byref(cfl), ctypes.c_void_p(side.cuda_stream))
+        bufs[1].add_(1.0)
+    assert rc == -1
+    assert "capture" in lib.claw_last_error().decode()
+    del graph
