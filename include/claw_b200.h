@@ -273,6 +273,12 @@ int claw_batch_autotune(claw_batch* b, const double* dt_trial, int repeats, int*
 /* Set the launch shape directly (a shape kept from an earlier tuning run). */
 int claw_batch_set_shape(claw_batch* b, int min_rows, int ctas_per_sm);
 
+/* FP64 fused multiply-add throughput of the current device in TFLOP/s (2
+ * flops per FMA; independent FMA chains, best of five timed launches), the
+ * ceiling beside HBM bandwidth for the FP64 step kernels.  No counterpart in
+ * the reference. */
+int claw_probe_fp64(double* tflops, double* ms_best);
+
 /* Last error message of the calling thread ("" if none). */
 const char* claw_last_error(void);
 

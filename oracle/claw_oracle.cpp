@@ -42,6 +42,8 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <atomic>
+#include <thread>
 
 extern "C" {
 
@@ -81,6 +83,15 @@ int orc_set_source(int id, int ndim, double xlower) {
 // Before-step routine (the example's b4step2; 0 = the reference's default
 // no-op).  1: the edge velocities (aux fields 1, 2) of the variable-velocity
 // advection solver scaled by cos(pi t / T), from an unscaled copy.
+// Host threads of the timing variant (orc_set_threads); 1 runs the serial
+// loops, which is the order every parity test compares against.
+static int g_threads = 1;
+
+int orc_set_threads(int n) {
+    g_threads = n < 1 ? 1 : n;
+    return g_threads;
+}
+
 static int g_b4 = 0;
 static double g_b4_period = 1.0;
 
@@ -710,6 +721,24 @@ extern "C" {
 // ------------------------------------------------------------------ step2 ---
 // src/2d/step2.f90:2-251.  qold/qnew/aux in the reference layout with ghost
 // cells; qnew must equal qold on entry.  Returns 0, or -1 for an unknown solver.
+}  // extern "C"
+
+// Run body(item, thread) for items 0..count-1 on g_threads host threads
+// (std::thread; items handed out in order from an atomic counter), then join.
+template <class F>
+static void parallel_items(int count, int nthreads, F&& body) {
+    std::atomic<int> next{0};
+    auto worker = [&](int tid) {
+        for (int k = next.fetch_add(1); k < count; k = next.fetch_add(1)) body(k, tid);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+}
+
+extern "C" {
+
 int orc_step2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const double* qold,
               double* qnew, const double* aux, double dx, double dy, double dt,
               const int* method, const int* mthlim, int use_fwave, double* cfl_out) {
@@ -728,43 +757,49 @@ int orc_step2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const dou
     auto A = [&](int ma, int i, int j) {
         return aux[(ma - 1) + maux * ((i - (1 - mbc)) + nx * (j - (1 - mbc)))];
     };
-    std::vector<double> qadd(meqn * n), fadd(meqn * n), gadd(2 * meqn * n), q1d(meqn * n);
-    std::vector<double> dtdx1d(n), dtdy1d(n), aux1(std::max(maux, 1) * n),
-        aux2(std::max(maux, 1) * n), aux3(std::max(maux, 1) * n);
-    std::vector<double> wave(meqn * mwaves * n), s(mwaves * n), amdq(meqn * n), apdq(meqn * n),
-        cqxx(meqn * n), bmasdq(meqn * n), bpasdq(meqn * n);
+    // flux2's work arrays (one set per thread in the OpenMP timing build)
+    struct Work {
+        std::vector<double> qadd, fadd, gadd, q1d, dtdx1d, dtdy1d, aux1, aux2, aux3, wave, s, amdq,
+            apdq, cqxx, bmasdq, bpasdq;
+        Work(int meqn, int mwaves, int maux, int n)
+            : qadd(meqn * n), fadd(meqn * n), gadd(2 * meqn * n), q1d(meqn * n), dtdx1d(n),
+              dtdy1d(n), aux1(std::max(maux, 1) * n), aux2(std::max(maux, 1) * n),
+              aux3(std::max(maux, 1) * n), wave(meqn * mwaves * n), s(mwaves * n), amdq(meqn * n),
+              apdq(meqn * n), cqxx(meqn * n), bmasdq(meqn * n), bpasdq(meqn * n) {}
+    };
     const Slice sl{meqn, 1 - mbc}, sa{maux, 1 - mbc};
-    auto GA = [&](int m, int k, int i) { return gadd[(m - 1) + meqn * (k - 1) + 2 * meqn * (i - (1 - mbc))]; };
     const int index_capa = method[5];
-    double cfl = 0.0;
     const double dtdx = dt / dx, dtdy = dt / dy;
-    if (index_capa == 0)
-        for (int i = 0; i < n; ++i) { dtdx1d[i] = dtdx; dtdy1d[i] = dtdy; }
+    auto init = [&](Work& w) {
+        if (index_capa == 0)
+            for (int i = 0; i < n; ++i) { w.dtdx1d[i] = dtdx; w.dtdy1d[i] = dtdy; }
+    };
 
-    // x-sweeps (src/2d/step2.f90:92-165)
-    for (int j = 0; j <= my + 1; ++j) {
+    // x-sweep of row j (src/2d/step2.f90:92-165)
+    auto x_slice = [&](int j, Work& w, double& cfl) {
+        auto GA = [&](int m, int k, int i) { return w.gadd[(m - 1) + meqn * (k - 1) + 2 * meqn * (i - (1 - mbc))]; };
         for (int i = 1 - mbc; i <= mx + mbc; ++i)
-            for (int m = 1; m <= meqn; ++m) q1d[sl.at(m, i)] = Q(qold, m, i, j);
+            for (int m = 1; m <= meqn; ++m) w.q1d[sl.at(m, i)] = Q(qold, m, i, j);
         if (index_capa > 0)
-            for (int i = 1 - mbc; i <= mx + mbc; ++i) dtdx1d[i - (1 - mbc)] = dtdx / A(index_capa, i, j);
+            for (int i = 1 - mbc; i <= mx + mbc; ++i) w.dtdx1d[i - (1 - mbc)] = dtdx / A(index_capa, i, j);
         if (maux > 0)
             for (int i = 1 - mbc; i <= mx + mbc; ++i)
                 for (int ma = 1; ma <= maux; ++ma) {
-                    aux1[sa.at(ma, i)] = A(ma, i, j - 1);
-                    aux2[sa.at(ma, i)] = A(ma, i, j);
-                    aux3[sa.at(ma, i)] = A(ma, i, j + 1);
+                    w.aux1[sa.at(ma, i)] = A(ma, i, j - 1);
+                    w.aux2[sa.at(ma, i)] = A(ma, i, j);
+                    w.aux3[sa.at(ma, i)] = A(ma, i, j + 1);
                 }
         double cfl1d;
-        flux2(1, maxm, meqn, mwaves, maux, mbc, mx, q1d.data(), dtdx1d.data(), aux1.data(),
-              aux2.data(), aux3.data(), method, mthlim, qadd.data(), fadd.data(), gadd.data(),
-              &cfl1d, wave.data(), s.data(), amdq.data(), apdq.data(), cqxx.data(),
-              bmasdq.data(), bpasdq.data(), rpn2, rpt2, use_fwave != 0);
+        flux2(1, maxm, meqn, mwaves, maux, mbc, mx, w.q1d.data(), w.dtdx1d.data(), w.aux1.data(),
+              w.aux2.data(), w.aux3.data(), method, mthlim, w.qadd.data(), w.fadd.data(),
+              w.gadd.data(), &cfl1d, w.wave.data(), w.s.data(), w.amdq.data(), w.apdq.data(),
+              w.cqxx.data(), w.bmasdq.data(), w.bpasdq.data(), rpn2, rpt2, use_fwave != 0);
         cfl = std::fmax(cfl, cfl1d);
         if (index_capa == 0) {
             for (int i = 1; i <= mx; ++i)
                 for (int m = 1; m <= meqn; ++m) {
-                    QN(m, i, j) = QN(m, i, j) + qadd[sl.at(m, i)] -
-                                  dtdx * (fadd[sl.at(m, i + 1)] - fadd[sl.at(m, i)]) -
+                    QN(m, i, j) = QN(m, i, j) + w.qadd[sl.at(m, i)] -
+                                  dtdx * (w.fadd[sl.at(m, i + 1)] - w.fadd[sl.at(m, i)]) -
                                   dtdy * (GA(m, 2, i) - GA(m, 1, i));
                     QN(m, i, j - 1) = QN(m, i, j - 1) - dtdy * GA(m, 1, i);
                     QN(m, i, j + 1) = QN(m, i, j + 1) + dtdy * GA(m, 2, i);
@@ -772,41 +807,42 @@ int orc_step2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const dou
         } else {
             for (int i = 1; i <= mx; ++i)
                 for (int m = 1; m <= meqn; ++m) {
-                    QN(m, i, j) = QN(m, i, j) + qadd[sl.at(m, i)] -
-                                  (dtdx * (fadd[sl.at(m, i + 1)] - fadd[sl.at(m, i)]) +
+                    QN(m, i, j) = QN(m, i, j) + w.qadd[sl.at(m, i)] -
+                                  (dtdx * (w.fadd[sl.at(m, i + 1)] - w.fadd[sl.at(m, i)]) +
                                    dtdy * (GA(m, 2, i) - GA(m, 1, i))) /
                                       A(index_capa, i, j);
                     QN(m, i, j - 1) = QN(m, i, j - 1) - dtdy * GA(m, 1, i) / A(index_capa, i, j - 1);
                     QN(m, i, j + 1) = QN(m, i, j + 1) + dtdy * GA(m, 2, i) / A(index_capa, i, j + 1);
                 }
         }
-    }
+    };
 
-    // y-sweeps (src/2d/step2.f90:173-248)
-    for (int i = 0; i <= mx + 1; ++i) {
+    // y-sweep of column i (src/2d/step2.f90:173-248)
+    auto y_slice = [&](int i, Work& w, double& cfl) {
+        auto GA = [&](int m, int k, int i) { return w.gadd[(m - 1) + meqn * (k - 1) + 2 * meqn * (i - (1 - mbc))]; };
         for (int j = 1 - mbc; j <= my + mbc; ++j)
-            for (int m = 1; m <= meqn; ++m) q1d[sl.at(m, j)] = Q(qold, m, i, j);
+            for (int m = 1; m <= meqn; ++m) w.q1d[sl.at(m, j)] = Q(qold, m, i, j);
         if (index_capa > 0)
-            for (int j = 1 - mbc; j <= my + mbc; ++j) dtdy1d[j - (1 - mbc)] = dtdy / A(index_capa, i, j);
+            for (int j = 1 - mbc; j <= my + mbc; ++j) w.dtdy1d[j - (1 - mbc)] = dtdy / A(index_capa, i, j);
         if (maux > 0)
             for (int j = 1 - mbc; j <= my + mbc; ++j)
                 for (int ma = 1; ma <= maux; ++ma) {
-                    aux1[sa.at(ma, j)] = A(ma, i - 1, j);
-                    aux2[sa.at(ma, j)] = A(ma, i, j);
-                    aux3[sa.at(ma, j)] = A(ma, i + 1, j);
+                    w.aux1[sa.at(ma, j)] = A(ma, i - 1, j);
+                    w.aux2[sa.at(ma, j)] = A(ma, i, j);
+                    w.aux3[sa.at(ma, j)] = A(ma, i + 1, j);
                 }
         double cfl1d;
-        flux2(2, maxm, meqn, mwaves, maux, mbc, my, q1d.data(), dtdy1d.data(), aux1.data(),
-              aux2.data(), aux3.data(), method, mthlim, qadd.data(), fadd.data(), gadd.data(),
-              &cfl1d, wave.data(), s.data(), amdq.data(), apdq.data(), cqxx.data(),
-              bmasdq.data(), bpasdq.data(), rpn2, rpt2, use_fwave != 0);
+        flux2(2, maxm, meqn, mwaves, maux, mbc, my, w.q1d.data(), w.dtdy1d.data(), w.aux1.data(),
+              w.aux2.data(), w.aux3.data(), method, mthlim, w.qadd.data(), w.fadd.data(),
+              w.gadd.data(), &cfl1d, w.wave.data(), w.s.data(), w.amdq.data(), w.apdq.data(),
+              w.cqxx.data(), w.bmasdq.data(), w.bpasdq.data(), rpn2, rpt2, use_fwave != 0);
         cfl = std::fmax(cfl, cfl1d);
         if (index_capa == 0) {
             for (int j = 1; j <= my; ++j)
                 for (int m = 1; m <= meqn; ++m) {
                     QN(m, i, j) = QN(m, i, j) +
-                                  (qadd[sl.at(m, j)] -
-                                   dtdy * (fadd[sl.at(m, j + 1)] - fadd[sl.at(m, j)]) -
+                                  (w.qadd[sl.at(m, j)] -
+                                   dtdy * (w.fadd[sl.at(m, j + 1)] - w.fadd[sl.at(m, j)]) -
                                    dtdx * (GA(m, 2, j) - GA(m, 1, j)));
                     QN(m, i - 1, j) = QN(m, i - 1, j) - dtdx * GA(m, 1, j);
                     QN(m, i + 1, j) = QN(m, i + 1, j) + dtdx * GA(m, 2, j);
@@ -814,14 +850,38 @@ int orc_step2(int meqn, int mwaves, int maux, int mbc, int mx, int my, const dou
         } else {
             for (int j = 1; j <= my; ++j)
                 for (int m = 1; m <= meqn; ++m) {
-                    QN(m, i, j) = QN(m, i, j) + qadd[sl.at(m, j)] -
-                                  (dtdy * (fadd[sl.at(m, j + 1)] - fadd[sl.at(m, j)]) +
+                    QN(m, i, j) = QN(m, i, j) + w.qadd[sl.at(m, j)] -
+                                  (dtdy * (w.fadd[sl.at(m, j + 1)] - w.fadd[sl.at(m, j)]) +
                                    dtdx * (GA(m, 2, j) - GA(m, 1, j))) /
                                       A(index_capa, i, j);
                     QN(m, i - 1, j) = QN(m, i - 1, j) - dtdx * GA(m, 1, j) / A(index_capa, i - 1, j);
                     QN(m, i + 1, j) = QN(m, i + 1, j) + dtdx * GA(m, 2, j) / A(index_capa, i + 1, j);
                 }
         }
+    };
+
+    double cfl = 0.0;
+    if (g_threads > 1) {
+        // Timing variant only: the reference's step2 is serial.  A slice
+        // updates its own row and the two beside it, so slices three apart
+        // never touch the same cell: each of three passes runs every third
+        // slice in parallel (the scheme step3.f90 uses for its 3D slices).
+        // Each cell then receives its contributions in another order than the
+        // serial sweep's.
+        const int nt = g_threads;
+        std::vector<Work> ws;
+        for (int t = 0; t < nt; ++t) { ws.emplace_back(meqn, mwaves, maux, n); init(ws.back()); }
+        std::vector<double> cfls(nt, 0.0);
+        for (int col = 0; col < 3; ++col)
+            parallel_items((my + 2 - col + 2) / 3, nt, [&](int k, int t) { x_slice(col + 3 * k, ws[t], cfls[t]); });
+        for (int col = 0; col < 3; ++col)
+            parallel_items((mx + 2 - col + 2) / 3, nt, [&](int k, int t) { y_slice(col + 3 * k, ws[t], cfls[t]); });
+        for (double c : cfls) cfl = std::fmax(cfl, c);
+    } else {
+        Work w(meqn, mwaves, maux, n);
+        init(w);
+        for (int j = 0; j <= my + 1; ++j) x_slice(j, w, cfl);
+        for (int i = 0; i <= mx + 1; ++i) y_slice(i, w, cfl);
     }
     *cfl_out = cfl;
     return 0;
@@ -1441,9 +1501,13 @@ int orc_step3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, c
     auto AX = [&](int ma, int i, int j, int k) {
         return aux[(ma - 1) + maux * ((i - (1 - mbc)) + nx * ((j - (1 - mbc)) + ny * (k - (1 - mbc))))];
     };
-    std::vector<double> q1d(meqn * n1), dtd1d(n1), qadd(meqn * n1), fadd(meqn * n1),
-        gadd(meqn * 6 * n1), hadd(meqn * 6 * n1), x1(maux * n1 * 3), x2(maux * n1 * 3),
-        x3(maux * n1 * 3);
+    // flux3's work arrays (one set per thread in the OpenMP timing build)
+    struct Work3 {
+        std::vector<double> q1d, dtd1d, qadd, fadd, gadd, hadd, x1, x2, x3;
+        Work3(int meqn, int maux, int n1)
+            : q1d(meqn * n1), dtd1d(n1), qadd(meqn * n1), fadd(meqn * n1), gadd(meqn * 6 * n1),
+              hadd(meqn * 6 * n1), x1(maux * n1 * 3), x2(maux * n1 * 3), x3(maux * n1 * 3) {}
+    };
     const Slice Q{meqn, 1 - mbc};
     const double dtdx = dt / dx, dtdy = dt / dy, dtdz = dt / dz;
     double cfl = 0.0;
@@ -1456,73 +1520,101 @@ int orc_step3(int meqn, int mwaves, int maux, int mbc, int mx, int my, int mz, c
         // directions: n = normal, e1 = y-like, e2 = z-like
         const int dn = ixyz - 1, d1 = trans_dir(ixyz, 2) - 1, d2 = trans_dir(ixyz, 3) - 1;
         const int len = dims[dn];
-        for (int i = 0; i < n1; ++i) dtd1d[i] = dtd[dn];
         // colour, block and slice loops run over the two slice indices in
         // the order of step3.f90: x: (k, j), y: (k, i), z: (j, i), i.e. the
         // higher-numbered axis outermost
         const int outer = std::max(d1, d2);  // slowest slice index
         const int inner = std::min(d1, d2);
         const int nblk_o = (dims[outer] + 2 + 1) / 2, nblk_i = (dims[inner] + 2 + 1) / 2;
-        for (int oo = 0; oo <= 1; ++oo)
-            for (int io = 0; io <= 1; ++io)
-                for (int ob = oo; ob <= nblk_o - 1; ob += 2)
-                    for (int ib = io; ib <= nblk_i - 1; ib += 2)
-                        for (int so = ob * 2; so <= std::min(ob * 2 + 1, dims[outer] + 1); ++so)
-                            for (int si = ib * 2; si <= std::min(ib * 2 + 1, dims[inner] + 1); ++si) {
-                                int P[3];
-                                P[outer] = so;
-                                P[inner] = si;
-                                auto cell = [&](int a, int de1, int de2, int* c) {
-                                    c[dn] = a;
-                                    c[d1] = P[d1] + de1;
-                                    c[d2] = P[d2] + de2;
-                                };
-                                for (int a = 1 - mbc; a <= len + mbc; ++a) {
-                                    int c[3];
-                                    cell(a, 0, 0, c);
-                                    for (int m = 1; m <= meqn; ++m) q1d[Q.at(m, a)] = QO(m, c[0], c[1], c[2]);
-                                }
-                                // aux1/aux2/aux3 = e1 offset -1/0/+1; third index = e2 offset -1..1
-                                for (int a = 1 - mbc; a <= len + mbc; ++a)
-                                    for (int l = -1; l <= 1; ++l)
-                                        for (int ma = 1; ma <= maux; ++ma) {
-                                            const int o = (ma - 1) + maux * ((a - (1 - mbc)) + n1 * (l + 1));
-                                            int c[3];
-                                            cell(a, -1, l, c); x1[o] = AX(ma, c[0], c[1], c[2]);
-                                            cell(a, 0, l, c); x2[o] = AX(ma, c[0], c[1], c[2]);
-                                            cell(a, 1, l, c); x3[o] = AX(ma, c[0], c[1], c[2]);
-                                        }
-                                const Aux3 A1{x1.data(), maux, 1 - mbc, n1}, A2{x2.data(), maux, 1 - mbc, n1},
-                                    A3{x3.data(), maux, 1 - mbc, n1};
-                                double cfl1d;
-                                flux3(ixyz, meqn, mwaves, mbc, len, q1d.data(), dtd1d.data(), dtd[d1],
-                                      dtd[d2], A1, A2, A3, method, mthlim, qadd.data(), fadd.data(),
-                                      gadd.data(), hadd.data(), &cfl1d, use_fwave != 0);
-                                cfl = std::fmax(cfl, cfl1d);
-                                const double te1 = dtd[d1], te2 = dtd[d2], tn = dtd[dn];
-                                for (int a = 1; a <= len; ++a)
-                                    for (int de2 = -1; de2 <= 1; ++de2)
-                                        for (int de1 = -1; de1 <= 1; ++de1)
-                                            for (int m = 1; m <= meqn; ++m) {
-                                                int c[3];
-                                                cell(a, de1, de2, c);
-                                                double& v = QN(m, c[0], c[1], c[2]);
-                                                if (de1 == 0 && de2 == 0) {
-                                                    v = v + qadd[Q.at(m, a)] -
-                                                        tn * (fadd[Q.at(m, a + 1)] - fadd[Q.at(m, a)]) -
-                                                        te1 * (Gv(gadd, m, 2, 0, a) - Gv(gadd, m, 1, 0, a)) -
-                                                        te2 * (Gv(hadd, m, 2, 0, a) - Gv(hadd, m, 1, 0, a));
-                                                    continue;
-                                                }
-                                                // e1 (G) term, then e2 (H) term
-                                                if (de1 == -1) v = v - te1 * Gv(gadd, m, 1, de2, a);
-                                                else if (de1 == 0) v = v - te1 * (Gv(gadd, m, 2, de2, a) - Gv(gadd, m, 1, de2, a));
-                                                else v = v + te1 * Gv(gadd, m, 2, de2, a);
-                                                if (de2 == -1) v = v - te2 * Gv(hadd, m, 1, de1, a);
-                                                else if (de2 == 0) v = v - te2 * (Gv(hadd, m, 2, de1, a) - Gv(hadd, m, 1, de1, a));
-                                                else v = v + te2 * Gv(hadd, m, 2, de1, a);
-                                            }
+        auto slice = [&](int so, int si, Work3& w, double& cfl) {
+            std::vector<double>& q1d = w.q1d;
+            std::vector<double>& qadd = w.qadd;
+            std::vector<double>& fadd = w.fadd;
+            std::vector<double>& gadd = w.gadd;
+            std::vector<double>& hadd = w.hadd;
+            int P[3];
+            P[outer] = so;
+            P[inner] = si;
+            auto cell = [&](int a, int de1, int de2, int* c) {
+                c[dn] = a;
+                c[d1] = P[d1] + de1;
+                c[d2] = P[d2] + de2;
+            };
+            for (int i = 0; i < n1; ++i) w.dtd1d[i] = dtd[dn];
+            for (int a = 1 - mbc; a <= len + mbc; ++a) {
+                int c[3];
+                cell(a, 0, 0, c);
+                for (int m = 1; m <= meqn; ++m) q1d[Q.at(m, a)] = QO(m, c[0], c[1], c[2]);
+            }
+            // aux1/aux2/aux3 = e1 offset -1/0/+1; third index = e2 offset -1..1
+            for (int a = 1 - mbc; a <= len + mbc; ++a)
+                for (int l = -1; l <= 1; ++l)
+                    for (int ma = 1; ma <= maux; ++ma) {
+                        const int o = (ma - 1) + maux * ((a - (1 - mbc)) + n1 * (l + 1));
+                        int c[3];
+                        cell(a, -1, l, c); w.x1[o] = AX(ma, c[0], c[1], c[2]);
+                        cell(a, 0, l, c); w.x2[o] = AX(ma, c[0], c[1], c[2]);
+                        cell(a, 1, l, c); w.x3[o] = AX(ma, c[0], c[1], c[2]);
+                    }
+            const Aux3 A1{w.x1.data(), maux, 1 - mbc, n1}, A2{w.x2.data(), maux, 1 - mbc, n1},
+                A3{w.x3.data(), maux, 1 - mbc, n1};
+            double cfl1d;
+            flux3(ixyz, meqn, mwaves, mbc, len, q1d.data(), w.dtd1d.data(), dtd[d1],
+                  dtd[d2], A1, A2, A3, method, mthlim, qadd.data(), fadd.data(),
+                  gadd.data(), hadd.data(), &cfl1d, use_fwave != 0);
+            cfl = std::fmax(cfl, cfl1d);
+            const double te1 = dtd[d1], te2 = dtd[d2], tn = dtd[dn];
+            for (int a = 1; a <= len; ++a)
+                for (int de2 = -1; de2 <= 1; ++de2)
+                    for (int de1 = -1; de1 <= 1; ++de1)
+                        for (int m = 1; m <= meqn; ++m) {
+                            int c[3];
+                            cell(a, de1, de2, c);
+                            double& v = QN(m, c[0], c[1], c[2]);
+                            if (de1 == 0 && de2 == 0) {
+                                v = v + qadd[Q.at(m, a)] -
+                                    tn * (fadd[Q.at(m, a + 1)] - fadd[Q.at(m, a)]) -
+                                    te1 * (Gv(gadd, m, 2, 0, a) - Gv(gadd, m, 1, 0, a)) -
+                                    te2 * (Gv(hadd, m, 2, 0, a) - Gv(hadd, m, 1, 0, a));
+                                continue;
                             }
+                            // e1 (G) term, then e2 (H) term
+                            if (de1 == -1) v = v - te1 * Gv(gadd, m, 1, de2, a);
+                            else if (de1 == 0) v = v - te1 * (Gv(gadd, m, 2, de2, a) - Gv(gadd, m, 1, de2, a));
+                            else v = v + te1 * Gv(gadd, m, 2, de2, a);
+                            if (de2 == -1) v = v - te2 * Gv(hadd, m, 1, de1, a);
+                            else if (de2 == 0) v = v - te2 * (Gv(hadd, m, 2, de1, a) - Gv(hadd, m, 1, de1, a));
+                            else v = v + te2 * Gv(hadd, m, 2, de1, a);
+                        }
+        };
+        auto block = [&](int ob, int ib, Work3& w, double& cfl) {
+            for (int so = ob * 2; so <= std::min(ob * 2 + 1, dims[outer] + 1); ++so)
+                for (int si = ib * 2; si <= std::min(ib * 2 + 1, dims[inner] + 1); ++si)
+                    slice(so, si, w, cfl);
+        };
+        if (g_threads > 1) {
+            // Timing variant: blocks of one colour are at least three slices
+            // apart, so they run in parallel as step3.f90:132-186 runs them;
+            // each cell still receives its contributions in the serial order.
+            const int nt = g_threads;
+            std::vector<Work3> ws;
+            for (int t = 0; t < nt; ++t) ws.emplace_back(meqn, maux, n1);
+            std::vector<double> cfls(nt, 0.0);
+            for (int oo = 0; oo <= 1; ++oo)
+                for (int io = 0; io <= 1; ++io) {
+                    const int no = (nblk_o - oo + 1) / 2, ni = (nblk_i - io + 1) / 2;
+                    parallel_items(no * ni, nt, [&](int k, int t) {
+                        block(oo + 2 * (k / ni), io + 2 * (k % ni), ws[t], cfls[t]);
+                    });
+                }
+            for (double c : cfls) cfl = std::fmax(cfl, c);
+        } else {
+            Work3 w(meqn, maux, n1);
+            for (int oo = 0; oo <= 1; ++oo)
+                for (int io = 0; io <= 1; ++io)
+                    for (int ob = oo; ob <= nblk_o - 1; ob += 2)
+                        for (int ib = io; ib <= nblk_i - 1; ib += 2) block(ob, ib, w, cfl);
+        }
     }
     *cfl_out = cfl;
     return 0;

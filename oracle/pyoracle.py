@@ -61,6 +61,8 @@ def _load(variant: str):
     if not os.path.exists(path):
         build()
     lib = ctypes.CDLL(path)
+    lib.orc_set_threads.argtypes = [ctypes.c_int]
+    lib.orc_set_threads.restype = ctypes.c_int
     lib.orc_set_solver.argtypes = [ctypes.c_int, _D, ctypes.c_int]
     lib.orc_set_solver.restype = ctypes.c_int
     lib.orc_set_source.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
