@@ -54,14 +54,10 @@ def traffic_per_launch(precision, cells):
     """DRAM bytes (read + write) per launch of the step kernel, scaled from
     the ncu capture summarised in profiles/ (bytes per cell-update at a size
     larger than L2); None when no capture is recorded."""
-    p = os.path.join(ROOT, "profiles", "dram_bytes_per_cell.txt")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        parts = line.split()
-        if len(parts) >= 2 and not line.startswith("#") and parts[0] == precision:
-            return float(parts[1]) * cells
-    return None
+    key = {"fp64_fma": "step2_char_kernel_fp64_fma", "fp64": "step2_kernel_fp64",
+           "fp32": "step2_char_kernel_fp32"}[precision]
+    bpc, _ = kernel_stats(key)
+    return bpc * cells if bpc is not None else None
 
 
 def load_peaks():
@@ -153,6 +149,20 @@ def whole_job_rate(updates_local, ms_local, world, device):
     return total / (ms_max * 1e-3), ms_max, total
 
 
+def host_cpu():
+    """The host's CPU model and logical core count (lscpu / os.cpu_count)."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
 def cpu_reference_sample(n, nsteps):
     """Time the CPU restatement (oracle, speed build) on nsteps whole n^2
     steps of the workload; returns (cell-updates/s, seconds, cores)."""
@@ -192,7 +202,7 @@ def run_reference_arm(args):
                    "step": f"one whole {n}^2 time step (bounded sample of a frame)"},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                          "sample": f"{args.steps} whole {n}^2 steps of the CPU restatement "
-                                   "(the reference's 2D step is serial)"},
+                                   "(the reference's 2D step is serial)", "host": host_cpu()},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -200,17 +210,93 @@ def run_reference_arm(args):
     return 0
 
 
-def other_configs(peaks):
+def kernel_stats(key):
+    """DRAM bytes and FP64 thread-operations per cell-update of one kernel
+    (one step), scaled from the ncu captures summarised in profiles/ (sizes
+    larger than L2); (None, None) when no capture is recorded."""
+    p = os.path.join(ROOT, "profiles", "dram_bytes_per_cell.txt")
+    if not os.path.exists(p):
+        return None, None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and not line.startswith("#") and parts[0] == key:
+            fp64 = float(parts[2]) if len(parts) >= 3 and parts[2] != "-" else None
+            return float(parts[1]), fp64
+    return None, None
+
+
+def roofline_entry(rate, alg_bytes, peaks, key=None, fp64_peak=None):
+    """Roofline of a side workload from its cell-update rate: algorithmic
+    bytes per cell x rate against the measured HBM copy bandwidth; the DRAM
+    traffic and FP64 operations per cell from the kernel's ncu capture when
+    one is recorded, and then the FP64 fraction against the probed FMA peak."""
+    achieved = rate * alg_bytes / 1e9
+    out = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": achieved / peaks["hbm_gbs"], "algorithmic_bytes_per_cell": alg_bytes,
+           "traffic_bytes_per_cell": None, "peak_source": peaks["source"]}
+    if key:
+        tb, fp64 = kernel_stats(key)
+        out["traffic_bytes_per_cell"] = tb
+        if fp64 is not None and fp64_peak:
+            # FP64 pipe: thread-instructions per second against the probe's
+            # (an FMA is one instruction and two flops)
+            out["fp64_inst_per_cell"] = fp64
+            out["fp64_tinst_per_s"] = rate * fp64 / 1e12
+            out["fp64_tinst_peak"] = fp64_peak / 2.0
+            out["fp64_frac"] = rate * fp64 / 1e12 / (fp64_peak / 2.0)
+            if out["fp64_frac"] > out["frac"]:
+                out["bound"] = "fp64"
+    return out
+
+
+def cpu_rate(make, steps, threads, dt):
+    """cell-updates/s of the CPU restatement (speed build, `threads` host
+    threads) over `steps` whole steps of one grid; returns (rate, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import OracleGrid
+    rd, solver, params, q0, aux = make()
+    g = OracleGrid(rd.clawdata, solver, params, variant="fast")
+    g.lib.orc_set_threads(threads)
+    try:
+        g.set_q(q0)
+        if aux is not None:
+            g.set_aux(aux)
+        cells = int(np.prod(rd.clawdata.num_cells))
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            g.step(dt)
+        sec = time.perf_counter() - t0
+    finally:
+        g.lib.orc_set_threads(1)
+    return cells * steps / sec, sec
+
+
+def other_configs(peaks, cpu=True):
     """The other workloads of the suite, measured once each after the
-    headline (device time from CUDA events inside the library): 1D acoustics
-    (800 cells, 10 frames to t=1), 3D heterogeneous acoustics (256^3, the
-    first frame t=0..0.1, FP64 reference order, FP64 contracted and FP32), the dimensionally
-    split steps (2D radial 4096^2 to t=0.03, Godunov and Strang; 3D 256^3
-    Godunov, first frame) and the batched 2D Euler ensemble (256 instances,
-    sides log-uniform in 128..1024, to t=0.25)."""
-    from classic_b200 import problems
+    headline (device time from CUDA events inside the library), each with
+    its roofline and a CPU baseline of the restatement on this host (a
+    bounded sample; one core, and all cores where the reference's path is
+    threaded -- its 3D step is OpenMP-parallel, its 1D and 2D steps serial):
+    1D acoustics (800 cells, 10 frames to t=1), 2D radial acoustics at
+    1024^2 (first frame), 3D heterogeneous acoustics (256^3 and 512^3, the
+    first frame t=0..0.1; FP64 reference order, contracted FP64, FP32), the
+    dimensionally split steps (2D radial 4096^2 to t=0.03, Godunov and
+    Strang; 3D 256^3 Godunov, first frame) and the batched 2D Euler ensemble
+    (256 instances, sides log-uniform in 128..1024, to t=0.25)."""
+    from classic_b200 import _lib, problems
     from classic_b200.solver import BatchSolver, Solver
+    import ctypes
     out = {}
+    nproc = os.cpu_count() or 1
+    fp64_peak = None
+    try:
+        tf, msb = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        if _lib.load().claw_probe_fp64(ctypes.byref(tf), ctypes.byref(msb)) == 0:
+            fp64_peak = tf.value
+            out["fp64_fma_probe"] = {"tflops": tf.value, "ms": msb.value,
+                                     "what": "independent FP64 FMA chains, 2 flops per FMA"}
+    except Exception as e:
+        out["fp64_fma_probe"] = {"error": str(e)}
     try:
         rd, solver, params, q0, _ = problems.acoustics_1d_config()
         s = Solver(rd.clawdata, solver, params)
@@ -222,28 +308,91 @@ def other_configs(peaks):
             steps += st["steps_taken"]
             ms += st["device_ms"]
         s.close()
-        out["acoustics_1d_800"] = {"cell_updates_per_s": 800 * steps / (ms * 1e-3), "steps": steps,
-                                   "device_ms": ms, "note": "one CTA runs the whole claw1 loop per frame"}
+        rate = 800 * steps / (ms * 1e-3)
+        e = {"cell_updates_per_s": rate, "steps": steps, "device_ms": ms,
+             "note": "one CTA runs the whole claw1 loop per frame (latency-bound, one SM)",
+             "roofline": roofline_entry(rate, 32, peaks)}
+        if cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            from pyoracle import OracleGrid
+            o = OracleGrid(rd.clawdata, solver, params, variant="fast")
+            o.set_q(q0)
+            t0 = time.perf_counter()
+            t, dt, osteps = 0.0, float(rd.clawdata.dt_initial), 0
+            for _ in range(10):
+                info, so = o.advance(t, t + 0.1, dt)
+                t, dt = so["t_reached"], so["dt_next"]
+                osteps += so["steps_taken"]
+            sec = time.perf_counter() - t0
+            e["cpu_baseline"] = {"value": 800 * osteps / sec, "unit": "cell-updates/s", "cores": 1,
+                                 "kind": "port", "sample": f"the whole run ({osteps} steps, {sec:.2f} s)"}
+        out["acoustics_1d_800"] = e
     except Exception as e:  # a failed side measurement must not hide the headline
         out["acoustics_1d_800"] = {"error": str(e)}
+    # 2D radial acoustics at 1024^2: the first frame (t = 0 .. 0.03)
     for prec in ("fp64", "fp64_fma", "fp32"):
-        key = f"hetero_acoustics_3d_256_{prec}"
+        key = f"radial_2d_1024_{prec}"
         try:
-            rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=256)
+            rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=1024)
             s = Solver(rd.clawdata, solver, params, precision=prec)
             s.set_q(q0)
-            s.set_aux(aux)
-            info, st = s.advance(0.0, 0.1, 0.01)
+            s.advance(0.0, 0.03, 0.01)  # warm-up frame
+            s.set_q(q0)
+            info, st = s.advance(0.0, 0.03, 0.01)
             s.close()
-            n3 = 256 ** 3
-            upd = n3 * (st["steps_taken"] + st["steps_rejected"])
+            ex = st["steps_taken"] + st["steps_rejected"]
+            rate = 1024 ** 2 * ex / (st["device_ms"] * 1e-3)
             es = 4 if prec == "fp32" else 8
-            rate = upd / (st["device_ms"] * 1e-3)
-            out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
-                        "device_ms": st["device_ms"],
-                        "hbm_frac_algorithmic": rate * 10 * es / 1e9 / peaks["hbm_gbs"]}
+            kern = {"fp64": "step2_kernel_fp64", "fp64_fma": "step2_char_kernel_fp64_fma",
+                    "fp32": "step2_char_kernel_fp32"}[prec]
+            e = {"cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
+                 "l2": "q (25 MB per FP64 buffer) fits in L2: the rate is not HBM-bound at this size",
+                 "roofline": roofline_entry(rate, 6 * es, peaks, kern, fp64_peak)}
+            if cpu and prec == "fp64":
+                mk = lambda: problems.radial_acoustics_2d(n=1024)[:4] + (None,)
+                r1, s1 = cpu_rate(mk, 5, 1, 0.0008)
+                rn, sn = cpu_rate(mk, 10, nproc, 0.0008)
+                e["cpu_baseline"] = {"value": r1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                                     "sample": f"5 whole 1024^2 steps from the initial data ({s1:.1f} s); "
+                                               "the reference's 2D step is serial",
+                                     "threaded": {"value": rn, "cores": nproc,
+                                                  "sample": f"10 steps ({sn:.1f} s), every third slice in parallel"}}
+            out[key] = e
         except Exception as e:
             out[key] = {"error": str(e)}
+    for n in (256, 512):
+        for prec in ("fp64", "fp64_fma", "fp32"):
+            key = f"hetero_acoustics_3d_{n}_{prec}"
+            try:
+                rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=n)
+                s = Solver(rd.clawdata, solver, params, precision=prec)
+                s.set_q(q0)
+                s.set_aux(aux)
+                info, st = s.advance(0.0, 0.1, 0.01)
+                s.close()
+                n3 = n ** 3
+                upd = n3 * (st["steps_taken"] + st["steps_rejected"])
+                es = 4 if prec == "fp32" else 8
+                rate = upd / (st["device_ms"] * 1e-3)
+                kern = {"fp64": "sweep3p_fp64", "fp64_fma": "sweep3f_fp64_fma",
+                        "fp32": "sweep3f_fp32"}[prec]
+                e = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
+                     "device_ms": st["device_ms"],
+                     "roofline": roofline_entry(rate, 10 * es, peaks, kern, fp64_peak)}
+                if cpu and prec == "fp64" and n == 256:
+                    mk_s = lambda: problems.heterogeneous_acoustics_3d(n=96)
+                    mk_n = lambda: problems.heterogeneous_acoustics_3d(n=256)
+                    r1, s1 = cpu_rate(mk_s, 1, 1, 0.002)
+                    rn, sn = cpu_rate(mk_n, 1, nproc, 0.002)
+                    e["cpu_baseline"] = {
+                        "value": rn, "unit": "cell-updates/s", "cores": nproc, "kind": "port",
+                        "sample": f"1 whole 256^3 step on {nproc} threads ({sn:.1f} s): the reference's "
+                                  "step3 is OpenMP-parallel over 2x2 colour blocks, restated the same way",
+                        "one_core": {"value": r1, "cores": 1,
+                                     "sample": f"1 whole step of the same problem at 96^3 ({s1:.1f} s)"}}
+                out[key] = e
+            except Exception as e:
+                out[key] = {"error": str(e)}
     # dimensionally split steps (dimsp2 / dimsp3), FP64 reference order
     for key, dim, split in (("radial_2d_4096_godunov_split_fp64", 2, "godunov"),
                             ("radial_2d_4096_strang_split_fp64", 2, "strang"),
@@ -265,7 +414,7 @@ def other_configs(peaks):
             rate = cells * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
-                        "hbm_frac_algorithmic": rate * nbytes / 1e9 / peaks["hbm_gbs"]}
+                        "roofline": roofline_entry(rate, nbytes, peaks)}
         except Exception as e:
             out[key] = {"error": str(e)}
     try:
@@ -279,12 +428,26 @@ def other_configs(peaks):
         b.close()
         upd = sum(nn * nn * (x["steps_taken"] + x["steps_rejected"]) for nn, x in zip(sizes, st))
         ms = st[0]["device_ms"]
-        out["euler_batch_256"] = {"cell_updates_per_s": upd / (ms * 1e-3), "cell_updates": upd,
-                                  "device_ms": ms, "launches": st[0]["launches"],
-                                  "steps_min_max": [min(x["steps_taken"] for x in st),
-                                                    max(x["steps_taken"] for x in st)],
-                                  "autotuned_shape": {"min_rows": shape["min_rows"],
-                                                      "ctas_per_sm": shape["ctas_per_sm"]}}
+        rate = upd / (ms * 1e-3)
+        e = {"cell_updates_per_s": rate, "cell_updates": upd,
+             "device_ms": ms, "launches": st[0]["launches"],
+             "steps_min_max": [min(x["steps_taken"] for x in st),
+                               max(x["steps_taken"] for x in st)],
+             "autotuned_shape": {"min_rows": shape["min_rows"],
+                                 "ctas_per_sm": shape["ctas_per_sm"]},
+             "roofline": roofline_entry(rate, 64, peaks, "step2_batch_kernel_euler", fp64_peak)}
+        if cpu:
+            nn = 512
+            mk = lambda: problems.euler_quadrants(n=nn, seed=7)[:4] + (None,)
+            r1, s1 = cpu_rate(mk, 20, 1, 2e-4)
+            rn, sn = cpu_rate(mk, 40, nproc, 2e-4)
+            e["cpu_baseline"] = {"value": r1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                                 "sample": f"20 whole steps of one 512^2 instance from its initial data "
+                                           f"({s1:.1f} s); the reference advances one grid per claw2 "
+                                           "call, serially",
+                                 "threaded": {"value": rn, "cores": nproc,
+                                              "sample": f"40 steps ({sn:.1f} s), every third slice in parallel"}}
+        out["euler_batch_256"] = e
     except Exception as e:
         out["euler_batch_256"] = {"error": str(e)}
     return out
@@ -442,14 +605,21 @@ def main():
 
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
-        configs = other_configs(peaks)
+        configs = other_configs(peaks, cpu=args.cpu_steps > 0)
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_steps > 0:
         rate, sec, cores = cpu_reference_sample(n, args.cpu_steps)
+        nproc = os.cpu_count() or 1
+        mk = lambda: problems.radial_acoustics_2d(n=n)[:4] + (None,)
+        rn, sn = cpu_rate(mk, max(1, args.cpu_steps), nproc, 0.9 * (2.0 / n) / 2.0)
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-               "sample": f"{args.cpu_steps} whole {n}^2 steps of the CPU restatement "
-                         f"({sec:.1f} s)"}
+               "sample": f"{args.cpu_steps} whole {n}^2 steps of the CPU restatement from the "
+                         f"initial data ({sec:.1f} s); the reference's 2D step is serial",
+               "host": host_cpu(),
+               "threaded": {"value": rn, "cores": nproc,
+                            "sample": f"{max(1, args.cpu_steps)} whole steps ({sn:.1f} s), every "
+                                      "third slice in parallel (not the reference's scheme)"}}
 
     if rank == 0:
         line = {

@@ -108,6 +108,7 @@ SIGNATURES = {
                                      ctypes.POINTER(ctypes.c_longlong)]),
     "claw_launch_count": (ctypes.c_longlong, [_P]),
     "claw_debug_fault": (ctypes.c_int, [_P, ctypes.c_longlong, ctypes.c_int]),
+    "claw_set_steps_max": (ctypes.c_int, [_P, ctypes.c_int]),
     "claw_totals": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "claw_step2d_noalloc": (ctypes.c_int, [ctypes.POINTER(ClawConfig), _P, _P, ctypes.c_longlong,
                                            _P, ctypes.c_longlong, ctypes.c_double, _D, _P]),

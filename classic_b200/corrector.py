@@ -372,11 +372,14 @@ def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=
 
 
 def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25, tol=1e-10,
-                  cfl_desired=0.9, cfl_max=1.0, alpha=1.0, interval=1):
-    """The corrected coarse run of one instance (claw2's dt control on the
-    host, alpha times the corrector after every `interval` accepted steps,
-    fed the window's start state and increment).  Returns (q, steps,
-    corrected tile fraction, device seconds)."""
+                  alpha=1.0, interval=1):
+    """The corrected coarse run of one instance.  The library's claw2
+    (claw_advance: device-side dt control with its rejections, dt_max and
+    steps_max rules) advances `interval` accepted steps per call (nv(1) =
+    interval; info 11 ends a window), then alpha times the corrector is
+    applied on the device, fed the window's start state and increment: one
+    host round trip per window.  Returns (q, steps, corrected tile
+    fraction, wall seconds of the run with the device synchronised)."""
     if alpha != 1.0:
         v = norm.values.copy()
         v[12:16] = v[12:16] / max(alpha, 1e-30)
@@ -386,30 +389,26 @@ def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25,
     rd, solver, params, q0, _ = problems.euler_quadrants(n=n, seed=seed, gamma=gamma)
     s = Solver(rd.clawdata, solver, params)
     s.set_q(q0)
+    s.set_steps_max(interval)
     nd = norm.device()
     st = _stream()
     x = torch.empty((1, n, n, 16), dtype=torch.bfloat16, device="cuda")
-    qold = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
     qwin = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
     flags = torch.empty(((n + 15) // 16) ** 2, dtype=torch.int32, device="cuda")
     good = torch.zeros((), dtype=torch.int64, device="cuda")
     t, dt, steps, tiles = 0.0, float(rd.clawdata.dt_initial), 0, 0
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    e0.record()
+    w0 = time.perf_counter()
     while t < tfinal:
-        dt = min(dt, tfinal - t)
         qc, ld, fs = q_view(s)
-        qold.copy_(qc)
-        if steps % interval == 0:
-            qwin.copy_(qc)
-        cfl = s.step(dt)
-        if cfl > cfl_max:
-            qn, _, _ = q_view(s)
-            qn.copy_(qold)
-            dt = dt * cfl_desired / cfl
-            continue
-        if steps % interval == interval - 1:
+        qwin.copy_(qc)
+        torch.cuda.current_stream().synchronize()  # the step stream does not wait on torch's
+        info, sa = s.advance(t, tfinal, dt)
+        if info not in (0, 11):
+            raise RuntimeError(f"corrected run: claw_advance info {info}")
+        t, dt = sa["t_reached"], sa["dt_next"]
+        steps += sa["steps_taken"]
+        if sa["steps_taken"] == interval:
             qs, ld, fs = q_view(s)
             qsc = qs.contiguous() if ld != n else qs
             check(lib.nn_features(_p(qwin), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(x), st),
@@ -419,26 +418,28 @@ def corrected_run(net: ConvNet, norm: Norm, seed, n=256, gamma=1.4, tfinal=0.25,
                                           _p(flags), st), "nn_apply_correction")
             good += flags.sum()
             tiles += flags.numel()
-        t += dt
-        dt = dt * cfl_desired / cfl if cfl > 0 else dt
-        steps += 1
-    e1.record()
     torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
     q = s.get_q()
     s.close()
-    return q, steps, good.item() / max(tiles, 1), e0.elapsed_time(e1) / 1e3
+    return q, steps, good.item() / max(tiles, 1), wall
 
 
-def plain_run(seed, n, gamma=1.4, tfinal=0.25):
-    """The plain FP64 run of one instance (claw2's device-side dt control);
-    returns (q, steps, device seconds)."""
+def plain_run(seed, n, gamma=1.4, tfinal=0.25, precision="fp64"):
+    """The plain run of one instance (claw2's device-side dt control);
+    returns (q, steps, wall seconds of the advance with the device
+    synchronised, as corrected_run measures)."""
+    torch = _torch()
     rd, solver, params, q0, _ = problems.euler_quadrants(n=n, seed=seed, gamma=gamma)
-    s = Solver(rd.clawdata, solver, params)
+    s = Solver(rd.clawdata, solver, params, precision=precision)
     s.set_q(q0)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
     info, st = s.advance(0.0, tfinal, float(rd.clawdata.dt_initial))
+    wall = time.perf_counter() - w0
     q = s.get_q()
     s.close()
-    return q, st["steps_taken"], st["device_ms"] / 1e3
+    return q, st["steps_taken"], wall
 
 
 def block_average(q, r):

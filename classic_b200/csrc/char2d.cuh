@@ -30,24 +30,6 @@ struct CharAcoustics2D {
     real cc, zz, hz;  // c, Z, 1/(2Z)
 };
 
-__device__ __forceinline__ double rcp_newton(double a) {
-    // reciprocal: hardware estimate (~23 bits) refined by two Newton-Raphson
-    // steps y <- y + y(1 - a y), each doubling the correct bits
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
-    double e = fma(-a, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-a, y, 1.0);
-    y = fma(y, e, y);
-    return y;
-}
-__device__ __forceinline__ float rcp_newton(float a) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
-    const float e = fmaf(-a, y, 1.0f);
-    return fmaf(y, e, y);
-}
-
 // x with the sign of s flipped in (x * sign(s)), and copysign, by bit operations.
 __device__ __forceinline__ double sign_times(double x, double s) {
     return __longlong_as_double(__double_as_longlong(x) ^
@@ -65,9 +47,25 @@ __device__ __forceinline__ float sign_times(float x, float s) {
 //   MC       phi a = sign(a) max(0, min(2A, 2N, (A+N)/2))
 // (multiply phi's arguments by a, reversing min/max when a < 0).  a == 0 gives
 // 0, as the reference skips a zero wave.  Other limiters use the ratio.
+// MC in FP64 by compare-and-select on magnitudes.  When a and n share a
+// sign, phi a = sign(a) 2 min(|a|, |n|, (|a|+|n|)/4); otherwise 0.  Same value
+// as the min/max form below (every candidate is formed by the same
+// operations), but no fmin/fmax: their NaN rules cost extra instructions in
+// FP64, and the select picks one of two registers.
+__device__ __forceinline__ double mc_strength(double a, double n) {
+    const double mn = fabs(a) < fabs(n) ? a : n;  // |mn| = min(|a|, |n|)
+    const double q = 0.25 * (fabs(a) + fabs(n));
+    const double r = q < fabs(mn) ? q : mn;       // |r| = the smaller of the two
+    const int ah = __double2hiint(a), nh = __double2hiint(n);
+    // +-2 with the sign of a when the signs agree, else +0 (n = +-0 gives r = 0)
+    const int s2 = (ah ^ nh) >= 0 ? ((ah & (int)0x80000000u) | 0x40000000) : 0;
+    return fabs(r) * __hiloint2double(s2, 0);
+}
+
 template <typename real, int LIM>
 __device__ __forceinline__ real limited_strength(real a, real n, int lim_rt) {
     const int lim = LIM >= 0 ? LIM : lim_rt;
+    if constexpr (LIM == 4 && sizeof(real) == 8) return mc_strength(a, n);
     if (LIM == 1 || LIM == 2 || LIM == 4) {
         const real A = fabs(a), N = sign_times(n, a);
         real m;
@@ -136,6 +134,12 @@ struct ColSrc {
 //                   ring box, read from global memory
 enum { CHAR_BC_EXTRAP = 0, CHAR_BC_WALLS = 1, CHAR_BC_PERX = 2 };
 
+// Two adjacent values of one field (columns c0, c0+1) as one shared-memory
+// load; the pair starts on a 16-byte (FP64) / 8-byte (FP32) boundary.
+template <typename real> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
 template <typename real, int LIM, int BCM>
 __global__ void __launch_bounds__(32 * WARPS2D, CLAW_CHAR_MINB)
 step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
@@ -143,6 +147,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     constexpr bool WALLS = BCM != CHAR_BC_EXTRAP;
     constexpr int kUnroll = CLAW_CHAR_UNROLL;
     using R = CharRing<real>;
+    using P2 = typename Pair<real>::type;
     constexpr int W = R::W;
     constexpr unsigned FULL = 0xffffffffu;
     ClawCtl* ctl = A.ctl;
@@ -198,20 +203,9 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
         const int x0 = b - R::XQ;
         const int rfirst = r0 - 2, rlast = r0 + nr + 1;
         const int nrows = rlast - rfirst + 1;
-        auto colsrc = [&](int col) -> ColSrc {
-            ColSrc cs;
-            cs.src = bc_map(col, mx, A.bc[0], A.bc[1], cs.neg);
-            cs.glob = (cs.src - x0) < 0 || (cs.src - x0) >= W;
-            cs.idx = cs.glob ? 0 : cs.src - x0;
-            return cs;
-        };
-        const ColSrc sM = colsrc(c0 - 1), s0 = colsrc(c0), s1 = colsrc(c1);
-        const bool any_global = PX && __any_sync(FULL, sM.glob || s0.glob || s1.glob);
-        const bool out_lane = lane >= 1 && lane <= 30;
-        const bool out0 = out_lane && c0 < mx, out1 = out_lane && c1 < mx;
+        const int skip1 = strip == 0 ? *(volatile const int*)&ctl->skip_row : 0;  // test hook
 
         auto seq_of = [&](int r) -> uint32_t { return seq_base + (uint32_t)(r - rfirst); };
-        const int skip1 = strip == 0 ? *(volatile const int*)&ctl->skip_row : 0;  // test hook
         auto issue = [&](int r) {
             if (skip1 != 0 && r == skip1 - 1) return;
             const uint32_t sq = seq_of(r);
@@ -230,159 +224,215 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
             const uint32_t sq = seq_of(r);
             return mbar_wait_bounded(&bars[sq & (RING - 1)], (sq >> RING_LOG) & 1u, wait_ns);
         };
-        // field m of column cs at row r (boundary conditions applied)
-        auto fetch = [&](const real* sq, int sr, bool nyneg, const ColSrc& cs, int m) -> real {
-            real v = sq[m * W + cs.idx];
-            if constexpr (PX) {
-                if (any_global && cs.glob) v = qold[m * A.fstride + (long long)sr * A.ld + cs.src];
-            }
-            if constexpr (WALLS) {
-                if (m == 1 && cs.neg) v = -v;
-                if (m == 2 && nyneg) v = -v;
-            }
-            return v;
-        };
         auto row_ptr = [&](int r) -> const real* {
             return reinterpret_cast<const real*>(ring + (int)(seq_of(r) & (RING - 1)) * R::SLOT);
         };
+        const bool out_lane = lane >= 1 && lane <= 30;
 
-        // carried per column k = 0, 1
-        real q2p[2][3] = {};          // x-part of (c_k, t) awaiting row t+1's transfer
-        real axp[2] = {}, axv[2] = {};  // x-slice t-1 -> row t (p, v)
-        real a1y[2] = {}, a2y[2] = {};  // y-interface t strengths
-        real a2y_lo[2] = {}, A2y_lo[2] = {}, Fpy_lo[2] = {}, Fvy_lo[2] = {};  // y-interface t-1
-        int last_issued = rfirst + (nrows < RING ? nrows : RING) - 1;
-        int fail_row = rlast + 1;
+        // The march over the rows of one work item.  INT: every column of the
+        // strip (b-3 .. b+61) is interior, so a lane's columns sit at ring
+        // index 2+2*lane (+1) with no x boundary condition: pairs of values
+        // load and store as one vector access.  Otherwise the columns go
+        // through the boundary maps (edge strips).
+        auto march = [&](auto int_tag) {
+            constexpr bool INT = decltype(int_tag)::value;
+            auto colsrc = [&](int col) -> ColSrc {
+                ColSrc cs;
+                cs.src = bc_map(col, mx, A.bc[0], A.bc[1], cs.neg);
+                cs.glob = (cs.src - x0) < 0 || (cs.src - x0) >= W;
+                cs.idx = cs.glob ? 0 : cs.src - x0;
+                return cs;
+            };
+            const ColSrc sM = colsrc(c0 - 1), s0 = colsrc(c0), s1 = colsrc(c1);
+            const bool any_global = !INT && PX && __any_sync(FULL, sM.glob || s0.glob || s1.glob);
+            const bool out0 = out_lane && (INT || c0 < mx), out1 = out_lane && (INT || c1 < mx);
+            const int ib = 2 + 2 * lane;  // ring index of c0 in an interior strip
+            // field m of column cs at row r (boundary conditions applied)
+            auto fetch = [&](const real* sq, int sr, bool nyneg, const ColSrc& cs, int m) -> real {
+                real v = sq[m * W + cs.idx];
+                if constexpr (PX && !INT) {
+                    if (any_global && cs.glob) v = qold[m * A.fstride + (long long)sr * A.ld + cs.src];
+                }
+                if constexpr (WALLS) {
+                    if (!INT && m == 1 && cs.neg) v = -v;
+                    if (m == 2 && nyneg) v = -v;
+                }
+                return v;
+            };
+            // fields m of columns c0, c1 at row r
+            auto fetch2 = [&](const real* sq, int sr, bool nyneg, int m, real& v0, real& v1) {
+                if constexpr (INT) {
+                    const P2 v = *reinterpret_cast<const P2*>(sq + m * W + ib);
+                    v0 = v.x;
+                    v1 = v.y;
+                    if constexpr (WALLS) {
+                        if (m == 2 && nyneg) { v0 = -v0; v1 = -v1; }
+                    }
+                } else {
+                    v0 = fetch(sq, sr, nyneg, s0, m);
+                    v1 = fetch(sq, sr, nyneg, s1, m);
+                }
+            };
+            auto fetchM = [&](const real* sq, int sr, bool nyneg, int m) -> real {
+                if constexpr (INT) return sq[m * W + ib - 1];
+                else return fetch(sq, sr, nyneg, sM, m);
+            };
 
-        if (!wait_row(rfirst) || !wait_row(rfirst + 1)) { failed = true; fail_row = rfirst; }
-        if (!failed) {
-            bool ng0, ng1;
-            const int sr0 = bc_map(rfirst, my, A.bc[2], A.bc[3], ng0);
-            const int sr1 = bc_map(rfirst + 1, my, A.bc[2], A.bc[3], ng1);
-            const real* q0p = row_ptr(rfirst);
-            const real* q1p = row_ptr(rfirst + 1);
+            // carried per column k = 0, 1
+            real q2p[2][3] = {};            // x-part of (c_k, t) awaiting row t+1's transfer
+            real axp[2] = {}, axv[2] = {};  // x-slice t-1 -> row t (p, v)
+            real a1y[2] = {}, a2y[2] = {};  // y-interface t strengths
+            real a2y_lo[2] = {}, A2y_lo[2] = {}, Fpy_lo[2] = {}, Fvy_lo[2] = {};  // y-interface t-1
+            real pc[2] = {}, vc[2] = {};    // p, v of row t (row t+1 of the previous trip)
+            int last_issued = rfirst + (nrows < RING ? nrows : RING) - 1;
+            int fail_row = rlast + 1;
+
+            if (!wait_row(rfirst) || !wait_row(rfirst + 1)) { failed = true; fail_row = rfirst; }
+            if (!failed) {
+                bool ng0, ng1;
+                const int sr0 = bc_map(rfirst, my, A.bc[2], A.bc[3], ng0);
+                const int sr1 = bc_map(rfirst + 1, my, A.bc[2], A.bc[3], ng1);
+                const real* q0p = row_ptr(rfirst);
+                const real* q1p = row_ptr(rfirst + 1);
+                real p0[2], v0[2];
+                fetch2(q0p, sr0, ng0, 0, p0[0], p0[1]);
+                fetch2(q0p, sr0, ng0, 2, v0[0], v0[1]);
+                fetch2(q1p, sr1, ng1, 0, pc[0], pc[1]);
+                fetch2(q1p, sr1, ng1, 2, vc[0], vc[1]);
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const ColSrc& cs = k ? s1 : s0;
-                const real dp = fetch(q1p, sr1, ng1, cs, 0) - fetch(q0p, sr0, ng0, cs, 0);
-                const real dv = fetch(q1p, sr1, ng1, cs, 2) - fetch(q0p, sr0, ng0, cs, 2);
-                a1y[k] = (Z * dv - dp) * h;
-                a2y[k] = (Z * dv + dp) * h;
+                for (int k = 0; k < 2; ++k) {
+                    const real dp = pc[k] - p0[k];
+                    const real dv = vc[k] - v0[k];
+                    a1y[k] = (Z * dv - dp) * h;
+                    a2y[k] = (Z * dv + dp) * h;
+                }
             }
-        }
 
-        // two rows per trip: the carried state rotates by renaming, not copies
+            // two rows per trip: the carried state rotates by renaming, not copies
 #pragma unroll kUnroll
-        for (int t = r0 - 1; t <= r0 + nr && !failed; ++t) {
-            if (!wait_row(t + 1)) { failed = true; fail_row = t + 1; break; }
-            bool ngt, ngn;
-            const int srt = bc_map(t, my, A.bc[2], A.bc[3], ngt);
-            const int srn = bc_map(t + 1, my, A.bc[2], A.bc[3], ngn);
-            const real* qt = row_ptr(t);
-            const real* qn = row_ptr(t + 1);
-            // row t: p, u at columns c0-1, c0, c1; v at c0, c1.  row t+1: p, v.
-            const real pM = fetch(qt, srt, ngt, sM, 0), uM = fetch(qt, srt, ngt, sM, 1);
-            real p[2], u[2], v[2], pn[2], vn[2];
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const ColSrc& cs = k ? s1 : s0;
-                p[k] = fetch(qt, srt, ngt, cs, 0);
-                u[k] = fetch(qt, srt, ngt, cs, 1);
-                v[k] = fetch(qt, srt, ngt, cs, 2);
-                pn[k] = fetch(qn, srn, ngn, cs, 0);
-                vn[k] = fetch(qn, srn, ngn, cs, 2);
-            }
+            for (int t = r0 - 1; t <= r0 + nr && !failed; ++t) {
+                if (!wait_row(t + 1)) { failed = true; fail_row = t + 1; break; }
+                bool ngt = false, ngn = false;
+                int srt = 0, srn = 0;
+                if constexpr (WALLS || PX) {
+                    srt = bc_map(t, my, A.bc[2], A.bc[3], ngt);
+                    srn = bc_map(t + 1, my, A.bc[2], A.bc[3], ngn);
+                }
+                const real* qt = row_ptr(t);
+                const real* qn = row_ptr(t + 1);
+                // row t: p, u at columns c0-1, c0, c1 (p carried); v carried.
+                // row t+1: p, v.
+                const real pM = fetchM(qt, srt, ngt, 0), uM = fetchM(qt, srt, ngt, 1);
+                real p[2] = {pc[0], pc[1]}, v[2] = {vc[0], vc[1]}, u[2], pn[2], vn[2];
+                fetch2(qt, srt, ngt, 1, u[0], u[1]);
+                fetch2(qn, srn, ngn, 0, pn[0], pn[1]);
+                fetch2(qn, srn, ngn, 2, vn[0], vn[1]);
 
-            // ---- x-slice t: interfaces I0 = (c0-1 | c0) and I1 = (c0 | c1) ----
-            const real a1_0 = (Z * (u[0] - uM) - (p[0] - pM)) * h;
-            const real a2_0 = (Z * (u[0] - uM) + (p[0] - pM)) * h;
-            const real a1_1 = (Z * (u[1] - u[0]) - (p[1] - p[0])) * h;
-            const real a2_1 = (Z * (u[1] - u[0]) + (p[1] - p[0])) * h;
-            const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
-            const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
-            // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
-            const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
-            const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim);
-            const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
-            const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim);
-            const real Fp0 = fxp * (l2_0 - l1_0), Fu0 = fxu * (l1_0 + l2_0);
-            const real Fp1 = fxp * (l2_1 - l1_1), Fu1 = fxu * (l1_1 + l2_1);
-            const real A1_0 = fma(cZ, a1_0, real(2) * Fp0), A2_0 = fma(cZ, a2_0, real(-2) * Fp0);
-            const real A1_1 = fma(cZ, a1_1, real(2) * Fp1), A2_1 = fma(cZ, a2_1, real(-2) * Fp1);
-            const real FpR = __shfl_down_sync(FULL, Fp0, 1), FuR = __shfl_down_sync(FULL, Fu0, 1);
-            const real A1R = __shfl_down_sync(FULL, A1_0, 1);
-            // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0
-            real q3[2][3];
-            {
-                const real S0 = A1_1 + A2_0, S1 = A1R + A2_1;
-                const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
-                const real n00 = (p[0] + axp[0]) - qpx * (a2_0 + a1_1) - dtdx * (Fp1 - Fp0) + real(2) * gS0;
-                const real n01 = u[0] + qux * (a1_1 - a2_0) - dtdx * (Fu1 - Fu0);
-                const real n02 = v[0] + axv[0];
-                const real n10 = (p[1] + axp[1]) - qpx * (a2_1 + a1_R) - dtdx * (FpR - Fp1) + real(2) * gS1;
-                const real n11 = u[1] + qux * (a1_R - a2_1) - dtdx * (FuR - Fu1);
-                const real n12 = v[1] + axv[1];
-                q3[0][0] = q2p[0][0] - gS0; q3[0][1] = q2p[0][1]; q3[0][2] = q2p[0][2] + dS0;
-                q3[1][0] = q2p[1][0] - gS1; q3[1][1] = q2p[1][1]; q3[1][2] = q2p[1][2] + dS1;
-                q2p[0][0] = n00; q2p[0][1] = n01; q2p[0][2] = n02;
-                q2p[1][0] = n10; q2p[1][1] = n11; q2p[1][2] = n12;
-                axp[0] = -gS0; axv[0] = -dS0;
-                axp[1] = -gS1; axv[1] = -dS1;
-            }
+                // ---- x-slice t: interfaces I0 = (c0-1 | c0) and I1 = (c0 | c1) ----
+                const real a1_0 = (Z * (u[0] - uM) - (p[0] - pM)) * h;
+                const real a2_0 = (Z * (u[0] - uM) + (p[0] - pM)) * h;
+                const real a1_1 = (Z * (u[1] - u[0]) - (p[1] - p[0])) * h;
+                const real a2_1 = (Z * (u[1] - u[0]) + (p[1] - p[0])) * h;
+                const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
+                const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
+                // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
+                const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
+                const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim);
+                const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
+                const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim);
+                const real Fp0 = fxp * (l2_0 - l1_0), Fu0 = fxu * (l1_0 + l2_0);
+                const real Fp1 = fxp * (l2_1 - l1_1), Fu1 = fxu * (l1_1 + l2_1);
+                const real A1_0 = fma(cZ, a1_0, real(2) * Fp0), A2_0 = fma(cZ, a2_0, real(-2) * Fp0);
+                const real A1_1 = fma(cZ, a1_1, real(2) * Fp1), A2_1 = fma(cZ, a2_1, real(-2) * Fp1);
+                const real FpR = __shfl_down_sync(FULL, Fp0, 1), FuR = __shfl_down_sync(FULL, Fu0, 1);
+                const real A1R = __shfl_down_sync(FULL, A1_0, 1);
+                // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0
+                real q3[2][3];
+                {
+                    const real S0 = A1_1 + A2_0, S1 = A1R + A2_1;
+                    const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
+                    const real n00 = (p[0] + axp[0]) - qpx * (a2_0 + a1_1) - dtdx * (Fp1 - Fp0) + real(2) * gS0;
+                    const real n01 = u[0] + qux * (a1_1 - a2_0) - dtdx * (Fu1 - Fu0);
+                    const real n02 = v[0] + axv[0];
+                    const real n10 = (p[1] + axp[1]) - qpx * (a2_1 + a1_R) - dtdx * (FpR - Fp1) + real(2) * gS1;
+                    const real n11 = u[1] + qux * (a1_R - a2_1) - dtdx * (FuR - Fu1);
+                    const real n12 = v[1] + axv[1];
+                    q3[0][0] = q2p[0][0] - gS0; q3[0][1] = q2p[0][1]; q3[0][2] = q2p[0][2] + dS0;
+                    q3[1][0] = q2p[1][0] - gS1; q3[1][1] = q2p[1][1]; q3[1][2] = q2p[1][2] + dS1;
+                    q2p[0][0] = n00; q2p[0][1] = n01; q2p[0][2] = n02;
+                    q2p[1][0] = n10; q2p[1][1] = n11; q2p[1][2] = n12;
+                    axp[0] = -gS0; axv[0] = -dS0;
+                    axp[1] = -gS1; axv[1] = -dS1;
+                }
 
-            // ---- y: interface t+1 raw, interface t limited, y-part of (c_k, t-1) ----
-            real hS[2], kS[2], o[2][3], Fpy[2], Fvy[2], A2y[2], a1n[2], a2n[2];
+                // ---- y: interface t+1 raw, interface t limited, y-part of (c_k, t-1) ----
+                real hS[2], kS[2], o[2][3], Fpy[2], Fvy[2], A2y[2], a1n[2], a2n[2];
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const real dp = pn[k] - p[k], dv = vn[k] - v[k];
-                a1n[k] = (Z * dv - dp) * h;
-                a2n[k] = (Z * dv + dp) * h;
-                const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
-                const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim); // upwind t-1
-                Fpy[k] = fyp * (b2 - b1);
-                Fvy[k] = fyv * (b1 + b2);
-                const real A1y = fma(cZ, a1y[k], real(2) * Fpy[k]);  // into cell t-1
-                A2y[k] = fma(cZ, a2y[k], real(-2) * Fpy[k]);         // into cell t
-                const real Sy = A1y + A2y_lo[k];
-                hS[k] = gy * Sy;
-                kS[k] = dy4 * Sy;
-                o[k][0] = q3[k][0] - qpy * (a2y_lo[k] + a1y[k]) - dtdy * (Fpy[k] - Fpy_lo[k]) + real(2) * hS[k];
-                o[k][1] = q3[k][1];
-                o[k][2] = q3[k][2] + qvy * (a1y[k] - a2y_lo[k]) - dtdy * (Fvy[k] - Fvy_lo[k]);
-            }
-            // transverse transfers: column c0 from c0-1 (lane-1's c1) and c1;
-            // column c1 from c0 and c1+1 (lane+1's c0)
-            const real hL = __shfl_up_sync(FULL, hS[1], 1), kL = __shfl_up_sync(FULL, kS[1], 1);
-            const real hR = __shfl_down_sync(FULL, hS[0], 1), kR = __shfl_down_sync(FULL, kS[0], 1);
-            o[0][0] = o[0][0] - hL - hS[1];
-            o[0][1] = o[0][1] - kL + kS[1];
-            o[1][0] = o[1][0] - hS[0] - hR;
-            o[1][1] = o[1][1] - kS[0] + kR;
-            if (t - 1 >= r0) {
-                real* dst = qnew + (long long)(t - 1) * A.ld + c0;
-                if (out0) { dst[0] = o[0][0]; dst[A.fstride] = o[0][1]; dst[2 * A.fstride] = o[0][2]; }
-                if (out1) { dst[1] = o[1][0]; dst[A.fstride + 1] = o[1][1]; dst[2 * A.fstride + 1] = o[1][2]; }
-            }
+                for (int k = 0; k < 2; ++k) {
+                    const real dp = pn[k] - p[k], dv = vn[k] - v[k];
+                    a1n[k] = (Z * dv - dp) * h;
+                    a2n[k] = (Z * dv + dp) * h;
+                    const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
+                    const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim); // upwind t-1
+                    Fpy[k] = fyp * (b2 - b1);
+                    Fvy[k] = fyv * (b1 + b2);
+                    const real A1y = fma(cZ, a1y[k], real(2) * Fpy[k]);  // into cell t-1
+                    A2y[k] = fma(cZ, a2y[k], real(-2) * Fpy[k]);         // into cell t
+                    const real Sy = A1y + A2y_lo[k];
+                    hS[k] = gy * Sy;
+                    kS[k] = dy4 * Sy;
+                    o[k][0] = q3[k][0] - qpy * (a2y_lo[k] + a1y[k]) - dtdy * (Fpy[k] - Fpy_lo[k]) + real(2) * hS[k];
+                    o[k][1] = q3[k][1];
+                    o[k][2] = q3[k][2] + qvy * (a1y[k] - a2y_lo[k]) - dtdy * (Fvy[k] - Fvy_lo[k]);
+                }
+                // transverse transfers: column c0 from c0-1 (lane-1's c1) and c1;
+                // column c1 from c0 and c1+1 (lane+1's c0)
+                const real hL = __shfl_up_sync(FULL, hS[1], 1), kL = __shfl_up_sync(FULL, kS[1], 1);
+                const real hR = __shfl_down_sync(FULL, hS[0], 1), kR = __shfl_down_sync(FULL, kS[0], 1);
+                o[0][0] = o[0][0] - hL - hS[1];
+                o[0][1] = o[0][1] - kL + kS[1];
+                o[1][0] = o[1][0] - hS[0] - hR;
+                o[1][1] = o[1][1] - kS[0] + kR;
+                if (t - 1 >= r0) {
+                    real* dst = qnew + (long long)(t - 1) * A.ld + c0;
+                    if constexpr (INT) {
+                        if (out_lane) {
+                            *reinterpret_cast<P2*>(dst) = P2{o[0][0], o[1][0]};
+                            *reinterpret_cast<P2*>(dst + A.fstride) = P2{o[0][1], o[1][1]};
+                            *reinterpret_cast<P2*>(dst + 2 * A.fstride) = P2{o[0][2], o[1][2]};
+                        }
+                    } else {
+                        if (out0) { dst[0] = o[0][0]; dst[A.fstride] = o[0][1]; dst[2 * A.fstride] = o[0][2]; }
+                        if (out1) { dst[1] = o[1][0]; dst[A.fstride + 1] = o[1][1]; dst[2 * A.fstride + 1] = o[1][2]; }
+                    }
+                }
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                a2y_lo[k] = a2y[k];
-                A2y_lo[k] = A2y[k];
-                Fpy_lo[k] = Fpy[k];
-                Fvy_lo[k] = Fvy[k];
-                a1y[k] = a1n[k];
-                a2y[k] = a2n[k];
+                for (int k = 0; k < 2; ++k) {
+                    a2y_lo[k] = a2y[k];
+                    A2y_lo[k] = A2y[k];
+                    Fpy_lo[k] = Fpy[k];
+                    Fvy_lo[k] = Fvy[k];
+                    a1y[k] = a1n[k];
+                    a2y[k] = a2n[k];
+                    pc[k] = pn[k];
+                    vc[k] = vn[k];
+                }
+                __syncwarp();
+                if (t - 1 + RING <= rlast) {
+                    if (lane == 0) issue(t - 1 + RING);
+                    last_issued = t - 1 + RING;
+                }
+                __syncwarp();
             }
-            __syncwarp();
-            if (t - 1 + RING <= rlast) {
-                if (lane == 0) issue(t - 1 + RING);
-                last_issued = t - 1 + RING;
+            if (failed) {
+                for (int r = fail_row + 1; r <= last_issued; ++r) (void)wait_row(r);
+                if (lane == 0) atomicOr(&ctl->err, CTL_ERR_TMA_TIMEOUT);
             }
-            __syncwarp();
-        }
-        if (failed) {
-            for (int r = fail_row + 1; r <= last_issued; ++r) (void)wait_row(r);
-            if (lane == 0) atomicOr(&ctl->err, CTL_ERR_TMA_TIMEOUT);
-        }
+        };
+        // interior strip: columns b-3 .. b+61 inside the grid
+        const bool interior = b - 3 >= 0 && b + 61 <= mx - 1;
+        if (interior) march(std::true_type{});
+        else march(std::false_type{});
         seq_base += (uint32_t)nrows;
     }
     // Courant number as flux2 forms it (dt/dx * c over x-interfaces, dt/dy * c

@@ -188,6 +188,64 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// ------------------------------------------------- contracted arithmetic ---
+// Reciprocal and square root for the contracted (CLAW_FP64_FMA) kernels, by
+// Newton-Raphson refinement of the hardware estimates (rcp.approx /
+// rsqrt.approx, about 23 correct bits): each step doubles the correct bits,
+// so two steps reach double precision to within about an ulp.  The
+// reference-order kernels keep IEEE division and sqrt.
+__device__ __forceinline__ double rcp_newton(double a) {
+    // y <- y + y (1 - a y)
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    double e = fma(-a, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-a, y, 1.0);
+    y = fma(y, e, y);
+    return y;
+}
+__device__ __forceinline__ float rcp_newton(float a) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+    const float e = fmaf(-a, y, 1.0f);
+    return fmaf(y, e, y);
+}
+// sqrt(a): y ~ 1/sqrt(a) refined by y <- y (3 - a y^2) / 2 twice, then the
+// root s = a y corrected once by s <- s + y (a - s^2) / 2 (Newton on s^2 = a).
+// a = 0 gives 0 and a < 0 NaN, as sqrt does.
+__device__ __forceinline__ double sqrt_newton(double a) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    double h = 0.5 * a;
+    y = y * fma(-h * y, y, 1.5);
+    y = y * fma(-h * y, y, 1.5);
+    const double s = a * y;
+    const double r = fma(0.5 * y, fma(-s, s, a), s);
+    return a == 0.0 ? a : r;
+}
+
+// Arithmetic policy of a kernel build: IEEE division and square root in the
+// reference-order build (bit-identical to the CPU restatement), Newton
+// reciprocals and roots in the contracted build.
+template <bool FAST>
+struct Arith {
+    template <typename real>
+    __device__ __forceinline__ static real rcp(real a) { return real(1) / a; }
+    template <typename real>
+    __device__ __forceinline__ static real div(real a, real b) { return a / b; }
+    template <typename real>
+    __device__ __forceinline__ static real root(real a) { return sqrt(a); }
+};
+template <>
+struct Arith<true> {
+    template <typename real>
+    __device__ __forceinline__ static real rcp(real a) { return rcp_newton(a); }
+    template <typename real>
+    __device__ __forceinline__ static real div(real a, real b) { return a * rcp_newton(b); }
+    __device__ __forceinline__ static double root(double a) { return sqrt_newton(a); }
+    __device__ __forceinline__ static float root(float a) { return sqrtf(a); }
+};
+
 // ------------------------------------------------------------- limiter ---
 // Limiter function phi(r) of src/2d/inlinelimiter.f90:71-97
 // (1 minmod, 2 superbee, 3 van Leer, 4 MC, 5 Beam-Warming).
@@ -202,6 +260,27 @@ __device__ __forceinline__ real phi_limiter(int meth, real r) {
             const real c = (one + r) * real(0.5);  // == (1+r)/2 exactly
             return fmax(zero, fmin(fmin(c, two), two * r));
         }
+        case 5: return r;
+        default: return one;
+    }
+}
+
+// phi(r) of the contracted build: the same functions by compare-and-select
+// (no fmin/fmax, whose NaN rules cost extra FP64 instructions) and a Newton
+// reciprocal in van Leer's quotient.
+template <typename real>
+__device__ __forceinline__ real phi_limiter_fast(int meth, real r) {
+    const real zero = real(0), one = real(1), two = real(2);
+    auto mn = [](real a, real b) { return a < b ? a : b; };
+    auto mx = [](real a, real b) { return a > b ? a : b; };
+    switch (meth) {
+        case 1: return mx(zero, mn(one, r));
+        case 2: return mx(mx(zero, mn(one, two * r)), mn(two, r));
+        case 3: {
+            const real ar = fabs(r);
+            return (r + ar) * rcp_newton(one + ar);
+        }
+        case 4: return mx(zero, mn(mn((one + r) * real(0.5), two), two * r));
         case 5: return r;
         default: return one;
     }

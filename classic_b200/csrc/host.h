@@ -43,6 +43,10 @@ int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, 
 // (char2d.cuh, built with fused multiply-add); nullptr if cfg is not served.
 std::unique_ptr<Runner> make_char_runner(const claw_config& cfg);
 
+// 2D unsplit step of the contracted build for the methods and solvers the
+// characteristic kernel does not serve (fma2d.cu); nullptr if cfg is not served.
+std::unique_ptr<Runner> make_fast_runner2d(const claw_config& cfg);
+
 // 2D dimensionally split step (step2ds.cuh, one fused launch per step);
 // nullptr if cfg is not served.
 std::unique_ptr<Runner> make_split_runner(const claw_config& cfg);

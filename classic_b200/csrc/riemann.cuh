@@ -22,6 +22,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "common.cuh"
+
 #ifndef EULER_MINB
 #define EULER_MINB 2
 #endif
@@ -80,12 +82,24 @@ struct Acoustics2D {
 // eigenvectors of the transverse Jacobian at the same interface's Roe average.
 // (LeVeque, Finite Volume Methods for Hyperbolic Problems, 15.3 and 18.8;
 // Harten & Hyman, J. Comput. Phys. 50, 1983.)
-template <typename real_>
+// FAST (the contracted build): Newton reciprocals and square roots instead
+// of IEEE division and sqrt (to about an ulp), compare-and-select instead of
+// fmin/fmax.
+template <typename real_, bool FAST = false>
 struct EulerRoe2D {
     using real = real_;
     static constexpr int meqn = 4, mwaves = 3, maux = 0;
     static constexpr int min_blocks = EULER_MINB;  // registers for the Roe state
     real gamma, gamma1;
+    using AR = Arith<FAST>;
+    __device__ __forceinline__ static real min0(real x) {
+        if constexpr (FAST) return x < real(0) ? x : real(0);
+        else return fmin(x, real(0));
+    }
+    __device__ __forceinline__ static real max0(real x) {
+        if constexpr (FAST) return x > real(0) ? x : real(0);
+        else return fmax(x, real(0));
+    }
     __host__ __device__ static constexpr bool wave_zero(int, int) { return false; }
     __host__ __device__ static constexpr bool trans_zero(int, int) { return false; }
 
@@ -111,22 +125,22 @@ struct EulerRoe2D {
     // One reciprocal per square root and per sum (divisions are this solver's
     // costly operations); 1/rho = (1/sqrt(rho))^2.
     __device__ __forceinline__ Roe average(const real* qL, const real* qR, int mu, int mv) const {
-        const real rhsqrtl = sqrt(qL[0]);
-        const real rhsqrtr = sqrt(qR[0]);
-        const real il = real(1) / rhsqrtl;
-        const real ir = real(1) / rhsqrtr;
+        const real rhsqrtl = AR::root(qL[0]);
+        const real rhsqrtr = AR::root(qR[0]);
+        const real il = AR::rcp(rhsqrtl);
+        const real ir = AR::rcp(rhsqrtr);
         const real pl = gamma1 * (qL[3] - real(0.5) * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) * (il * il));
         const real pr = gamma1 * (qR[3] - real(0.5) * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) * (ir * ir));
-        const real i2 = real(1) / (rhsqrtl + rhsqrtr);
+        const real i2 = AR::rcp(rhsqrtl + rhsqrtr);
         Roe r;
         r.u = (qL[mu] * il + qR[mu] * ir) * i2;
         r.v = (qL[mv] * il + qR[mv] * ir) * i2;
         r.enth = ((qL[3] + pl) * il + (qR[3] + pr) * ir) * i2;
         const real u2v2 = r.u * r.u + r.v * r.v;
         const real a2 = gamma1 * (r.enth - real(0.5) * u2v2);
-        r.a = sqrt(a2);
-        r.g1a2 = gamma1 / a2;
-        r.ha = real(0.5) / r.a;
+        r.a = AR::root(a2);
+        r.g1a2 = AR::div(gamma1, a2);
+        r.ha = AR::div(real(0.5), r.a);
         r.euv = r.enth - u2v2;
         r.hu = real(0.5) * u2v2;
         return r;
@@ -134,9 +148,9 @@ struct EulerRoe2D {
 
     // normal velocity and sound speed of a conserved state (one division)
     __device__ __forceinline__ void state(const real* q, int mu, int mv, real& un, real& c) const {
-        const real ri = real(1) / q[0];
+        const real ri = AR::rcp(q[0]);
         const real p = gamma1 * (q[3] - real(0.5) * (q[mu] * q[mu] + q[mv] * q[mv]) * ri);
-        c = sqrt(gamma * p * ri);
+        c = AR::root(gamma * p * ri);
         un = q[mu] * ri;
     }
 
@@ -177,7 +191,7 @@ struct EulerRoe2D {
         const real s1 = u1 - c1;
         if (!(s0 >= real(0) && s[0] > real(0))) {
             real sfract;
-            if (s0 < real(0) && s1 > real(0)) sfract = s0 * (s1 - s[0]) / (s1 - s0);
+            if (s0 < real(0) && s1 > real(0)) sfract = AR::div(s0 * (s1 - s[0]), s1 - s0);
             else if (s[0] < real(0)) sfract = s[0];
             else sfract = real(0);
 #pragma unroll
@@ -195,7 +209,7 @@ struct EulerRoe2D {
                 state(q2, mu, mv, u2, c2);
                 const real s2 = u2 + c2;
                 real sf3;
-                if (s2 < real(0) && s3 > real(0)) sf3 = s2 * (s3 - s[2]) / (s3 - s2);
+                if (s2 < real(0) && s3 > real(0)) sf3 = AR::div(s2 * (s3 - s[2]), s3 - s2);
                 else if (s[2] < real(0)) sf3 = s[2];
                 else sf3 = real(0);
 #pragma unroll
@@ -232,10 +246,8 @@ struct EulerRoe2D {
         sb[2] = r.v + r.a;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            bm[m] = (fmin(sb[0], real(0)) * w[0][m] + fmin(sb[1], real(0)) * w[1][m]) +
-                    fmin(sb[2], real(0)) * w[2][m];
-            bp[m] = (fmax(sb[0], real(0)) * w[0][m] + fmax(sb[1], real(0)) * w[1][m]) +
-                    fmax(sb[2], real(0)) * w[2][m];
+            bm[m] = (min0(sb[0]) * w[0][m] + min0(sb[1]) * w[1][m]) + min0(sb[2]) * w[2][m];
+            bp[m] = (max0(sb[0]) * w[0][m] + max0(sb[1]) * w[1][m]) + max0(sb[2]) * w[2][m];
         }
     }
 };

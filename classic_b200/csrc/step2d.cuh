@@ -52,13 +52,20 @@ template <>
 struct BoxW<float> { static constexpr int value = 36; static constexpr int XQ = 4; };
 static_assert(STRIP % 4 == 0, "strip width must keep b a multiple of 4");
 
-// Method policy: -1 = read from the kernel arguments at run time.
-template <int ORDER, int TRANS, int LIM, int CAPA, int FWAVE>
+// Method policy: -1 = read from the kernel arguments at run time.  FAST = 1
+// is the contracted build (CLAW_FP64_FMA): Newton reciprocals instead of IEEE
+// divisions in the limiter ratio and the capacity scalings, compare-and-select
+// instead of fmin/fmax; the Courant number is formed as in the reference-order
+// build, so the dt sequence is the same.
+template <int ORDER, int TRANS, int LIM, int CAPA, int FWAVE, int FAST = 0>
 struct Method2D {
     static constexpr int order = ORDER, trans = TRANS, lim = LIM, capa = CAPA, fwave = FWAVE;
+    static constexpr bool fast = FAST != 0;
 };
 using MethodGeneric2D = Method2D<-1, -1, -1, -1, -1>;
 using MethodMC2D = Method2D<2, 2, 4, 0, 0>;  // order 2, transverse 2, MC, no capa
+using MethodGeneric2DFast = Method2D<-1, -1, -1, -1, -1, 1>;
+using MethodMC2DFast = Method2D<2, 2, 4, 0, 0, 1>;
 
 template <class S>
 struct Step2Args {
@@ -213,6 +220,16 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
         limit = (A.mthlim[0] | A.mthlim[1] | A.mthlim[2] | A.mthlim[3] | A.mthlim[4] |
                  A.mthlim[5] | A.mthlim[6] | A.mthlim[7]) != 0;
     auto lim_of = [&](int mw) -> int { return M::lim >= 0 ? M::lim : A.mthlim[mw]; };
+    using AR = Arith<M::fast>;
+    // max of two Courant numbers (the same value as fmax for non-NaN operands)
+    auto dmax = [](double a, double b) -> double {
+        if constexpr (M::fast) return b > a ? b : a;
+        else return fmax(a, b);
+    };
+    auto phi = [](int ml, real r) -> real {
+        if constexpr (M::fast) return phi_limiter_fast<real>(ml, r);
+        else return phi_limiter<real>(ml, r);
+    };
     const int lane = threadIdx.x & 31;
     const int mx = A.mx, my = A.my;
 
@@ -338,8 +355,8 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
             double em = 0.0;
 #pragma unroll
             for (int mw = 0; mw < MW; ++mw)
-                em = fmax(em, fmax(dt1 * (double)sy[mw], -dt0 * (double)sy[mw]));
-            cfl = fmax(cfl, em);
+                em = dmax(em, dmax(dt1 * (double)sy[mw], -dt0 * (double)sy[mw]));
+            cfl = dmax(cfl, em);
         }
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
@@ -370,16 +387,16 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
             const auto cx = iface_ctx(A.solver, 1, qm_t, qc_t);
             if constexpr (solver_ctx<S>::value) A.solver.rpn_ctx(1, cx, qm_t, qc_t, w, s, amdq, apdq);
             else A.solver.rpn(1, qm_t, qc_t, a_m, a_c, w, s, amdq, apdq);
-            const real dtm = capa ? dtdx / a_m[ic] : dtdx;  // dtdx1d(i-1)
-            const real dtc = capa ? dtdx / a_c[ic] : dtdx;  // dtdx1d(i)
+            const real dtm = capa ? AR::div(dtdx, a_m[ic]) : dtdx;  // dtdx1d(i-1)
+            const real dtc = capa ? AR::div(dtdx, a_c[ic]) : dtdx;  // dtdx1d(i)
             {
                 const double dm = capa ? dtdx_d / (double)a_m[ic] : dtdx_d;
                 const double dc = capa ? dtdx_d / (double)a_c[ic] : dtdx_d;
                 double em = 0.0;
 #pragma unroll
                 for (int mw = 0; mw < MW; ++mw)
-                    em = fmax(em, fmax(dc * (double)s[mw], -dm * (double)s[mw]));
-                cfl = (cx_ok && t >= -1 && t <= my) ? fmax(cfl, em) : cfl;
+                    em = dmax(em, dmax(dc * (double)s[mw], -dm * (double)s[mw]));
+                cfl = (cx_ok && t >= -1 && t <= my) ? dmax(cfl, em) : cfl;
             }
             real send1[ME], qadd[ME], F[ME], cq[ME];
 #pragma unroll
@@ -418,8 +435,8 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                         const int ml = lim_of(mw);
                         if (ml == 0) continue;
                         const real dl = __shfl_up_sync(FULL, dotr[mw], 1);
-                        const real r = (s[mw] > real(0) ? dl : dotr[mw]) / wn2[mw];
-                        const real ph = wn2[mw] != real(0) ? phi_limiter<real>(ml, r) : real(1);
+                        const real r = AR::div(s[mw] > real(0) ? dl : dotr[mw], wn2[mw]);
+                        const real ph = wn2[mw] != real(0) ? phi(ml, r) : real(1);
 #pragma unroll
                         for (int m = 0; m < ME; ++m)
                             if (!S::wave_zero(1, m)) w[mw][m] = ph * w[mw][m];
@@ -499,9 +516,9 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                         Bx = dtdy * G1;
                     }
                 } else {
-                    q2 = ((qc_t[m] + Ax_prev[m]) + qa) - (dtdx * dF + dtdy * (G2 - G1)) / a_c[ic];
-                    Ax = dtdy * G2 / a_cn[ic];
-                    Bx = dtdy * G1 / a_cp[ic];
+                    q2 = ((qc_t[m] + Ax_prev[m]) + qa) - AR::div(dtdx * dF + dtdy * (G2 - G1), a_c[ic]);
+                    Ax = AR::div(dtdy * G2, a_cn[ic]);
+                    Bx = AR::div(dtdy * G1, a_cp[ic]);
                 }
                 q3[m] = (!tz || capa) ? q2_prev[m] - Bx : q2_prev[m];  // x-part of (c, t-1)
                 q2_prev[m] = q2;
@@ -520,11 +537,11 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
             double em = 0.0;
 #pragma unroll
             for (int mw = 0; mw < MW; ++mw)
-                em = fmax(em, fmax(dt1 * (double)sn[mw], -dt0 * (double)sn[mw]));
-            cfl = (cy_ok && t + 1 <= my) ? fmax(cfl, em) : cfl;
+                em = dmax(em, dmax(dt1 * (double)sn[mw], -dt0 * (double)sn[mw]));
+            cfl = (cy_ok && t + 1 <= my) ? dmax(cfl, em) : cfl;
         }
-        const real dty_p = capa ? dtdy / a_cp[ic] : dtdy;  // dtdy1d(t-1)
-        const real dty_t = capa ? dtdy / a_c[ic] : dtdy;   // dtdy1d(t)
+        const real dty_p = capa ? AR::div(dtdy, a_cp[ic]) : dtdy;  // dtdy1d(t-1)
+        const real dty_t = capa ? AR::div(dtdy, a_c[ic]) : dtdy;   // dtdy1d(t)
         real cqy[ME], Fy[ME], dotr_y[MW];
 #pragma unroll
         for (int m = 0; m < ME; ++m) { cqy[m] = real(0); Fy[m] = real(0); }
@@ -554,8 +571,8 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                         nn = first ? wy[mw][m] * wy[mw][m] : nn + wy[mw][m] * wy[mw][m];
                         first = false;
                     }
-                    const real r = (sy[mw] > real(0) ? dotl_y[mw] : dotr_y[mw]) / nn;
-                    const real ph = nn != real(0) ? phi_limiter<real>(ml, r) : real(1);
+                    const real r = AR::div(sy[mw] > real(0) ? dotl_y[mw] : dotr_y[mw], nn);
+                    const real ph = nn != real(0) ? phi(ml, r) : real(1);
 #pragma unroll
                     for (int m = 0; m < ME; ++m)
                         if (!S::wave_zero(2, m)) wy[mw][m] = ph * wy[mw][m];
@@ -619,10 +636,10 @@ __device__ __forceinline__ void step2_rows(const Step2Args<S>& A, const StepCons
                 else if (!tz) q5 = q5 + (-(dtdx * (G2 - G1)));
                 q6 = tz ? q5 : q5 - __shfl_down_sync(FULL, dtdx * G1, 1);  // from column c+1
             } else {
-                const real Al = __shfl_up_sync(FULL, dtdx * G2 / a_pp[ic], 1);
-                const real Br = __shfl_down_sync(FULL, dtdx * G1 / a_mp[ic], 1);
+                const real Al = __shfl_up_sync(FULL, AR::div(dtdx * G2, a_pp[ic]), 1);
+                const real Br = __shfl_down_sync(FULL, AR::div(dtdx * G1, a_mp[ic]), 1);
                 const real q4 = q3[m] + Al;
-                const real q5 = (q4 + qa) - (dtdy * dF + dtdx * (G2 - G1)) / a_cp[ic];
+                const real q5 = (q4 + qa) - AR::div(dtdy * dF + dtdx * (G2 - G1), a_cp[ic]);
                 q6 = q5 - Br;
             }
             qo[m] = q6;

@@ -45,7 +45,7 @@ def main():
     else:
         rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=args.n)
         cmax = 1.0
-        prec = "fp64" if args.split == "unsplit" else args.precision
+        prec = args.precision
     rd.clawdata.dimensional_split = args.split
     s = Solver(rd.clawdata, solver, params, precision=prec)
     s.set_q(q0)

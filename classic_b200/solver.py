@@ -184,6 +184,10 @@ class Solver:
                      "claw_advance_host")
         return info, st.as_dict()
 
+    def set_steps_max(self, n: int):
+        """nv(1) of the following advance calls: return (info 11) after n steps."""
+        check(self.lib.claw_set_steps_max(self._h, int(n)), "claw_set_steps_max")
+
     def launch_count(self) -> int:
         return int(self.lib.claw_launch_count(self._h))
 
@@ -324,14 +328,17 @@ class BatchSolver:
     ABI): one persistent launch per step over the rows of every instance
     still running."""
 
-    def __init__(self, clawdatas, solver: str, params: dict | None = None):
+    def __init__(self, clawdatas, solver: str, params: dict | None = None,
+                 precision: str = "fp64"):
+        """precision "fp64" (reference order) or "fp64_fma" (the contracted
+        build: fused multiply-adds, Newton reciprocals and roots)."""
         self.lib = _lib.load()
         cds = [c.clawdata if isinstance(c, ClawRunData) else c for c in clawdatas]
         self.count = len(cds)
         arr = (ClawConfig * self.count)()
         self.q_shapes = []
         for k, cd in enumerate(cds):
-            arr[k] = make_config(cd, solver, params, "fp64")
+            arr[k] = make_config(cd, solver, params, precision)
             cells = [arr[k].num_cells[d] for d in range(2)]
             self.q_shapes.append((arr[k].num_eqn, cells[1], cells[0]))
         self._cfgs = arr

@@ -186,6 +186,12 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial,
 int claw_advance_host(claw_handle* h, double* q, double tstart, double tend,
                       double dt_initial, claw_stats* stats);
 
+/* nv(1) of the following claw_advance calls: the most time steps one call
+ * takes before it returns info 11 with the state reached (claw2ez passes it
+ * to every claw2 call; src/2d/claw2.f:497, 596, 766-769); starts as
+ * cfg.steps_max. */
+int claw_set_steps_max(claw_handle* h, int steps_max);
+
 /* Device view of the current q (for zero-copy users): pointer, element size,
  * row pitch and field pitch in elements. */
 int claw_q_device(claw_handle* h, void** ptr, int* elem_bytes, long long* ld,

@@ -267,3 +267,42 @@ def test_frames_written_and_restart_continues(tmp_path):
     info, st = o.advance(t1, t1 + dtout, float(rd.clawdata.dt_initial))
     assert info == 0 and st["t_reached"] == fr2[0].t
     assert same(fr2[0].q, o.get_q())
+
+
+def test_steps_max_windows_equal_one_advance():
+    """nv(1) per call (claw_set_steps_max): each call stops after 7 steps with
+    info 11 and dtv(5); chaining the calls as claw2ez chains frames gives the
+    same state, step count and dt as one call (and the oracle's claw2 with
+    the same nv(1) returns the same info)."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=96)
+    one = Solver(rd.clawdata, solver, params)
+    one.set_q(q0)
+    info, st = one.advance(0.0, 0.2, 0.01)
+    assert info == 0
+    win = Solver(rd.clawdata, solver, params)
+    win.set_q(q0)
+    win.set_steps_max(7)
+    t, dt, steps, calls = 0.0, 0.01, 0, 0
+    while t < 0.2:
+        info_w, sw = win.advance(t, 0.2, dt)
+        assert info_w in (0, 11)
+        assert sw["steps_taken"] <= 7
+        if info_w == 11:
+            assert sw["steps_taken"] == 7 and sw["t_reached"] < 0.2
+        t, dt = sw["t_reached"], sw["dt_next"]
+        steps += sw["steps_taken"]
+        calls += 1
+    assert steps == st["steps_taken"] and calls > 2
+    assert dt == st["dt_next"] and t == st["t_reached"]
+    assert same(win.get_q(), one.get_q())
+    rd.clawdata.steps_max = 7
+    o = OracleGrid(rd.clawdata, solver, params)
+    o.set_q(q0)
+    info_o, so = o.advance(0.0, 0.2, 0.01)
+    g = Solver(rd.clawdata, solver, params)
+    g.set_q(q0)
+    info_g, sg = g.advance(0.0, 0.2, 0.01)
+    assert info_o == info_g == 11 and sg["steps_taken"] == so["steps_taken"] == 7
+    assert same(g.get_q(), o.get_q())
+    for s in (one, win, g):
+        s.close()
