@@ -417,39 +417,42 @@ def other_configs(peaks, cpu=True):
                         "roofline": roofline_entry(rate, nbytes, peaks)}
         except Exception as e:
             out[key] = {"error": str(e)}
-    try:
-        sizes = problems.euler_ensemble_sizes(256, seed=0)
-        insts = [problems.euler_quadrants(n=nn, seed=1000 + k) for k, nn in enumerate(sizes)]
-        b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4})
-        for k, inst in enumerate(insts):
-            b.set_q(k, inst[3])
-        shape = b.autotune(repeats=2)  # launch shape chosen before the timed run
-        info, st = b.advance(0.0, 0.25)
-        b.close()
-        upd = sum(nn * nn * (x["steps_taken"] + x["steps_rejected"]) for nn, x in zip(sizes, st))
-        ms = st[0]["device_ms"]
-        rate = upd / (ms * 1e-3)
-        e = {"cell_updates_per_s": rate, "cell_updates": upd,
-             "device_ms": ms, "launches": st[0]["launches"],
-             "steps_min_max": [min(x["steps_taken"] for x in st),
-                               max(x["steps_taken"] for x in st)],
-             "autotuned_shape": {"min_rows": shape["min_rows"],
-                                 "ctas_per_sm": shape["ctas_per_sm"]},
-             "roofline": roofline_entry(rate, 64, peaks, "step2_batch_kernel_euler", fp64_peak)}
-        if cpu:
-            nn = 512
-            mk = lambda: problems.euler_quadrants(n=nn, seed=7)[:4] + (None,)
-            r1, s1 = cpu_rate(mk, 20, 1, 2e-4)
-            rn, sn = cpu_rate(mk, 40, nproc, 2e-4)
-            e["cpu_baseline"] = {"value": r1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-                                 "sample": f"20 whole steps of one 512^2 instance from its initial data "
-                                           f"({s1:.1f} s); the reference advances one grid per claw2 "
-                                           "call, serially",
-                                 "threaded": {"value": rn, "cores": nproc,
-                                              "sample": f"40 steps ({sn:.1f} s), every third slice in parallel"}}
-        out["euler_batch_256"] = e
-    except Exception as e:
-        out["euler_batch_256"] = {"error": str(e)}
+    sizes = problems.euler_ensemble_sizes(256, seed=0)
+    for prec in ("fp64", "fp64_fma"):
+        key = "euler_batch_256" if prec == "fp64" else "euler_batch_256_fp64_fma"
+        try:
+            insts = [problems.euler_quadrants(n=nn, seed=1000 + k) for k, nn in enumerate(sizes)]
+            b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4}, precision=prec)
+            for k, inst in enumerate(insts):
+                b.set_q(k, inst[3])
+            shape = b.autotune(repeats=2)  # launch shape chosen before the timed run
+            info, st = b.advance(0.0, 0.25)
+            b.close()
+            upd = sum(nn * nn * (x["steps_taken"] + x["steps_rejected"]) for nn, x in zip(sizes, st))
+            ms = st[0]["device_ms"]
+            rate = upd / (ms * 1e-3)
+            kern = "step2_batch_kernel_euler" + ("_fp64_fma" if prec == "fp64_fma" else "")
+            e = {"cell_updates_per_s": rate, "cell_updates": upd, "precision": prec,
+                 "device_ms": ms, "launches": st[0]["launches"],
+                 "steps_min_max": [min(x["steps_taken"] for x in st),
+                                   max(x["steps_taken"] for x in st)],
+                 "autotuned_shape": {"min_rows": shape["min_rows"],
+                                     "ctas_per_sm": shape["ctas_per_sm"]},
+                 "roofline": roofline_entry(rate, 64, peaks, kern, fp64_peak)}
+            if cpu and prec == "fp64":
+                nn = 512
+                mk = lambda: problems.euler_quadrants(n=nn, seed=7)[:4] + (None,)
+                r1, s1 = cpu_rate(mk, 20, 1, 2e-4)
+                rn, sn = cpu_rate(mk, 40, nproc, 2e-4)
+                e["cpu_baseline"] = {"value": r1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                                     "sample": f"20 whole steps of one 512^2 instance from its initial data "
+                                               f"({s1:.1f} s); the reference advances one grid per claw2 "
+                                               "call, serially",
+                                     "threaded": {"value": rn, "cores": nproc,
+                                                  "sample": f"40 steps ({sn:.1f} s), every third slice in parallel"}}
+            out[key] = e
+        except Exception as e:
+            out[key] = {"error": str(e)}
     return out
 
 

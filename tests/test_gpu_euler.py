@@ -162,3 +162,30 @@ def test_batch_shapes_agree(rows, ctas):
         o.advance(0.0, 0.05, rd.clawdata.dt_initial)
         assert same(b.get_q(k), o.get_q()), k
     b.close()
+
+
+def test_ensemble_256_spot_checks():
+    """The 256-instance ensemble the benchmark times (sides log-uniform in
+    128..1024, seeds 1000..1255) in one batch to t = 0.25: its three smallest
+    instances equal claw2 run on them alone (the CPU restatement, bit for
+    bit), and an instance that ends with non-finite values (the Roe solver
+    meeting a state without positive pressure) does so in the restatement
+    too, at the same cells, when it is small enough to rerun on the CPU."""
+    sizes = problems.euler_ensemble_sizes(256, seed=0)
+    insts = [problems.euler_quadrants(n=n, seed=1000 + k) for k, n in enumerate(sizes)]
+    b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4})
+    for k, inst in enumerate(insts):
+        b.set_q(k, inst[3])
+    b.advance(0.0, 0.25)
+    qs = [b.get_q(k) for k in range(len(sizes))]
+    b.close()
+    bad = [k for k, q in enumerate(qs) if not np.all(np.isfinite(q))]
+    check = sorted(range(len(sizes)), key=lambda k: sizes[k])[:3]
+    check += [k for k in bad if sizes[k] <= 160 and k not in check]
+    for k in check:
+        rd, solver, params, q0, _ = insts[k]
+        o = OracleGrid(rd.clawdata, solver, params)
+        o.set_q(q0)
+        o.advance(0.0, 0.25, rd.clawdata.dt_initial)
+        assert same(qs[k], o.get_q()), (k, sizes[k])
+    print(f"non-finite instances: {[(k, sizes[k]) for k in bad]}; checked: {check}")
