@@ -89,7 +89,10 @@ struct CharArgs {
     int bc[4];
     int lim;
     double dx, dy;
-    long long units;
+    // Work items: row block b (brows rows) of strip s, item = b * nstrips + s,
+    // so the warps at work on one row block hold adjacent strips and stream
+    // neighbouring DRAM pages.  Warp w takes items w, w + nwarps, ...
+    int brows, nblocks;
     int nwarps;
     ClawCtl* ctl;
     CharAcoustics2D<real> s;
@@ -188,16 +191,14 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     uint32_t seq_base = 0;
     bool any_work = false;
 
-    const long long gw = (long long)blockIdx.x * WARPS2D + warp;
-    long long u0 = (gw < A.nwarps) ? gw * A.units / A.nwarps : 0;
-    const long long u1 = (gw < A.nwarps) ? (gw + 1) * A.units / A.nwarps : 0;
+    const int gw = blockIdx.x * WARPS2D + warp;
+    const int items = A.nstrips * A.nblocks;
 
-    while (u0 < u1 && !failed) {
+    for (int item = gw; gw < A.nwarps && item < items && !failed; item += A.nwarps) {
         any_work = true;
-        const int strip = (int)(u0 / my);
-        const int r0 = (int)(u0 % my);
-        const int nr = (int)min((long long)(my - r0), u1 - u0);
-        u0 += nr;
+        const int strip = item % A.nstrips;
+        const int r0 = (item / A.nstrips) * A.brows;
+        const int nr = min(A.brows, my - r0);
         const int b = strip * STRIP2;
         const int c0 = b - 2 + 2 * lane, c1 = c0 + 1;  // this lane's two columns
         const int x0 = b - R::XQ;

@@ -1,6 +1,7 @@
 // Characteristic-variable 2D acoustics runner (char2d.cuh).  This
 // translation unit is compiled with fused multiply-add contraction; it
 // serves CLAW_FP64_FMA and CLAW_FP32.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 
@@ -50,10 +51,15 @@ struct CharRunner : Runner {
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
-        args.units = (long long)args.nstrips * g.my;
-        const long long want = args.units / 48 > 0 ? args.units / 48 : 1;
+        // Row blocks: as many as fill the resident warps with one item each
+        // (items = strips x blocks), at least 32 rows high.
         const long long full = (long long)nsm * per_sm * WARPS2D;
-        const long long nw = want < full ? want : full;
+        long long nb = std::max(1LL, full / args.nstrips);
+        nb = std::min(nb, std::max(1LL, (long long)(g.my + 31) / 32));
+        args.brows = (int)((g.my + nb - 1) / nb);
+        args.nblocks = (g.my + args.brows - 1) / args.brows;
+        const long long items = (long long)args.nstrips * args.nblocks;
+        const long long nw = std::min(items, full);
         grid = (int)((nw + WARPS2D - 1) / WARPS2D);
         args.nwarps = (int)nw;
         return 0;
