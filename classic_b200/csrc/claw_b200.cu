@@ -70,13 +70,6 @@ int make_map3(CUtensorMap* map, void* base, int es, long long n0, long long n1, 
 
 }  // namespace clawb200
 
-#ifndef CLAW_LD_PAD
-#define CLAW_LD_PAD 32  // doubles (256 bytes) added to a row pitch that is a multiple of 4 KB
-#endif
-#ifndef CLAW_FS_PAD
-#define CLAW_FS_PAD 64  // doubles (512 bytes) added to a field pitch that is a multiple of 1 MB
-#endif
-
 namespace {
 
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
@@ -484,12 +477,7 @@ int claw_create(const claw_config* cfg, claw_handle** out) {
     g.dy = g.dim >= 2 ? (cfg->upper[1] - cfg->lower[1]) / (double)(float)g.my : 1.0;
     g.dz = g.dim >= 3 ? (cfg->upper[2] - cfg->lower[2]) / (double)(float)g.mz : 1.0;
     g.ld = g.dim == 1 ? g.mx : round_up(g.mx, 32);
-    // Row and field pitches that are multiples of 4 KB / 1 MB send the rows a
-    // warp streams and the three fields of one row to the same DRAM channels;
-    // an extra 256 (512) bytes spreads them.
-    if (g.dim >= 2 && (g.ld * g.es) % 4096 == 0) g.ld += CLAW_LD_PAD * 8 / g.es;
     g.fstride = g.ld * g.my * g.mz;
-    if (g.dim >= 2 && (g.fstride * g.es) % (1 << 20) == 0) g.fstride += CLAW_FS_PAD * 8 / g.es;
     const int ax = g.mx + 4;
     g.ald = g.dim == 1 ? ax : round_up(ax, 4);
     g.afstride = g.ald * (g.dim >= 2 ? g.my + 4 : 1) * (g.dim >= 3 ? g.mz + 4 : 1);

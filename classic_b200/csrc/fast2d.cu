@@ -51,17 +51,10 @@ struct CharRunner : Runner {
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
-        // Row blocks: as many as fill the resident warps with one item each
-        // (items = strips x blocks), at least 32 rows high.
         const long long full = (long long)nsm * per_sm * WARPS2D;
-        long long nb = std::max(1LL, full / args.nstrips);
-        nb = std::min(nb, std::max(1LL, (long long)(g.my + 31) / 32));
-        args.brows = (int)((g.my + nb - 1) / nb);
-        args.nblocks = (g.my + args.brows - 1) / args.brows;
-        const long long items = (long long)args.nstrips * args.nblocks;
-        const long long nw = std::min(items, full);
-        grid = (int)((nw + WARPS2D - 1) / WARPS2D);
-        args.nwarps = (int)nw;
+        const int nw = row_blocks(full, args.nstrips, g.my, 32, &args.brows, &args.nblocks);
+        grid = (nw + WARPS2D - 1) / WARPS2D;
+        args.nwarps = nw;
         return 0;
     }
 

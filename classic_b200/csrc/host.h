@@ -30,6 +30,20 @@ struct Runner {
     virtual int launches_per_step() const { return 1; }
 };
 
+// Row-block-major work items of a 2D column-march kernel: as many row blocks
+// as fill `full` resident warps with one item (strip x row block) each, every
+// block at least min_rows high.  Returns the warps to launch.
+inline int row_blocks(long long full, int nstrips, int my, int min_rows, int* brows, int* nblocks) {
+    long long nb = full / nstrips;
+    if (nb < 1) nb = 1;
+    const long long cap = (my + min_rows - 1) / min_rows;
+    if (nb > cap) nb = cap > 0 ? cap : 1;
+    *brows = (int)((my + nb - 1) / nb);
+    *nblocks = (my + *brows - 1) / *brows;
+    const long long items = (long long)nstrips * *nblocks;
+    return (int)(items < full ? items : full);
+}
+
 // Record an error message (claw_last_error) and return code.
 int fail(int code, const char* fmt, ...);
 void set_last_error(const char* msg);

@@ -66,13 +66,10 @@ struct Runner2D : Runner {
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "step2 kernel cannot be resident on an SM");
         args.units = (long long)args.nstrips * g.my;
-        // every warp gets at least ~48 rows of one strip so the 4-row march
-        // prologue stays a small fraction of its work
-        const long long want = std::max(1LL, args.units / 48);
         const long long full = (long long)nsm * per_sm * WARPS2D;
-        const long long nw = std::min(full, want);
-        grid = (int)((nw + WARPS2D - 1) / WARPS2D);
-        args.nwarps = (int)nw;
+        const int nw = row_blocks(full, args.nstrips, g.my, 32, &args.brows, &args.nblocks);
+        grid = (nw + WARPS2D - 1) / WARPS2D;
+        args.nwarps = nw;
         return 0;
     }
 

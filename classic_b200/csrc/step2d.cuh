@@ -82,6 +82,13 @@ struct Step2Args {
     double dx, dy;
     long long units;          // nstrips * my
     int nwarps;               // warps sharing the units
+    // Row-block-major work items (brows > 0): item = block * nstrips + strip,
+    // block b covering rows [b brows, (b+1) brows); warp w takes items w,
+    // w + nwarps, ...  The warps at work on one row block hold adjacent
+    // strips, so they stream neighbouring DRAM pages.  brows = 0: warp w
+    // takes units [w units / nwarps, (w+1) units / nwarps) in strip-major
+    // order.
+    int brows, nblocks;
     // source term (src/2d/claw2.f:635-738): 0 none, 1 Godunov, 2 Strang; the
     // radial term of examples/acoustics_2d_radial/1drad/src1.f on every row
     int src_split;
@@ -727,7 +734,15 @@ step2_kernel(const __grid_constant__ Step2Args<S> A) {
     // claw2 wraps the source steps around step2; a single step (claw_step) is step2 alone
     if (SRC && ctl->mode == CTL_ADVANCE) K.src = A.src_split;
 
-    while (u0 < u1 && !failed) {
+    if (A.brows > 0) {
+        const int items = A.nstrips * A.nblocks;
+        for (int item = (int)gw; gw < A.nwarps && item < items && !failed; item += A.nwarps) {
+            const int strip = item % A.nstrips, r0 = (item / A.nstrips) * A.brows;
+            step2_rows<S, M, SRC>(A, K, strip, r0, min(A.brows, my - r0), ring, bars, seq_base,
+                                  cfl, failed);
+        }
+    }
+    while (A.brows == 0 && u0 < u1 && !failed) {
         const int strip = (int)(u0 / my);
         const int r0 = (int)(u0 % my);
         const int nr = (int)min((long long)(my - r0), u1 - u0);

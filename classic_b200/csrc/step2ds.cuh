@@ -577,7 +577,15 @@ split2_kernel(const __grid_constant__ Step2Args<S> A) {
     const long long gw = (long long)blockIdx.x * WARPS2D + warp;
     long long u0 = (gw < A.nwarps) ? gw * A.units / A.nwarps : 0;
     const long long u1 = (gw < A.nwarps) ? (gw + 1) * A.units / A.nwarps : 0;
-    while (u0 < u1 && !failed) {
+    if (A.brows > 0) {  // row-block-major work items (Step2Args)
+        const int items = A.nstrips * A.nblocks;
+        for (int item = (int)gw; gw < A.nwarps && item < items && !failed; item += A.nwarps) {
+            const int strip = item % A.nstrips, r0 = (item / A.nstrips) * A.brows;
+            split2_rows<S, M, STRANG, SRC>(A, K, strip, r0, min(A.brows, my - r0), ring, bars,
+                                           seq_base, cfl, failed);
+        }
+    }
+    while (A.brows == 0 && u0 < u1 && !failed) {
         const int strip = (int)(u0 / my);
         const int r0 = (int)(u0 % my);
         const int nr = (int)min((long long)(my - r0), u1 - u0);

@@ -5,6 +5,11 @@
     python -m classic_b200.profile_step --dim 3 --n 128 --steps 2
     python -m classic_b200.profile_step --n 2048 --split godunov --precision fp64
     python -m classic_b200.profile_step --nn --n 256 --steps 3
+    python -m classic_b200.profile_step --batch 16 --n 512 --steps 3 --precision fp64_fma
+
+With --batch K each step is one launch of the batched Euler ensemble kernel
+over K seeded four-quadrant instances of n^2 cells (one claw_batch_advance
+over `steps` time steps).
 
 With --nn each step is one forward pass of the corrector network (five
 tcgen05 convolutions) on a batch of 8 random n x n inputs.
@@ -26,7 +31,21 @@ def main():
     ap.add_argument("--precision", default="fp64_fma", choices=["fp64", "fp64_fma", "fp32"])
     ap.add_argument("--split", default="unsplit", choices=["unsplit", "godunov", "strang"])
     ap.add_argument("--nn", action="store_true", help="the corrector network's forward pass")
+    ap.add_argument("--batch", type=int, default=0, help="Euler ensemble of this many instances")
     args = ap.parse_args()
+    if args.batch:
+        from .solver import BatchSolver
+        insts = [problems.euler_quadrants(n=args.n, seed=1000 + k) for k in range(args.batch)]
+        prec = "fp64_fma" if args.precision == "fp64_fma" else "fp64"
+        b = BatchSolver([i[0] for i in insts], "euler_roe_2d", {"gamma": 1.4}, precision=prec)
+        for k, inst in enumerate(insts):
+            b.set_q(k, inst[3])
+        dt = 1e-3 * 256 / args.n
+        b.advance(0.0, args.steps * dt, [dt] * args.batch)  # one launch per step
+        print(f"{args.steps} ensemble steps of {args.batch} x {args.n}^2 ({prec}), "
+              f"sum rho = {sum(float(b.get_q(k)[0].sum()) for k in range(args.batch)):.12e}")
+        b.close()
+        return
     if args.nn:
         import torch
 
