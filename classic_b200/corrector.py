@@ -241,8 +241,8 @@ class PairGenerator:
         self.n, self.r, self.gamma, self.tfinal = n, ratio, gamma, tfinal
         self.lib = _lib.load()
 
-    def run(self, seed, norm: Norm, keep_steps, x_out, t_out, slot0, cfl_desired=0.9,
-            net=None, alpha=1.0, gamma_tol=1e-10, interval=1):
+    def run(self, seed, norm: Norm, keep_steps, x_out, t_out, slot0, net=None, alpha=1.0,
+            gamma_tol=1e-10, interval=1, fine_precision="fp64"):
         """Advance one instance to tfinal in windows of `interval` coarse
         steps; for the windows whose index is in keep_steps write features
         (the window's start state and increment) / targets (the block-averaged
@@ -252,21 +252,23 @@ class PairGenerator:
         grid runs its own corrected trajectory (alpha times the network at
         the end of each window), so the pairs cover the states the corrector
         meets at inference, with targets from the fine run at the same times.
-        Returns (windows, slots used)."""
+        Both grids advance with the library's claw2 (device-side dt control):
+        the coarse one `interval` steps per call (nv(1) = interval), the fine
+        one to the time the coarse window reached.  Returns (windows, slots
+        used)."""
         torch = _torch()
         n, r = self.n, self.r
         rdf, solver, params, qf0, _ = problems.euler_quadrants(n=n * r, seed=seed, gamma=self.gamma)
         rdc, _, _, _, _ = problems.euler_quadrants(n=n, seed=seed, gamma=self.gamma)
-        fine = Solver(rdf.clawdata, solver, params)
+        fine = Solver(rdf.clawdata, solver, params, precision=fine_precision)
         coarse = Solver(rdc.clawdata, solver, params)
+        coarse.set_steps_max(interval)
         fine.set_q(qf0)
         nd = norm.device()
         st = _stream()
-        t, dt, dtf = 0.0, 1e-3, 1e-3 / r
-        qold = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
         qwin = torch.empty((4, n, n), dtype=torch.float64, device="cuda")  # window start
         qfa = torch.empty((4, n, n), dtype=torch.float64, device="cuda")
-        step, slot = 0, slot0
+        win, slot = 0, slot0
         keep = set(keep_steps)
         if net is not None:
             xin = torch.empty((1, n, n, 16), dtype=torch.bfloat16, device="cuda")
@@ -278,33 +280,28 @@ class PairGenerator:
             qc, ldc, fsc = q_view(coarse)
             check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qc), ldc, fsc, n, n, r, 4, st),
                   "nn_block_average")
+        t, dt, dtf = 0.0, 1e-3, 1e-3 / r
         while t < self.tfinal:
-            dt = min(dt, self.tfinal - t)
             qf, ldf, fsf = q_view(fine)
             qc, ldc, fsc = q_view(coarse)
-            first = step % interval == 0
-            if net is None and first:
+            if net is None:
                 check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qc), ldc, fsc, n, n, r, 4, st),
                       "nn_block_average")
-            qold.copy_(qc)
-            if first:
-                qwin.copy_(qc)
-            cfl = coarse.step(dt)
-            if cfl > 1.0:  # rejected: retry from the same state with a smaller dt
-                qn, _, _ = q_view(coarse)
-                qn.copy_(qold)
-                dt = dt * cfl_desired / cfl
-                continue
-            qs, ldc, fsc = q_view(coarse)
-            info, sf = fine.advance(t, t + dt, dtf)
+            qwin.copy_(qc)
+            torch.cuda.current_stream().synchronize()  # the solvers' streams do not wait on torch's
+            info, sc = coarse.advance(t, self.tfinal, dt)
+            if info not in (0, 11):
+                raise RuntimeError(f"coarse run info {info}")
+            t1 = sc["t_reached"]
+            info, sf = fine.advance(t, t1, dtf)
             if info != 0:
                 raise RuntimeError(f"fine run info {info}")
             dtf = sf["dt_next"]
-            qsc = qs.contiguous()
-            last = step % interval == interval - 1
-            win = step // interval
-            if last and win in keep:
-                qf, _, _ = q_view(fine)
+            full = sc["steps_taken"] == interval
+            qs, ldc, fsc = q_view(coarse)
+            qsc = qs.contiguous() if ldc != n else qs
+            if full and win in keep:
+                qf, ldf, fsf = q_view(fine)
                 check(self.lib.nn_block_average(_p(qf), ldf, fsf, _p(qfa), n, n * n, n, n, r, 4, st),
                       "nn_block_average")
                 check(self.lib.nn_features(_p(qwin), _p(qsc), n, n * n, n, n, slot, _p(nd), _p(x_out),
@@ -312,19 +309,19 @@ class PairGenerator:
                 check(self.lib.nn_residual_target(_p(qfa), _p(qsc), n, n * n, n, n, slot, _p(nd),
                                                   _p(t_out), st), "nn_residual_target")
                 slot += 1
-            if net is not None and last:
+            if net is not None and full:
                 check(self.lib.nn_features(_p(qwin), _p(qsc), n, n * n, n, n, 0, _p(nd), _p(xin), st),
                       "nn_features")
                 out = net.forward(xin)
                 check(self.lib.nn_apply_correction(_p(qs), ldc, fsc, n, n, _p(out), 16, _p(nda),
                                                    self.gamma, gamma_tol, _p(flags), st),
                       "nn_apply_correction")
-            t = sf["t_reached"]
-            dt = dt * cfl_desired / cfl if cfl > 0 else dt
-            step += 1
+            torch.cuda.current_stream().synchronize()
+            t, dt = t1, sc["dt_next"]
+            win += 1
         fine.close()
         coarse.close()
-        return step // interval, slot - slot0
+        return win, slot - slot0
 
 
 def train(net: ConvNet, x, target, iters=2000, batch=16, crop=64, lr=1e-3, seed=0, log=None,

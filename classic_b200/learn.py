@@ -30,7 +30,7 @@ def _log(*a):
     print(*a, flush=True)
 
 
-def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0, interval=1):
+def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0, interval=1, fine_precision="fp64"):
     torch = C._torch()
     total = len(seeds) * keep
     x = torch.empty((total, n, n, 16), dtype=torch.bfloat16, device="cuda")
@@ -43,7 +43,8 @@ def generate(seeds, norm, n, keep, rng, net=None, alpha=1.0, interval=1):
         est = int(0.6 * n) // interval  # windows of `interval` coarse steps
         kept = sorted(rng.choice(np.arange(1 if interval > 1 else 2, est),
                                  size=min(keep, est - 2), replace=False).tolist())
-        steps, k = gen.run(seed, norm, kept, x, t, used, net=net, alpha=alpha, interval=interval)
+        steps, k = gen.run(seed, norm, kept, x, t, used, net=net, alpha=alpha, interval=interval,
+                           fine_precision=fine_precision)
         if k and not (torch.isfinite(x[used:used + k].float()).all() and
                       torch.isfinite(t[used:used + k]).all()):
             k = 0  # a run that left the physical states: drop its pairs
@@ -133,6 +134,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--interval", type=int, default=1,
                     help="coarse steps between corrections (windows of the pairs)")
+    ap.add_argument("--fine-precision", default="fp64", choices=["fp64", "fp64_fma"],
+                    help="arithmetic of the fine runs that make the training targets "
+                         "(evaluation always uses the reference-order FP64 fine run)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     torch = C._torch()
@@ -141,7 +145,8 @@ def main(argv=None):
     held_seeds = list(range(20000, 20000 + args.heldout))
     t0 = time.perf_counter()
     K = args.interval
-    x, t, steps = generate(train_seeds, C.default_norm(), args.n, args.keep, rng, interval=K)
+    x, t, steps = generate(train_seeds, C.default_norm(), args.n, args.keep, rng, interval=K,
+                           fine_precision=args.fine_precision)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t0
     _log(f"pairs: {x.shape[0]} from {len(train_seeds)} seeds in {t_gen:.1f} s "
@@ -163,7 +168,7 @@ def main(argv=None):
     for rnd in range(args.rounds):
         seeds_r = list(range(50000 + 1000 * rnd, 50000 + 1000 * rnd + args.round_seeds))
         xr, tr_, _ = generate(seeds_r, norm, args.n, args.keep, rng, net=net, alpha=0.5,
-                              interval=K)
+                              interval=K, fine_precision=args.fine_precision)
         if args.clip > 0:
             tr_.clamp_(-args.clip, args.clip)
         C.project_tiles(tr_)
