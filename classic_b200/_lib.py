@@ -125,6 +125,7 @@ SIGNATURES = {
                                           ctypes.POINTER(ClawStats)]),
     "claw_last_error": (ctypes.c_char_p, []),
     "claw_probe_fp64": (ctypes.c_int, [_D, _D]),
+    "claw_check_newton": (ctypes.c_int, [_D, ctypes.c_int, _D, _D]),
     # learned corrector kernels (include/claw_nn.h)
     "nn_conv3x3_forward": (ctypes.c_int, [_P, _P, _P, _P, _P] + [ctypes.c_int] * 7 + [_P]),
     "nn_conv3x3_wgrad": (ctypes.c_int, [_P] * 6 + [ctypes.c_int] * 5 + [_P]),

@@ -439,6 +439,25 @@ def plain_run(seed, n, gamma=1.4, tfinal=0.25, precision="fp64"):
     return q, st["steps_taken"], wall
 
 
+def save_trained(path, net: ConvNet, norm: Norm, alpha: float, interval: int):
+    """One .npz with everything a corrected run needs: the FP32 master
+    weights and biases of the five layers, the feature / target scaling, the
+    chosen correction strength alpha and the correction interval."""
+    st = net.state()
+    np.savez(path, **{f"w{k}": w for k, w in enumerate(st["w"])},
+             **{f"b{k}": b for k, b in enumerate(st["b"])},
+             norm=norm.values, alpha=np.float64(alpha), interval=np.int64(interval))
+
+
+def load_trained(path):
+    """(net, norm, alpha, interval) from a file written by save_trained."""
+    d = np.load(path)
+    net = ConvNet(seed=0)
+    net.load({"w": [d[f"w{k}"] for k in range(len(LAYERS))],
+              "b": [d[f"b{k}"] for k in range(len(LAYERS))]})
+    return net, Norm(np.array(d["norm"], dtype=np.float64)), float(d["alpha"]), int(d["interval"])
+
+
 def block_average(q, r):
     m, h, w = q.shape
     return q.reshape(m, h // r, r, w // r, r).mean(axis=(2, 4))

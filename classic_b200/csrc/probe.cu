@@ -6,6 +6,7 @@
 #include <cstdio>
 
 #include "../../include/claw_b200.h"
+#include "common.cuh"
 
 namespace clawb200 {
 int fail(int code, const char* fmt, ...);
@@ -29,7 +30,32 @@ __global__ void __launch_bounds__(256) fp64_fma_probe(double* out, int iters, do
     out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+__global__ void newton_check_kernel(const double* x, int n, double* r, double* q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        r[i] = clawb200::rcp_newton(x[i]);
+        q[i] = clawb200::sqrt_newton(x[i]);
+    }
+}
+
 }  // namespace
+
+extern "C" int claw_check_newton(const double* x, int n, double* rcp, double* root) {
+    if (!x || !rcp || !root || n < 1) return clawb200::fail(CLAW_E_INVALID, "bad arguments");
+    double* d = nullptr;
+    const size_t bytes = sizeof(double) * (size_t)n;
+    if (cudaMalloc(&d, 3 * bytes) != cudaSuccess) return clawb200::fail(CLAW_E_CUDA, "cudaMalloc failed");
+    int rc = 0;
+    if (cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice) != cudaSuccess) rc = CLAW_E_CUDA;
+    if (!rc) {
+        newton_check_kernel<<<(n + 255) / 256, 256>>>(d, n, d + n, d + 2 * (size_t)n);
+        if (cudaGetLastError() != cudaSuccess || cudaMemcpy(rcp, d + n, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(root, d + 2 * (size_t)n, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = CLAW_E_CUDA;
+    }
+    cudaFree(d);
+    return rc ? clawb200::fail(rc, "claw_check_newton failed") : 0;
+}
 
 extern "C" int claw_probe_fp64(double* tflops, double* ms_best) {
     if (!tflops) return clawb200::fail(CLAW_E_INVALID, "null argument");

@@ -227,9 +227,7 @@ def main(argv=None):
         with open(args.out, "w") as f:
             json.dump(dict(summary=summary, rows=rows, losses=losses, norm=norm.values.tolist(),
                            args=vars(args)), f, indent=1)
-        np.savez(args.out.replace(".json", "_weights.npz"),
-                 **{f"w{k}": w for k, w in enumerate(net.state()["w"])},
-                 **{f"b{k}": b for k, b in enumerate(net.state()["b"])})
+        C.save_trained(args.out.replace(".json", "_trained.npz"), net, norm, alpha, K)
     return summary
 
 

@@ -285,6 +285,12 @@ int claw_batch_set_shape(claw_batch* b, int min_rows, int ctas_per_sm);
  * the reference. */
 int claw_probe_fp64(double* tflops, double* ms_best);
 
+/* Test hook: the contracted build's Newton-refined reciprocal and square root
+ * (rcp_newton, sqrt_newton: hardware estimate plus Newton-Raphson steps)
+ * evaluated on the device for n host values x, so a test can hold them to
+ * IEEE 1/x and sqrt(x).  No counterpart in the reference. */
+int claw_check_newton(const double* x, int n, double* rcp, double* root);
+
 /* Last error message of the calling thread ("" if none). */
 const char* claw_last_error(void);
 
