@@ -14,6 +14,8 @@
 // the network: block averages of a fine grid, input features, residual
 // targets, and the corrector's application with a per-tile conservative
 // projection and a positivity fallback to the plain step.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -73,18 +75,18 @@ __device__ __forceinline__ void load_halo(__nv_bfloat16* xs, const __nv_bfloat16
 }
 
 // ------------------------------------------------- forward conv, tcgen05 ---
-// The same convolution as an implicit GEMM on the 5th-generation tensor
-// cores.  A CTA (4 warps) owns an output tile of 16 rows x 8 columns: M = 128
-// pixels, N = COUT, K = 9 taps x CIN.  The halo tile (18 x 10 pixels) and the
-// weights sit in shared memory in the UMMA no-swizzle K-major layout (core
-// matrices of 8 rows x 16 bytes: 8 pixels or 8 output channels, 8 input
-// channels), so each tap's operand A is the halo tile itself with the start
-// address moved by the tap's offset: 8-row groups (tile rows) are HW*16
-// bytes apart, 8-channel chunks one halo plane apart.  One thread issues the
-// 9 x CIN/16 tcgen05.mma (M128 N=COUT K16, BF16 -> FP32) into a TMEM
-// accumulator of COUT columns and commits them to an mbarrier; each warp
-// then reads its 32 pixels (TMEM lanes) with tcgen05.ld and applies bias,
-// GELU and the stores.
+// The convolution as an implicit GEMM on the 5th-generation tensor cores.
+// A tile is 16 rows x 8 columns of output: M = 128 pixels, N = COUT, K = 9
+// taps x CIN.  The halo tile (18 x 10 pixels) and the weights sit in shared
+// memory in the UMMA no-swizzle K-major layout (core matrices of 8 rows x 16
+// bytes: 8 pixels or 8 output channels, 8 input channels), so each tap's
+// operand A is the halo tile itself with the start address moved by the
+// tap's offset: 8-row groups (tile rows) are HW*16 bytes apart, 8-channel
+// chunks one halo plane apart.  One thread issues the 9 x CIN/16
+// tcgen05.mma (M128 N=COUT K16, BF16 -> FP32) into a TMEM accumulator and
+// commits them to an mbarrier; each warp of the tile's group then reads its
+// 32 pixels (TMEM lanes) with tcgen05.ld and applies bias, GELU and the
+// stores.  These are the shared pieces; the kernel is conv3x3_fwd_tcp below.
 namespace tc {
 constexpr int TW = 8, TH = 16, HW = TW + 2, HH = TH + 2, NPX = HW * HH;
 constexpr int NTH = 128;
@@ -136,124 +138,193 @@ __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.
 
 template <int CIN, int COUT>
 __host__ __device__ constexpr int a_bytes() { return (CIN / 8) * NPX * 16; }
-template <int CIN, int COUT>
-__host__ __device__ constexpr int smem_bytes() {
-    return ((a_bytes<CIN, COUT>() + 127) / 128) * 128 + 9 * (CIN / 8) * COUT * 16 + COUT * 4;
-}
 }  // namespace tc
 
+// ------------------------------------- forward conv, tcgen05, persistent ---
+// The implicit GEMM in a persistent CTA that keeps the weights in shared
+// memory and pipelines its tiles.  The driver keeps one CTA of a TMEM-allocating kernel
+// per SM, so the CTA runs NPIPE independent pipelines, one per group of four
+// warps, each with three halo stages in shared memory and two TMEM
+// accumulators of its own.  In a pipeline, while the tensor core runs tile
+// i's 9 x CIN/16 MMAs into one accumulator, the group runs tile i-1's
+// epilogue (tcgen05.ld, bias, GELU, stores) from the other, then starts the
+// copies of tile i+2's halo into the third stage (cp.async, 16-byte chunks).
+// A stage is refilled only after the MMAs that read it have committed (the
+// epilogue's mbarrier wait); an accumulator is reused only after every
+// thread's tcgen05.ld of it has completed (tcgen05 fences around the group's
+// named barrier).  Every wait is bounded.
+namespace tcp {
+constexpr int NST = 3;    // halo stages per pipeline
+constexpr int NPIPE = 4;  // pipelines (groups of 4 warps) per CTA
+constexpr int NTH = NPIPE * tc::NTH;
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(clawb200::smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void wait_group1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(tc::NTH) : "memory");
+}
+template <int CIN>
+__host__ __device__ constexpr int stage_bytes() { return ((tc::a_bytes<CIN, 0>() + 127) / 128) * 128; }
+template <int CIN, int COUT>
+__host__ __device__ constexpr int smem_bytes() {
+    return NPIPE * NST * stage_bytes<CIN>() + 9 * (CIN / 8) * COUT * 16 + COUT * 4;
+}
+}  // namespace tcp
+
 template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
-__global__ void __launch_bounds__(tc::NTH) conv3x3_fwd_tc(const __nv_bfloat16* __restrict__ x,
-                                                           const __nv_bfloat16* __restrict__ wt,
-                                                           const float* __restrict__ bias, void* out,
-                                                           float* __restrict__ zsave, int h, int w) {
+__global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat16* __restrict__ x,
+                                                            const __nv_bfloat16* __restrict__ wt,
+                                                            const float* __restrict__ bias, void* out,
+                                                            float* __restrict__ zsave, int n, int h,
+                                                            int w) {
     using namespace tc;
     static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "UMMA M128: N in {16, 32}, K in steps of 16");
-    constexpr int KC = CIN / 8;                 // 16-byte chunks per pixel
-    constexpr int APLANE = NPX * 16;            // bytes of one chunk plane of the halo tile
-    constexpr int AOFF = ((a_bytes<CIN, COUT>() + 127) / 128) * 128;
-    constexpr int BPLANE = COUT * 16;           // bytes of one (tap, chunk) plane of the weights
+    constexpr int KC = CIN / 8;
+    constexpr int APLANE = NPX * 16;
+    constexpr int ASTAGE = tcp::stage_bytes<CIN>();
+    constexpr int BPLANE = COUT * 16;
     extern __shared__ __align__(16) unsigned char smem[];  // 16-byte alignment is all UMMA needs without swizzle
-    unsigned char* As = smem;                   // [KC][NPX][8 channels]
-    unsigned char* Bs = smem + AOFF;            // [9][KC][COUT][8 channels]
-    float* bs = reinterpret_cast<float*>(Bs + 9 * KC * BPLANE);
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[tcp::NPIPE][2];
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nimg = blockIdx.z, y0 = blockIdx.y * TH, x0 = blockIdx.x * TW;
+    const int g = warp >> 2;               // pipeline of this thread
+    const int gt = tid & (tc::NTH - 1);    // thread within the pipeline
+    const int gw = warp & 3;               // warp within the pipeline = its TMEM lane quarter
+    unsigned char* As = smem + g * tcp::NST * ASTAGE;        // this pipeline's [NST][KC][NPX][8 ch]
+    unsigned char* Bs = smem + tcp::NPIPE * tcp::NST * ASTAGE;  // [9][KC][COUT][8 ch]
+    float* bs = reinterpret_cast<float*>(Bs + 9 * KC * BPLANE);
+    const int tiles_x = w / TW, tiles_img = tiles_x * (h / TH);
+    const int ntiles = tiles_img * n;
 
-    for (int e = tid; e < NPX * KC; e += NTH) {
-        const int pix = e / KC, kc = e % KC;
-        const int gy = y0 + pix / HW - 1, gx = x0 + pix % HW - 1;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (gy >= 0 && gy < h && gx >= 0 && gx < w)
-            v = *reinterpret_cast<const uint4*>(x + (((long long)nimg * h + gy) * w + gx) * CIN + kc * 8);
-        *reinterpret_cast<uint4*>(As + kc * APLANE + pix * 16) = v;
-    }
-    for (int e = tid; e < COUT * 9 * KC; e += NTH) {  // wt[co][tap][ci] -> [tap][kc][co]
+    for (int e = tid; e < COUT * 9 * KC; e += tcp::NTH) {  // wt[co][tap][ci] -> [tap][kc][co]
         const int co = e / (9 * KC), r = e % (9 * KC), tap = r / KC, kc = r % KC;
         *reinterpret_cast<uint4*>(Bs + (tap * KC + kc) * BPLANE + co * 16) =
             *reinterpret_cast<const uint4*>(wt + ((long long)co * 9 + tap) * CIN + kc * 8);
     }
-    for (int e = tid; e < COUT; e += NTH) bs[e] = bias[e];
-    if (warp == 0) alloc(&tslot, 32);
-    if (tid == 0) {
-        clawb200::mbar_init(&bar, 1);
+    for (int e = tid; e < COUT; e += tcp::NTH) bs[e] = bias[e];
+    if (warp == 0) alloc(&tslot, 64 * tcp::NPIPE);
+    if (gt == 0) {
+        clawb200::mbar_init(&bar[g][0], 1);
+        clawb200::mbar_init(&bar[g][1], 1);
         clawb200::fence_barrier_init();
     }
-    clawb200::fence_proxy_async_smem();  // the tensor core reads what the threads wrote
+    // halo tile of tile t into stage st of this pipeline (zeros outside the image)
+    auto load_tile = [&](int t, int st) {
+        if (t >= ntiles) return;
+        const int img = t / tiles_img, r = t % tiles_img;
+        const int y0 = (r / tiles_x) * TH, x0 = (r % tiles_x) * TW;
+        unsigned char* A = As + st * ASTAGE;
+        for (int e = gt; e < NPX * KC; e += tc::NTH) {
+            const int pix = e / KC, kc = e % KC;
+            const int gy = y0 + pix / HW - 1, gx = x0 + pix % HW - 1;
+            unsigned char* dst = A + kc * APLANE + pix * 16;
+            if (gy >= 0 && gy < h && gx >= 0 && gx < w)
+                tcp::cp16(dst, x + (((long long)img * h + gy) * w + gx) * CIN + kc * 8);
+            else
+                *reinterpret_cast<uint4*>(dst) = make_uint4(0, 0, 0, 0);
+        }
+    };
+    bool ok = true;
+    // epilogue of tile t, the j-th of this pipeline (accumulator j & 1)
+    auto epilogue = [&](int t, int j) {
+        const int b = j & 1;
+        const bool done = clawb200::mbar_wait_bounded(&bar[g][b], (uint32_t)((j >> 1) & 1));
+        if (!done) {  // never expected: record it, give the MMAs a second bound, skip the stores
+            if (lane == 0) atomicOr(&g_nn_err, 1);
+            (void)clawb200::mbar_wait_bounded(&bar[g][b], (uint32_t)((j >> 1) & 1));
+            ok = false;
+        }
+        fence_after();
+        const int img = t / tiles_img, r = t % tiles_img;
+        const int y0 = (r / tiles_x) * TH, x0 = (r % tiles_x) * TW;
+        const int m = gw * 32 + lane;
+        const long long pix = ((long long)img * h + y0 + m / TW) * w + x0 + m % TW;
+        const uint32_t trow = tslot + ((uint32_t)(gw * 32) << 16) + (uint32_t)(g * 64 + b * 32);
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) {
+            uint32_t rr[16];
+            ld16(trow + c0, rr);
+            wait_ld();
+            if (!ok) continue;
+            float z[16], yv[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                z[q] = __uint_as_float(rr[q]) + bs[c0 + q];
+                yv[q] = ACT ? gelu(z[q]) : z[q];
+            }
+            if (SAVEZ) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4)
+                    *reinterpret_cast<float4*>(zsave + pix * COUT + c0 + q) =
+                        make_float4(z[q], z[q + 1], z[q + 2], z[q + 3]);
+            }
+            if (OUTF32) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4)
+                    *reinterpret_cast<float4*>(static_cast<float*>(out) + pix * COUT + c0 + q) =
+                        make_float4(yv[q], yv[q + 1], yv[q + 2], yv[q + 3]);
+            } else {
+                uint32_t pk[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    pk[q] = pack2(__float2bfloat16_rn(yv[2 * q]), __float2bfloat16_rn(yv[2 * q + 1]));
+                uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * COUT + c0);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        }
+    };
+
+    const int first = blockIdx.x * tcp::NPIPE + g, stride = gridDim.x * tcp::NPIPE;
+    load_tile(first, 0);
+    tcp::commit_group();
+    load_tile(first + stride, 1);
+    tcp::commit_group();
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = tslot;
-
-    if (tid == 0) {
-        constexpr uint32_t idesc = idesc_bf16_f32(128, COUT);
-        const uint32_t a0 = clawb200::smem_u32(As), b0 = clawb200::smem_u32(Bs);
-        uint32_t acc = 0;
+    const uint32_t tacc = tslot + (uint32_t)(g * 64);
+    constexpr uint32_t idesc = idesc_bf16_f32(128, COUT);
+    const uint32_t b0 = clawb200::smem_u32(Bs);
+    int i = 0;
+    for (int t = first; t < ntiles; t += stride, ++i) {
+        tcp::wait_group1();  // tile i's copies have landed (tile i+1's may be pending)
+        clawb200::fence_proxy_async_smem();  // the tensor core reads what the threads wrote
+        fence_before();
+        tcp::group_sync(g);
+        fence_after();
+        if (gt == 0) {
+            const uint32_t a0 = clawb200::smem_u32(As + (i % tcp::NST) * ASTAGE);
+            const uint32_t acc_addr = tacc + (uint32_t)((i & 1) * 32);
+            uint32_t acc = 0;
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-            const int ky = tap / 3, kx = tap % 3;
+            for (int tap = 0; tap < 9; ++tap) {
+                const int ky = tap / 3, kx = tap % 3;
 #pragma unroll
-            for (int kk = 0; kk < CIN / 16; ++kk) {
-                const uint64_t da = desc(a0 + (ky * HW + kx) * 16 + 2 * kk * APLANE, APLANE, HW * 16);
-                const uint64_t db = desc(b0 + (tap * KC + 2 * kk) * BPLANE, BPLANE, 128);
-                mma(tmem, da, db, idesc, acc);
-                acc = 1;
+                for (int kk = 0; kk < CIN / 16; ++kk) {
+                    const uint64_t da = desc(a0 + (ky * HW + kx) * 16 + 2 * kk * APLANE, APLANE, HW * 16);
+                    const uint64_t db = desc(b0 + (tap * KC + 2 * kk) * BPLANE, BPLANE, 128);
+                    mma(acc_addr, da, db, idesc, acc);
+                    acc = 1;
+                }
             }
+            commit(&bar[g][i & 1]);
         }
-        commit(&bar);
+        if (i > 0) epilogue(t - stride, i - 1);
+        load_tile(t + 2 * stride, (i + 2) % tcp::NST);  // the stage tile i-1's MMAs read
+        tcp::commit_group();
+        fence_before();
     }
-    bool ok = clawb200::mbar_wait_bounded(&bar, 0);
-    if (!ok) {  // never expected: record it, give the MMAs a second bound, skip the stores
-        if (lane == 0) atomicOr(&g_nn_err, 1);
-        ok = false;
-        (void)clawb200::mbar_wait_bounded(&bar, 0);
-    }
-    fence_after();
-
-    // epilogue: warp w holds TMEM lanes 32w..32w+31 = pixels 32w..32w+31
-    const int m = warp * 32 + lane;
-    const int py = y0 + m / TW, px = x0 + m % TW;
-    const long long pix = ((long long)nimg * h + py) * w + px;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-    for (int c0 = 0; c0 < COUT; c0 += 16) {
-        uint32_t r[16];
-        ld16(trow + c0, r);
-        wait_ld();
-        if (!ok) continue;
-        float z[16], yv[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            z[j] = __uint_as_float(r[j]) + bs[c0 + j];
-            yv[j] = ACT ? gelu(z[j]) : z[j];
-        }
-        if (SAVEZ) {
-#pragma unroll
-            for (int j = 0; j < 16; j += 4)
-                *reinterpret_cast<float4*>(zsave + pix * COUT + c0 + j) = make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
-        }
-        if (OUTF32) {
-#pragma unroll
-            for (int j = 0; j < 16; j += 4)
-                *reinterpret_cast<float4*>(static_cast<float*>(out) + pix * COUT + c0 + j) =
-                    make_float4(yv[j], yv[j + 1], yv[j + 2], yv[j + 3]);
-        } else {
-            uint32_t pk[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-                pk[j] = pack2(__float2bfloat16_rn(yv[2 * j]), __float2bfloat16_rn(yv[2 * j + 1]));
-            uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * COUT + c0);
-            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-        }
-    }
+    if (i > 0) epilogue(first + (i - 1) * stride, i - 1);
+    asm volatile("cp.async.wait_all;" ::: "memory");
     fence_before();
     __syncthreads();
     if (warp == 0) {
         fence_after();
-        dealloc(tmem, 32);
+        dealloc(tslot, 64 * tcp::NPIPE);
     }
 }
 
@@ -555,12 +626,23 @@ int grid_for(long long n) {
 template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
 int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, int n, int h,
                int wd, cudaStream_t s) {
-    constexpr int SM = tc::smem_bytes<CIN, COUT>();
-    auto k = conv3x3_fwd_tc<CIN, COUT, ACT, OUTF32, SAVEZ>;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess)
+    constexpr int SM = tcp::smem_bytes<CIN, COUT>();
+    auto k = conv3x3_fwd_tcp<CIN, COUT, ACT, OUTF32, SAVEZ>;
+    // one persistent CTA per SM (the driver's limit for a TMEM-allocating kernel)
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess ||
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
         return NN_E_CUDA;
-    k<<<dim3(wd / tc::TW, h / tc::TH, n), tc::NTH, SM, s>>>(
-        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), b, y, z, h, wd);
+    int dev = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tcp::NTH, SM) != cudaSuccess || per_sm < 1)
+        return NN_E_CUDA;
+    const long long ntiles = (long long)n * (h / tc::TH) * (wd / tc::TW);
+    const long long groups = (ntiles + tcp::NPIPE - 1) / tcp::NPIPE;
+    const int grid = (int)std::min<long long>(groups, (long long)nsm * per_sm);
+    k<<<grid, tcp::NTH, SM, s>>>(static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w),
+                                b, y, z, n, h, wd);
     return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
 }
 
