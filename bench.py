@@ -393,6 +393,22 @@ def other_configs(peaks, cpu=True):
                 out[key] = e
             except Exception as e:
                 out[key] = {"error": str(e)}
+    # the contracted generic kernel (the methods the characteristic kernel does
+    # not take): radial acoustics 4096^2 with transverse_waves = 1, first frame
+    try:
+        rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
+        rd.clawdata.transverse_waves = 1
+        s = Solver(rd.clawdata, solver, params, precision="fp64_fma")
+        s.set_q(q0)
+        info, st = s.advance(0.0, 0.03, 0.01)
+        s.close()
+        rate = 4096 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
+        out["radial_2d_4096_trans1_fp64_fma_generic"] = {
+            "cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
+            "kernel": "step2_kernel, contracted build (Method2D FAST)",
+            "roofline": roofline_entry(rate, 48, peaks)}
+    except Exception as e:
+        out["radial_2d_4096_trans1_fp64_fma_generic"] = {"error": str(e)}
     # dimensionally split steps (dimsp2 / dimsp3), FP64 reference order
     for key, dim, split in (("radial_2d_4096_godunov_split_fp64", 2, "godunov"),
                             ("radial_2d_4096_strang_split_fp64", 2, "strang"),
@@ -453,6 +469,28 @@ def other_configs(peaks, cpu=True):
             out[key] = e
         except Exception as e:
             out[key] = {"error": str(e)}
+    # the learned corrector (the shipped network) on two unseen seeds: coarse
+    # 256^2 corrected / plain against the block-averaged 1024^2 FP64 run
+    try:
+        from classic_b200 import corrector as C
+        net, norm, alpha, interval = C.load_trained(
+            os.path.join(ROOT, "classic_b200", "data", "corrector_euler_256.npz"))
+        pl, co, tf_, tk_ = [], [], 0.0, 0.0
+        for seed in (61000, 61001):
+            qc, _, _ = C.plain_run(seed, 256)
+            qk, _, _, tk = C.corrected_run(net, norm, seed, n=256, alpha=alpha, interval=interval)
+            qf, _, tf = C.plain_run(seed, 1024)
+            ref = C.block_average(qf, 4)
+            pl.append(C.l1_error(qc, ref))
+            co.append(C.l1_error(qk, ref))
+            tf_ += tf
+            tk_ += tk
+        out["corrector_euler_256"] = {
+            "l1_vs_fine_plain": float(np.mean(pl)), "l1_vs_fine_corrected": float(np.mean(co)),
+            "wall_fine_over_corrected": tf_ / tk_, "alpha": alpha, "interval": interval,
+            "note": "2 unseen seeds; 200 held-out seeds in profiles/corrector_euler_256.md"}
+    except Exception as e:
+        out["corrector_euler_256"] = {"error": str(e)}
     return out
 
 
