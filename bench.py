@@ -428,9 +428,10 @@ def other_configs(peaks, cpu=True):
             info, st = s.advance(0.0, t1, dt0)
             s.close()
             rate = cells * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
+            kern = "split2_kernel_fp64" if split == "godunov" and dim == 2 else None
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
-                        "roofline": roofline_entry(rate, nbytes, peaks)}
+                        "roofline": roofline_entry(rate, nbytes, peaks, kern, fp64_peak)}
         except Exception as e:
             out[key] = {"error": str(e)}
     sizes = problems.euler_ensemble_sizes(256, seed=0)
@@ -476,6 +477,7 @@ def other_configs(peaks, cpu=True):
         net, norm, alpha, interval = C.load_trained(
             os.path.join(ROOT, "classic_b200", "data", "corrector_euler_256.npz"))
         pl, co, tf_, tk_ = [], [], 0.0, 0.0
+        C.corrected_run(net, norm, 61999, n=256, alpha=alpha, interval=interval)  # warm-up
         for seed in (61000, 61001):
             qc, _, _ = C.plain_run(seed, 256)
             qk, _, _, tk = C.corrected_run(net, norm, seed, n=256, alpha=alpha, interval=interval)
