@@ -393,22 +393,26 @@ def other_configs(peaks, cpu=True):
                 out[key] = e
             except Exception as e:
                 out[key] = {"error": str(e)}
-    # the contracted generic kernel (the methods the characteristic kernel does
-    # not take): radial acoustics 4096^2 with transverse_waves = 1, first frame
-    try:
-        rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
-        rd.clawdata.transverse_waves = 1
-        s = Solver(rd.clawdata, solver, params, precision="fp64_fma")
-        s.set_q(q0)
-        info, st = s.advance(0.0, 0.03, 0.01)
-        s.close()
-        rate = 4096 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
-        out["radial_2d_4096_trans1_fp64_fma_generic"] = {
-            "cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
-            "kernel": "step2_kernel, contracted build (Method2D FAST)",
-            "roofline": roofline_entry(rate, 48, peaks)}
-    except Exception as e:
-        out["radial_2d_4096_trans1_fp64_fma_generic"] = {"error": str(e)}
+    # other methods of the same workload in the contracted build: transverse 1
+    # (characteristic kernel), and MC / van Leer on the two waves (the
+    # contracted generic kernel); 4096^2, first frame
+    for key, trans, lims, kern in (
+            ("radial_2d_4096_trans1_fp64_fma", 1, ["mc", "mc"], "step2_char_kernel (order 2, transverse 1)"),
+            ("radial_2d_4096_mixed_limiters_fp64_fma", 2, ["mc", "vanleer"],
+             "step2_kernel, contracted build (Method2D FAST)")):
+        try:
+            rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
+            rd.clawdata.transverse_waves = trans
+            rd.clawdata.limiter = lims
+            s = Solver(rd.clawdata, solver, params, precision="fp64_fma")
+            s.set_q(q0)
+            info, st = s.advance(0.0, 0.03, 0.01)
+            s.close()
+            rate = 4096 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
+            out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
+                        "kernel": kern, "roofline": roofline_entry(rate, 48, peaks)}
+        except Exception as e:
+            out[key] = {"error": str(e)}
     # dimensionally split steps (dimsp2 / dimsp3), FP64 reference order
     for key, dim, split in (("radial_2d_4096_godunov_split_fp64", 2, "godunov"),
                             ("radial_2d_4096_strang_split_fp64", 2, "strang"),

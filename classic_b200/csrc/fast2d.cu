@@ -12,7 +12,7 @@ namespace clawb200 {
 
 namespace {
 
-template <typename real, int LIM, int BCM>
+template <typename real, int LIM, int BCM, int ORD, int TRN>
 struct CharRunner : Runner {
     CharArgs<real> args;
     int grid = 1, smem = 0;
@@ -43,12 +43,12 @@ struct CharRunner : Runner {
             if (rc) return rc;
         }
         smem = R::SMEM;
-        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, BCM>,
+        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, BCM, ORD, TRN>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM>,
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM, ORD, TRN>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
         const long long full = (long long)nsm * per_sm * WARPS2D;
@@ -59,15 +59,30 @@ struct CharRunner : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_char_kernel<real, LIM, BCM><<<grid, 32 * WARPS2D, smem, s>>>(args);
+        step2_char_kernel<real, LIM, BCM, ORD, TRN><<<grid, 32 * WARPS2D, smem, s>>>(args);
         return cudaGetLastError();
     }
 };
 
+// (order, transverse_waves): MC at order 2 has its own instantiations; the
+// other limiters read the limiter at run time (order 1 uses none).
 template <typename real, int BCM>
-std::unique_ptr<Runner> pick_lim(int lim) {
-    if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, BCM>());
-    return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM>());
+std::unique_ptr<Runner> pick_lim(int lim, int order, int trans) {
+    if (order == 2 && trans == 2) {
+        if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, BCM, 2, 2>());
+        return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM, 2, 2>());
+    }
+    if (order == 2 && trans == 1) {
+        if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, BCM, 2, 1>());
+        return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM, 2, 1>());
+    }
+    if (order == 2 && trans == 0) {
+        if (lim == 4) return std::unique_ptr<Runner>(new CharRunner<real, 4, BCM, 2, 0>());
+        return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM, 2, 0>());
+    }
+    if (order == 1 && trans == 1) return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM, 1, 1>());
+    if (order == 1 && trans == 0) return std::unique_ptr<Runner>(new CharRunner<real, -1, BCM, 1, 0>());
+    return nullptr;
 }
 
 template <typename real>
@@ -75,16 +90,18 @@ std::unique_ptr<Runner> pick(const claw_config& cfg) {
     const bool px = cfg.bc_lower[0] == BC_PERIODIC || cfg.bc_upper[0] == BC_PERIODIC;
     bool extrap = true;
     for (int d = 0; d < 2; ++d) extrap = extrap && cfg.bc_lower[d] == BC_EXTRAP && cfg.bc_upper[d] == BC_EXTRAP;
-    if (px) return pick_lim<real, CHAR_BC_PERX>(cfg.limiter[0]);
-    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(cfg.limiter[0]);
-    return pick_lim<real, CHAR_BC_WALLS>(cfg.limiter[0]);
+    const int o = cfg.order, tr = cfg.transverse_waves;
+    if (px) return pick_lim<real, CHAR_BC_PERX>(cfg.limiter[0], o, tr);
+    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(cfg.limiter[0], o, tr);
+    return pick_lim<real, CHAR_BC_WALLS>(cfg.limiter[0], o, tr);
 }
 
 }  // namespace
 
 std::unique_ptr<Runner> make_char_runner(const claw_config& cfg) {
     if (cfg.solver_id != CLAW_SOLVER_ACOUSTICS_2D || cfg.num_dim != 2) return nullptr;
-    if (cfg.order != 2 || cfg.transverse_waves != 2 || cfg.capa_index != 0 || cfg.use_fwaves)
+    if (cfg.order < 1 || cfg.order > 2 || cfg.transverse_waves < 0 || cfg.transverse_waves > cfg.order ||
+        cfg.capa_index != 0 || cfg.use_fwaves)
         return nullptr;
     for (int k = 1; k < cfg.num_waves; ++k)
         if (cfg.limiter[k] != cfg.limiter[0]) return nullptr;

@@ -1,6 +1,7 @@
-"""The contracted build of the generic 2D kernel and of the batch
-(precision "fp64_fma" for every method and solver the characteristic-variable
-kernel does not serve) against the CPU restatement.
+"""The contracted builds (precision "fp64_fma") against the CPU restatement:
+the characteristic-variable kernel at every (order, transverse_waves) it
+takes, and the generic kernel and the batch for what it does not take (mixed
+limiters, other solvers, capacity).
 
 This build contracts multiplies and adds into FMAs and replaces IEEE division
 and sqrt by Newton-refined reciprocals and roots (about an ulp), so it is not
@@ -33,11 +34,16 @@ def _pair(rd, solver, params, q0, aux=None):
     return g, o
 
 
-@pytest.mark.parametrize("lim", ["minmod", "superbee", "vanleer", "mc"])
-@pytest.mark.parametrize("order,trans", [(1, 1), (2, 1), (2, 0)])
-def test_acoustics_generic_fast(lim, order, trans):
+@pytest.mark.parametrize("lim", ["minmod", "superbee", "vanleer", "mc", ("mc", "vanleer")])
+@pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 1), (2, 0), (2, 2)])
+@pytest.mark.parametrize("bc", [("wall", "extrap", "periodic", "periodic"), ("extrap",) * 4,
+                                ("periodic", "periodic", "wall", "wall")])
+def test_acoustics_fast(lim, order, trans, bc):
+    """One limiter: the characteristic kernel; two different ones: the
+    contracted generic kernel."""
     rd, solver, params, q0, _ = problems.random_acoustics_2d(
-        45, 38, seed=9, limiter=lim, order=order, trans=trans, bc=("wall", "extrap", "periodic", "periodic"))
+        45, 38, seed=9, limiter="mc", order=order, trans=trans, bc=bc)
+    rd.clawdata.limiter = list(lim) if isinstance(lim, tuple) else [lim, lim]
     g, o = _pair(rd, solver, params, q0)
     for _ in range(20):
         cg, co = g.step(0.004), o.step(0.004)

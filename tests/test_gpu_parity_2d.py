@@ -231,6 +231,21 @@ def test_config2_1024_against_oracle_50_steps():
             assert np.all(d <= 1e-12), d
 
 
+@pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 0), (2, 1)])
+def test_fast_fp32_methods_track_fp64(order, trans):
+    """The FP32 characteristic kernel at the other (order, transverse_waves)
+    combinations, every BC class, against the CPU restatement."""
+    for bc in BCS:
+        rd, solver, params, q0, _ = problems.random_acoustics_2d(53, 41, seed=4, bc=bc, order=order,
+                                                                trans=trans, limiter="vanleer")
+        g, o = _pair(rd, solver, params, q0, precision="fp32")
+        for _ in range(10):
+            cg, co = g.step(0.004), o.step(0.004)
+            assert abs(cg - co) <= 1e-7 * co
+        assert np.all(rel_diff(g.get_q(), o.get_q()) < 1e-5)
+        g.close()
+
+
 def test_fast_fp32_tracks_fp64_all_bcs():
     for bc in BCS:
         rd, solver, params, q0, _ = problems.random_acoustics_2d(70, 33, seed=2, bc=bc)
