@@ -393,13 +393,13 @@ def other_configs(peaks, cpu=True):
                 out[key] = e
             except Exception as e:
                 out[key] = {"error": str(e)}
-    # other methods of the same workload in the contracted build: transverse 1
-    # (characteristic kernel), and MC / van Leer on the two waves (the
-    # contracted generic kernel); 4096^2, first frame
+    # other methods of the same workload in the contracted build (characteristic
+    # kernel): transverse 1, and MC / van Leer on the two waves (the limiters
+    # read at run time); 4096^2, first frame
     for key, trans, lims, kern in (
             ("radial_2d_4096_trans1_fp64_fma", 1, ["mc", "mc"], "step2_char_kernel (order 2, transverse 1)"),
             ("radial_2d_4096_mixed_limiters_fp64_fma", 2, ["mc", "vanleer"],
-             "step2_kernel, contracted build (Method2D FAST)")):
+             "step2_char_kernel (limiters read at run time)")):
         try:
             rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
             rd.clawdata.transverse_waves = trans

@@ -105,7 +105,7 @@ struct CharArgs {
     long long ld, fstride;
     int mx, my, nstrips;
     int bc[4];
-    int lim;
+    int lim, lim2;  // limiters of wave 1 (speed -c) and wave 2 (speed +c), mthlim(1:2)
     double dx, dy;
     // Work items: row block b (brows rows) of strip s, item = b * nstrips + s,
     // so the warps at work on one row block hold adjacent strips and stream
@@ -362,12 +362,12 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
                 const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
                 // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
-                real Fp0 = real(0), Fu0 = real(0), Fp1 = real(0), Fu1 = real(0);
+                [[maybe_unused]] real Fp0 = real(0), Fu0 = real(0), Fp1 = real(0), Fu1 = real(0);
                 if constexpr (ORD == 2) {
                     const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
-                    const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim);
+                    const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim2);
                     const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
-                    const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim);
+                    const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim2);
                     Fp0 = fxp * (l2_0 - l1_0);
                     Fu0 = fxu * (l1_0 + l2_0);
                     Fp1 = fxp * (l2_1 - l1_1);
@@ -382,7 +382,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                     if constexpr (TRN == 2) return fma(cZ, a, real(-2) * F);
                     else return cZ * a;
                 };
-                real FpR = real(0), FuR = real(0);
+                [[maybe_unused]] real FpR = real(0), FuR = real(0);
                 if constexpr (ORD == 2) {
                     FpR = __shfl_down_sync(FULL, Fp0, 1);
                     FuR = __shfl_down_sync(FULL, Fu0, 1);
@@ -432,7 +432,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                     Fvy[k] = real(0);
                     if constexpr (ORD == 2) {
                         const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
-                        const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim); // upwind t-1
+                        const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim2); // upwind t-1
                         Fpy[k] = fyp * (b2 - b1);
                         Fvy[k] = fyv * (b1 + b2);
                     }

@@ -8,6 +8,10 @@
 #include "char2d.cuh"
 #include "host.h"
 
+#ifndef CLAW_CHAR_MIN_ROWS
+#define CLAW_CHAR_MIN_ROWS 8  // fewest rows of a work item (small grids: more items, more warps)
+#endif
+
 namespace clawb200 {
 
 namespace {
@@ -35,6 +39,7 @@ struct CharRunner : Runner {
         args.bc[2] = cfg.bc_lower[1];
         args.bc[3] = cfg.bc_upper[1];
         args.lim = cfg.limiter[0];
+        args.lim2 = cfg.num_waves > 1 ? cfg.limiter[1] : cfg.limiter[0];
         args.dx = g.dx;
         args.dy = g.dy;
         args.ctl = g.ctl;
@@ -52,7 +57,7 @@ struct CharRunner : Runner {
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
         const long long full = (long long)nsm * per_sm * WARPS2D;
-        const int nw = row_blocks(full, args.nstrips, g.my, 32, &args.brows, &args.nblocks);
+        const int nw = row_blocks(full, args.nstrips, g.my, CLAW_CHAR_MIN_ROWS, &args.brows, &args.nblocks);
         grid = (nw + WARPS2D - 1) / WARPS2D;
         args.nwarps = nw;
         return 0;
@@ -91,9 +96,11 @@ std::unique_ptr<Runner> pick(const claw_config& cfg) {
     bool extrap = true;
     for (int d = 0; d < 2; ++d) extrap = extrap && cfg.bc_lower[d] == BC_EXTRAP && cfg.bc_upper[d] == BC_EXTRAP;
     const int o = cfg.order, tr = cfg.transverse_waves;
-    if (px) return pick_lim<real, CHAR_BC_PERX>(cfg.limiter[0], o, tr);
-    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(cfg.limiter[0], o, tr);
-    return pick_lim<real, CHAR_BC_WALLS>(cfg.limiter[0], o, tr);
+    // one limiter for both waves can be compiled in; two different ones are read at run time
+    const int lim = cfg.limiter[0] == cfg.limiter[1] ? cfg.limiter[0] : -1;
+    if (px) return pick_lim<real, CHAR_BC_PERX>(lim, o, tr);
+    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(lim, o, tr);
+    return pick_lim<real, CHAR_BC_WALLS>(lim, o, tr);
 }
 
 }  // namespace
@@ -103,8 +110,7 @@ std::unique_ptr<Runner> make_char_runner(const claw_config& cfg) {
     if (cfg.order < 1 || cfg.order > 2 || cfg.transverse_waves < 0 || cfg.transverse_waves > cfg.order ||
         cfg.capa_index != 0 || cfg.use_fwaves)
         return nullptr;
-    for (int k = 1; k < cfg.num_waves; ++k)
-        if (cfg.limiter[k] != cfg.limiter[0]) return nullptr;
+    if (cfg.num_waves != 2) return nullptr;
     if (cfg.precision == CLAW_FP32) return pick<float>(cfg);
     if (cfg.precision == CLAW_FP64_FMA) return pick<double>(cfg);
     return nullptr;

@@ -30,6 +30,10 @@ struct Runner {
     virtual int launches_per_step() const { return 1; }
 };
 
+#ifndef CLAW_STEP2_MIN_ROWS
+#define CLAW_STEP2_MIN_ROWS 16  // fewest rows of a work item of the generic and split 2D kernels
+#endif
+
 // Row-block-major work items of a 2D column-march kernel: as many row blocks
 // as fill `full` resident warps with one item (strip x row block) each, every
 // block at least min_rows high.  Returns the warps to launch.

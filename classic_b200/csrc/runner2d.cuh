@@ -67,7 +67,7 @@ struct Runner2D : Runner {
         if (per_sm < 1) return fail(CLAW_E_CUDA, "step2 kernel cannot be resident on an SM");
         args.units = (long long)args.nstrips * g.my;
         const long long full = (long long)nsm * per_sm * WARPS2D;
-        const int nw = row_blocks(full, args.nstrips, g.my, 32, &args.brows, &args.nblocks);
+        const int nw = row_blocks(full, args.nstrips, g.my, CLAW_STEP2_MIN_ROWS, &args.brows, &args.nblocks);
         grid = (nw + WARPS2D - 1) / WARPS2D;
         args.nwarps = nw;
         return 0;

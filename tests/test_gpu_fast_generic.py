@@ -1,7 +1,7 @@
 """The contracted builds (precision "fp64_fma") against the CPU restatement:
-the characteristic-variable kernel at every (order, transverse_waves) it
-takes, and the generic kernel and the batch for what it does not take (mixed
-limiters, other solvers, capacity).
+the characteristic-variable kernel for constant-coefficient acoustics (every
+order, transverse_waves and pair of limiters), and the generic kernel and the
+batch for the rest (other solvers, capacity).
 
 This build contracts multiplies and adds into FMAs and replaces IEEE division
 and sqrt by Newton-refined reciprocals and roots (about an ulp), so it is not
@@ -39,8 +39,8 @@ def _pair(rd, solver, params, q0, aux=None):
 @pytest.mark.parametrize("bc", [("wall", "extrap", "periodic", "periodic"), ("extrap",) * 4,
                                 ("periodic", "periodic", "wall", "wall")])
 def test_acoustics_fast(lim, order, trans, bc):
-    """One limiter: the characteristic kernel; two different ones: the
-    contracted generic kernel."""
+    """The characteristic kernel, with one limiter compiled in or a limiter
+    per wave read at run time."""
     rd, solver, params, q0, _ = problems.random_acoustics_2d(
         45, 38, seed=9, limiter="mc", order=order, trans=trans, bc=bc)
     rd.clawdata.limiter = list(lim) if isinstance(lim, tuple) else [lim, lim]
