@@ -228,7 +228,7 @@ int claw_totals(claw_handle* h, double* totals);
  *   aux         : device array [num_aux][my+4][aux_ld] or NULL
  *   stream      : a cudaStream_t (NULL = the default stream); the call waits
  *                 for it and returns the Courant number in *cfl
- * The step kernel's scratch (its 256-byte control block) is a static device
+ * The step kernel's scratch (its control block) lives in a 256-byte static device
  * array of the library; every call looks up its device address on the
  * current device and resets it, and calls that overlap on the GPU race on
  * it.  Requests whose scratch would exceed the 256-byte maximum are rejected
