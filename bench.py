@@ -13,12 +13,18 @@ cells / device time.
              host->device copy of q (pinned) before and the device->host copy
              after every frame inside the timed region
   roofline : the step kernel's algorithmic bytes (read q + write q,
-             48 B per cell-update) / its average launch time, CUDA events on
-             the library's stream over the timed region
+             48 B per cell-update) / its time per executed step (CUDA events
+             on the library's stream over the timed frames / accepted +
+             rejected steps); traffic from the kernel's ncu capture
   variants : the same frames on the reference-order FP64 kernel (bit-identical
              to the CPU restatement) and on the FP32 path
   cpu_baseline : the CPU restatement of step2/flux2 (the oracle) timed on
-             this host on a bounded sample (whole 4096^2 steps)
+             this host on a bounded sample (whole 4096^2 steps; one core as
+             the reference's serial step2, and all cores threaded beside it)
+  other_configs : the other workloads (1D, 2D 1024^2, 3D 256^3 / 512^3, the
+             split steps, the Euler ensemble, the learned corrector), each
+             with its roofline and, where the reference has a CPU path, a
+             CPU baseline
 
 The headline arithmetic is FP64 with fused multiply-adds in characteristic
 variables (precision "fp64_fma"): the same algorithm and dt sequence as the
@@ -26,8 +32,8 @@ reference-order path, within 1e-12 relative of it over the full run.
 
 --impl reference times that CPU restatement alone on the same metric.
 Under torchrun with N > 1 each rank runs an independent replica (the
-north-star workload does not shard), value = all ranks' cell-updates / max
-time over ranks.
+workload fits one GPU and does not shard), value = all ranks' cell-updates /
+max time over ranks.
 """
 from __future__ import annotations
 
