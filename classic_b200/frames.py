@@ -6,6 +6,8 @@ in-place flush of |q| < 1e-99 (src/2d/out2.f:70); the header carries grid
 number, AMR level, mx, my, xlow, ylow, dx, dy, and fort.t carries time, meqn,
 ngrids, maux, ndim, nghost and the format name.  ``read_frame`` parses a
 frame back (the restart path of src/2d/restart2.f reads the same layout).
+fort.info gets one record per output frame with the claw call's dt / CFL /
+step returns (``start_info``, ``append_info``).
 """
 from __future__ import annotations
 
@@ -39,6 +41,41 @@ def fortran_e(v: float, w: int = 26, d: int = 16) -> str:
 
 def _i5(n: int) -> str:
     return f"{n:5d}"
+
+
+def fortran_d(v: float, w: int = 15, d: int = 4) -> str:
+    """Fortran Dw.d edit descriptor (gfortran form: 0.dddD+ee)."""
+    return fortran_e(v, w, d).replace("E", "D")
+
+
+def fortran_i(n: int, w: int) -> str:
+    """Fortran Iw: right-justified, or w asterisks when the value does not fit."""
+    s = str(int(n))
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def start_info(outdir: str) -> str:
+    """Create (truncate) fort.info, as claw2ez opens it with status='unknown'
+    at the start of a run (src/2d/claw2ez.f:34; claw1ez.f:28, claw3ez.f:46)."""
+    path = os.path.join(outdir, "fort.info")
+    open(path, "w").close()
+    return path
+
+
+def append_info(outdir: str, tend: float, info: int, stats: dict) -> None:
+    """Append one output frame's record to fort.info: claw2ez's format 1010
+    (src/2d/claw2ez.f:308-309, 319-322) with dtv(3:5), cflv(3:4) and nv(2)
+    of the claw call that reached the frame."""
+    rec = ("tend =" + fortran_d(tend) + "\n"
+           "info =" + fortran_i(info, 5) + "\n"
+           "smallest dt =" + fortran_d(stats["dt_min"]) + "\n"
+           "largest dt =" + fortran_d(stats["dt_max_taken"]) + "\n"
+           "last dt =" + fortran_d(stats["dt_next"]) + "\n"
+           "largest cfl =" + fortran_d(stats["cfl_max_seen"]) + "\n"
+           "last cfl =" + fortran_d(stats["cfl_last"]) + "\n"
+           "steps taken =" + fortran_i(stats["steps_taken"], 4) + "\n\n")
+    with open(os.path.join(outdir, "fort.info"), "a") as f:
+        f.write(rec)
 
 
 def flush_tiny(q: np.ndarray) -> np.ndarray:

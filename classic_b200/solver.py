@@ -245,7 +245,8 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray | None,
     (frame 0 included when output_t0); raises on a nonzero info.
 
     With ``outdir`` every output frame is also written as fort.qNNNN /
-    fort.tNNNN (out2.f's format), and a restart run (clawdata.restart)
+    fort.tNNNN (out2.f's format) and gets a fort.info record (the dt / CFL /
+    step returns of the claw call that reached it), and a restart run (clawdata.restart)
     reads its q and start time from the frame clawdata.restart_file names in
     that directory and continues the frame numbering from it, as claw2ez does
     (src/2d/claw2ez.f:236-271; dtout keeps the data's t0)."""
@@ -273,6 +274,8 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray | None,
     if aux is not None:
         s.set_aux(aux)
     frames = []
+    if outdir is not None:
+        _frames.start_info(outdir)
     if not rest and (cd.output_t0 or int(cd.output_style) == 2):
         f0 = Frame(0, t0, q.copy())
         if outdir is not None:
@@ -313,6 +316,7 @@ def run(rundata, solver: str, params: dict | None, q0: np.ndarray | None,
             if outdir is not None:
                 _frames.write_frame(outdir, iframe, tend, q, lower, dxs, maux=int(cd.num_aux),
                                     nghost=int(cd.num_ghost))
+                _frames.append_info(outdir, tend, info, st)
             if on_frame:
                 on_frame(fr)
             if keep_frames:

@@ -48,3 +48,39 @@ def test_2d_layout_matches_out2(tmp_path):
     assert tl[0] == frames.fortran_e(0.5) + "    time"
     assert tl[1] == "    2                 meqn"
     assert tl[4] == "    2                 ndim"
+
+
+def test_fort_info_records(tmp_path):
+    """fort.info: claw2ez's format 1010 record (src/2d/claw2ez.f:308-309,
+    319-322) per output frame, D15.4 reals, I5 info, I4 step count (asterisks
+    when it does not fit); start_info truncates the file as the OPEN at the
+    start of a run does."""
+    out = str(tmp_path)
+    path = frames.start_info(out)
+    with open(path, "a") as f:
+        f.write("stale\n")
+    frames.start_info(out)
+    st = {"dt_min": 1.25e-3, "dt_max_taken": 2.5e-3, "dt_next": 2.4e-3,
+          "cfl_max_seen": 0.9, "cfl_last": 0.8999, "steps_taken": 40}
+    frames.append_info(out, 0.1, 0, st)
+    frames.append_info(out, 0.2, 11, dict(st, steps_taken=12345, dt_min=-0.0))
+    text = open(path).read()
+    assert text == (
+        "tend =     0.1000D+00\n"
+        "info =    0\n"
+        "smallest dt =     0.1250D-02\n"
+        "largest dt =     0.2500D-02\n"
+        "last dt =     0.2400D-02\n"
+        "largest cfl =     0.9000D+00\n"
+        "last cfl =     0.8999D+00\n"
+        "steps taken =  40\n"
+        "\n"
+        "tend =     0.2000D+00\n"
+        "info =   11\n"
+        "smallest dt =    -0.0000D+00\n"
+        "largest dt =     0.2500D-02\n"
+        "last dt =     0.2400D-02\n"
+        "largest cfl =     0.9000D+00\n"
+        "last cfl =     0.8999D+00\n"
+        "steps taken =****\n"
+        "\n")

@@ -3,6 +3,7 @@
 The FP64 path is built with separately rounded multiplies and adds in the
 reference's order of operations, so the comparison is bit-for-bit (value
 equality, +0 == -0) for q, the Courant number and the dt sequence."""
+import os
 import numpy as np
 import pytest
 
@@ -271,6 +272,14 @@ def test_frames_written_and_restart_continues(tmp_path):
     for k in range(4):
         t, q = F.read_frame(out, k)
         assert abs(t - fr[k].t) <= 1e-15 and np.allclose(q, fr[k].q, rtol=1e-15, atol=1e-99)
+    info_lines = open(os.path.join(out, "fort.info")).read().split("\n")
+    assert len(info_lines) == 3 * 9 + 1
+    for k in range(1, 4):
+        rec = info_lines[(k - 1) * 9:k * 9]
+        assert rec[0] == "tend =" + F.fortran_d(fr[k].t)
+        assert rec[1] == "info =    0"
+        assert rec[4] == "last dt =" + F.fortran_d(fr[k].stats["dt_next"])
+        assert rec[7] == "steps taken =" + F.fortran_i(fr[k].stats["steps_taken"], 4)
     rd.clawdata.restart = True
     rd.clawdata.restart_file = "fort.q0001"
     fr2 = run(rd, solver, params, None, outdir=out)
