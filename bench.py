@@ -399,24 +399,32 @@ def other_configs(peaks, cpu=True):
                 out[key] = e
             except Exception as e:
                 out[key] = {"error": str(e)}
-    # other methods of the same workload in the contracted build (characteristic
-    # kernel): transverse 1, and MC / van Leer on the two waves (the limiters
-    # read at run time); 4096^2, first frame
-    for key, trans, lims, kern in (
-            ("radial_2d_4096_trans1_fp64_fma", 1, ["mc", "mc"], "step2_char_kernel (order 2, transverse 1)"),
-            ("radial_2d_4096_mixed_limiters_fp64_fma", 2, ["mc", "vanleer"],
-             "step2_char_kernel (limiters read at run time)")):
+    # other methods of the same workload on the characteristic kernel: transverse
+    # 1; minmod, superbee and van Leer compiled in (FP64 contracted and FP32);
+    # MC / van Leer on the two waves (read at run time).  4096^2; a first frame
+    # (t 0 -> 0.02) warms up, the next (0.02 -> 0.05) is timed.
+    char_kern = "step2_char_kernel"
+    for key, trans, lims, prec, kern in (
+            ("radial_2d_4096_trans1_fp64_fma", 1, ["mc", "mc"], "fp64_fma", char_kern + " (order 2, transverse 1)"),
+            ("radial_2d_4096_minmod_fp64_fma", 2, ["minmod", "minmod"], "fp64_fma", char_kern),
+            ("radial_2d_4096_superbee_fp64_fma", 2, ["superbee", "superbee"], "fp64_fma", char_kern),
+            ("radial_2d_4096_vanleer_fp64_fma", 2, ["vanleer", "vanleer"], "fp64_fma", char_kern),
+            ("radial_2d_4096_vanleer_fp32", 2, ["vanleer", "vanleer"], "fp32", char_kern),
+            ("radial_2d_4096_mixed_limiters_fp64_fma", 2, ["mc", "vanleer"], "fp64_fma",
+             char_kern + " (limiters read at run time)")):
         try:
             rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
             rd.clawdata.transverse_waves = trans
             rd.clawdata.limiter = lims
-            s = Solver(rd.clawdata, solver, params, precision="fp64_fma")
+            s = Solver(rd.clawdata, solver, params, precision=prec)
             s.set_q(q0)
-            info, st = s.advance(0.0, 0.03, 0.01)
+            info, st = s.advance(0.0, 0.02, 0.01)
+            info, st = s.advance(0.02, 0.05, st["dt_next"])
             s.close()
             rate = 4096 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
-                        "kernel": kern, "roofline": roofline_entry(rate, 48, peaks)}
+                        "kernel": kern, "limiters": lims,
+                        "roofline": roofline_entry(rate, 48 if prec != "fp32" else 24, peaks)}
         except Exception as e:
             out[key] = {"error": str(e)}
     # dimensionally split steps (dimsp2 / dimsp3), FP64 reference order

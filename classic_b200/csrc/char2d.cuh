@@ -39,14 +39,6 @@ __device__ __forceinline__ float sign_times(float x, float s) {
     return __int_as_float(__float_as_int(x) ^ (__float_as_int(s) & (int)0x80000000u));
 }
 
-// phi(r) * a of inlinelimiter.f90:71-97 for the strength ratio r = n / a
-// (n = upwind neighbour's strength).  For minmod, superbee and MC the product
-// has an exact division-free form: with A = |a| and N = n sign(a),
-//   minmod   phi a = sign(a) max(0, min(A, N))
-//   superbee phi a = sign(a) max(0, min(A, 2N), min(2A, N))
-//   MC       phi a = sign(a) max(0, min(2A, 2N, (A+N)/2))
-// (multiply phi's arguments by a, reversing min/max when a < 0).  a == 0 gives
-// 0, as the reference skips a zero wave.  Other limiters use the ratio.
 // MC in FP64 by compare-and-select on magnitudes.  When a and n share a
 // sign, phi a = sign(a) 2 min(|a|, |n|, (|a|+|n|)/4); otherwise 0.  Same value
 // as the min/max form below (every candidate is formed by the same
@@ -75,27 +67,39 @@ __device__ __forceinline__ real mx2(real x, real y) {
     else return fmaxf(x, y);
 }
 
+// phi(r) * a of inlinelimiter.f90:71-97 (philim.f90 of src/2d) for the
+// strength ratio r = n / a (n = upwind neighbour's strength), written with
+// A = |a| and N = n sign(a), so that r = N / A (multiply phi's arguments by
+// a, reversing min/max when a < 0):
+//   minmod    sign(a) max(0, min(A, N))
+//   superbee  sign(a) max(0, min(A, 2N), min(2A, N))
+//   van Leer  sign(a) 2AN / (A + N) for N > 0, else 0   (one reciprocal)
+//   MC        sign(a) max(0, min(2A, 2N, (A + N) / 2))
+//   Beam-Warming  n
+// a == 0 gives 0, as the reference skips a zero wave.
 // LIM >= 0 fixes the limiter at compile time; LIM = -1 reads it at run time
-// (a warp-uniform branch), still taking the division-free forms for minmod,
-// superbee and MC.
+// (a warp-uniform branch).
 template <typename real, int LIM>
 __device__ __forceinline__ real limited_strength(real a, real n, int lim_rt) {
     const int lim = LIM >= 0 ? LIM : lim_rt;
-    if (lim == 1 || lim == 2 || lim == 4) {
-        if constexpr (sizeof(real) == 8) {
-            if (lim == 4) return mc_strength(a, n);
-        }
-        const real A = fabs(a), N = sign_times(n, a);
-        real m;
-        if (lim == 1) m = mn2(A, N);
-        else if (lim == 2) m = mx2(mn2(A, real(2) * N), mn2(real(2) * A, N));
-        else m = real(2) * mn2(mn2(A, N), real(0.25) * (A + N));
-        return sign_times(mx2(real(0), m), a);
+    if constexpr (sizeof(real) == 8) {
+        if (lim == 4) return mc_strength(a, n);
     }
     if (lim == 0) return a;
-    const real inv = rcp_newton(a != real(0) ? a : real(1));
-    const real r = n * inv;
-    return phi_limiter<real>(lim, r) * a;
+    if (lim == 5) return a != real(0) ? n : real(0);
+    const real A = fabs(a), N = sign_times(n, a);
+    real m;
+    if (lim == 1) {
+        m = mn2(A, N);
+    } else if (lim == 2) {
+        m = mx2(mn2(A, real(2) * N), mn2(real(2) * A, N));
+    } else if (lim == 3) {
+        const real pos = N > real(0) ? N : real(0);
+        m = real(2) * A * pos * rcp_newton(A + (N > real(0) ? N : real(1)));
+    } else {
+        m = real(2) * mn2(mn2(A, N), real(0.25) * (A + N));
+    }
+    return sign_times(mx2(real(0), m), a);
 }
 
 template <typename real>

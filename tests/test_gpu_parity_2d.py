@@ -232,13 +232,16 @@ def test_config2_1024_against_oracle_50_steps():
             assert np.all(d <= 1e-12), d
 
 
-@pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 0), (2, 1)])
-def test_fast_fp32_methods_track_fp64(order, trans):
-    """The FP32 characteristic kernel at the other (order, transverse_waves)
-    combinations, every BC class, against the CPU restatement."""
+@pytest.mark.parametrize("lim", ["minmod", "superbee", "vanleer", ("mc", "minmod"), ("vanleer", "none")])
+@pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 0), (2, 1), (2, 2)])
+def test_fast_fp32_methods_track_fp64(order, trans, lim):
+    """The FP32 characteristic kernel at every (order, transverse_waves)
+    combination, each limiter compiled in or a pair read at run time, every
+    BC class, against the CPU restatement."""
     for bc in BCS:
         rd, solver, params, q0, _ = problems.random_acoustics_2d(53, 41, seed=4, bc=bc, order=order,
-                                                                trans=trans, limiter="vanleer")
+                                                                trans=trans)
+        rd.clawdata.limiter = list(lim) if isinstance(lim, tuple) else [lim, lim]
         g, o = _pair(rd, solver, params, q0, precision="fp32")
         for _ in range(10):
             cg, co = g.step(0.004), o.step(0.004)
