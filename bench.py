@@ -75,22 +75,66 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks, power and clock-event (throttle) reasons sampled during the
+    timed region: NVML read in-process every 10 ms (the GPU this process runs
+    on, mapped through CUDA_VISIBLE_DEVICES), else `nvidia-smi -lms 200`.
+    Only reads; changes no setting."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h): SwPowerCap 0x4, HwSlowdown 0x8,
+    # SwThermalSlowdown 0x20, HwThermalSlowdown 0x40
+    BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+            ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
-    def __init__(self, index):
-        self.index = index
-        self.rows = []
+    def __init__(self, device):
+        self.device = device
+        self.rows = []  # (sm MHz, max sm MHz, power W, reason bits)
         self.proc = None
         self.thread = None
+        self.nvml = None
+        self.halt = threading.Event()
+        self.first = threading.Event()
+
+    def _nvml_start(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            idx = torch.cuda._get_nvml_device_index(self.device)
+        except Exception:
+            idx = self.device
+        h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+        reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        self.nvml = pynvml
+
+        def loop():
+            while not self.halt.is_set():
+                try:
+                    sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    pw = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    self.rows.append((sm, smax, pw, int(reasons(h))))
+                except pynvml.NVMLError:
+                    pass
+                self.first.set()
+                self.halt.wait(0.01)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+        self.first.wait(2.0)
 
     def start(self):
         try:
+            self._nvml_start()
+            return
+        except Exception:
+            self.nvml = None
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
@@ -102,30 +146,41 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+            if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                bits = 0
+                for k, (_, bit) in enumerate(self.BITS):
+                    if "Active" in parts[5 + k] and "Not" not in parts[5 + k]:
+                        bits |= bit
+                pw = float(parts[3]) if parts[3].replace(".", "").isdigit() else float("nan")
+                self.rows.append((float(parts[1]), float(parts[2]), pw, bits))
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        if self.thread:
+        if self.nvml is not None:
+            self.halt.set()
             self.thread.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for k, n in enumerate(names):
-                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            source = "nvml, 10 ms"
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+            source = "nvidia-smi, 200 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        rows = list(self.rows)
+        reasons = sorted({n for r in rows for n, bit in self.BITS if r[3] & bit})
+        pw = [r[2] for r in rows if r[2] == r[2]]
+        return {"sm_mhz": float(np.median([r[0] for r in rows])) if rows else None,
+                "sm_max_mhz": max(r[1] for r in rows) if rows else None,
+                "power_w": float(np.median(pw)) if pw else None,
+                "reasons": reasons, "samples": len(rows), "source": source}
 
 
 def dist_setup():
@@ -488,6 +543,19 @@ def other_configs(peaks, cpu=True):
             out[key] = e
         except Exception as e:
             out[key] = {"error": str(e)}
+    # time to an L1 error (the metric's second half): 2D radial acoustics at
+    # 512^2 / 1024^2 / 2048^2 in each precision against a 4096^2 truth; the
+    # batched Euler ensemble against one claw2 call per instance (32 instances)
+    try:
+        from classic_b200 import accuracy
+        out["time_to_l1_radial_2d"] = accuracy.radial_time_to_l1()
+    except Exception as e:
+        out["time_to_l1_radial_2d"] = {"error": str(e)}
+    try:
+        from classic_b200 import accuracy
+        out["euler_ensemble_batched_vs_serial"] = accuracy.ensemble_batched_vs_serial(32)
+    except Exception as e:
+        out["euler_ensemble_batched_vs_serial"] = {"error": str(e)}
     # the learned corrector (the shipped network) on two unseen seeds: coarse
     # 256^2 corrected / plain against the block-averaged 1024^2 FP64 run
     try:
