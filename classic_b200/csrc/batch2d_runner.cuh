@@ -122,8 +122,7 @@ struct BatchRunnerT : BatchRunner {
     int nsm_ = 1, per_sm_ = 1;
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_batch_kernel<S, M><<<grid, 32 * WARPS2D, smem, s>>>(b);
-        return cudaGetLastError();
+        return launch_step(step2_batch_kernel<S, M>, dim3(grid), dim3(32 * WARPS2D), smem, s, b);
     }
 };
 

@@ -184,6 +184,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     constexpr unsigned FULL = 0xffffffffu;
     ClawCtl* ctl = A.ctl;
     __shared__ double red[WARPS2D];
+    grid_dependency_sync();
     if (*(volatile int*)&ctl->done) return;
     const int cur = *(volatile int*)&ctl->cur;
     const double dtd = *(volatile double*)&ctl->dt;

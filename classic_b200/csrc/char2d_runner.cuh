@@ -65,8 +65,8 @@ struct CharRunner : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_char_kernel<real, LIM, BCM, ORD, TRN><<<grid, 32 * WARPS2D, smem, s>>>(args);
-        return cudaGetLastError();
+        return launch_step(step2_char_kernel<real, LIM, BCM, ORD, TRN>, dim3(grid), dim3(32 * WARPS2D), smem, s,
+                           args);
     }
 };
 

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <memory>
+#include <utility>
 
 #include "../../include/claw_b200.h"
 #include "common.cuh"
@@ -46,6 +47,30 @@ inline int row_blocks(long long full, int nstrips, int my, int min_rows, int* br
     *nblocks = (my + *brows - 1) / *brows;
     const long long items = (long long)nstrips * *nblocks;
     return (int)(items < full ? items : full);
+}
+
+// Launch a step kernel; with CLAW_PDL, with programmatic stream serialization
+// (the kernel calls grid_dependency_sync before it reads what the previous
+// launch wrote).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_step(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                               Args&&... args) {
+#if CLAW_PDL
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+#else
+    kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+    return cudaGetLastError();
+#endif
 }
 
 // Record an error message (claw_last_error) and return code.

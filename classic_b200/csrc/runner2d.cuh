@@ -74,8 +74,7 @@ struct Runner2D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        step2_kernel<S, M, SRC><<<grid, 32 * WARPS2D, smem, s>>>(args);
-        return cudaGetLastError();
+        return launch_step(step2_kernel<S, M, SRC>, dim3(grid), dim3(32 * WARPS2D), smem, s, args);
     }
 };
 

@@ -82,10 +82,10 @@ struct Runner3D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        kernel<0, false>()<<<grid[0], NT3P, SMEM, s>>>(args[0]);
-        kernel<1, false>()<<<grid[1], NT3P, SMEM, s>>>(args[1]);
-        kernel<2, true>()<<<grid[2], NT3P, SMEM, s>>>(args[2]);
-        return cudaGetLastError();
+        cudaError_t e = launch_step(kernel<0, false>(), dim3(grid[0]), dim3(NT3P), SMEM, s, args[0]);
+        if (e == cudaSuccess) e = launch_step(kernel<1, false>(), dim3(grid[1]), dim3(NT3P), SMEM, s, args[1]);
+        if (e == cudaSuccess) e = launch_step(kernel<2, true>(), dim3(grid[2]), dim3(NT3P), SMEM, s, args[2]);
+        return e;
     }
     int launches_per_step() const override { return 3; }
 };
@@ -163,9 +163,10 @@ struct SplitRunner3D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        split3_x_kernel<S, BUILD><<<grid[0], 32 * DS3_WARPS, 0, s>>>(args);
-        split3_yz_kernel<S, 1, BUILD><<<grid[1], 32 * DS3_WARPS, 0, s>>>(args);
-        split3_yz_kernel<S, 2, BUILD><<<grid[2], 32 * DS3_WARPS, 0, s>>>(args);
+        cudaError_t e = launch_step(split3_x_kernel<S, BUILD>, dim3(grid[0]), dim3(32 * DS3_WARPS), 0, s, args);
+        if (e == cudaSuccess) e = launch_step(split3_yz_kernel<S, 1, BUILD>, dim3(grid[1]), dim3(32 * DS3_WARPS), 0, s, args);
+        if (e == cudaSuccess) e = launch_step(split3_yz_kernel<S, 2, BUILD>, dim3(grid[2]), dim3(32 * DS3_WARPS), 0, s, args);
+        if (e != cudaSuccess) return e;
         return cudaGetLastError();
     }
     int launches_per_step() const override { return 3; }

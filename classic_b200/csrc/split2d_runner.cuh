@@ -77,8 +77,7 @@ struct SplitRunner2D : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        split2_kernel<S, M, STRANG, SRC, BUILD><<<grid, 32 * WARPS2D, smem, s>>>(args);
-        return cudaGetLastError();
+        return launch_step(split2_kernel<S, M, STRANG, SRC, BUILD>, dim3(grid), dim3(32 * WARPS2D), smem, s, args);
     }
 };
 

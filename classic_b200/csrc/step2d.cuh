@@ -707,6 +707,7 @@ __global__ void __launch_bounds__(32 * WARPS2D, step2_minb<S>::value)
 step2_kernel(const __grid_constant__ Step2Args<S> A) {
     ClawCtl* ctl = A.ctl;
     __shared__ double red[WARPS2D];
+    grid_dependency_sync();
     if (*(volatile int*)&ctl->done) return;
     const int cur = *(volatile int*)&ctl->cur;
     const double dtd = *(volatile double*)&ctl->dt;
@@ -785,6 +786,7 @@ step2_batch_kernel(const __grid_constant__ Step2Batch<S> B) {
     constexpr unsigned FULL = 0xffffffffu;
     __shared__ int pre[BATCH_MAX + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    grid_dependency_sync();
     // units of the active instances, then their prefix sums
     for (int k = threadIdx.x; k < B.count; k += blockDim.x)
         pre[k + 1] = *(volatile int*)&B.ctls[k].done ? 0 : B.units[k];

@@ -540,6 +540,7 @@ split2_kernel(const __grid_constant__ Step2Args<S> A) {
     using real = typename S::real;
     ClawCtl* ctl = A.ctl;
     __shared__ double red[3 * WARPS2D];
+    grid_dependency_sync();
     if (*(volatile int*)&ctl->done) return;
     const int cur = *(volatile int*)&ctl->cur;
     const double dtd = *(volatile double*)&ctl->dt;

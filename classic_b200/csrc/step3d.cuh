@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typen
     double* red = reinterpret_cast<double*>(sq + QST3 * NT3);
 
     ClawCtl* ctl = a.ctl;
+    grid_dependency_sync();
     if (ctl->done) return;
     const int cur = ctl->cur;
     const real* __restrict__ qold = a.q[cur];

@@ -504,6 +504,7 @@ __global__ void __launch_bounds__(NT3P, 1) sweep3f_kernel(const Sweep3Args<typen
                                             RING3 * NPL3F * NS3 + term3_bufs<real>() * NTERM3 * NT3 +
                                             (XCH3 + QST3 + VST3) * NT3);
     ClawCtl* ctl = a.ctl;
+    grid_dependency_sync();
     if (ctl->done) return;
     // warps 2k (role 0) and 2k+1 (role 1) share 32 slices
     const double cfl = ((threadIdx.x >> 5) & 1) ? sweep3f_march<S, DIR, M, 1>(a, smem_raw)

@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(32 * DS3_WARPS) split3_x_kernel(const Split3Ar
     constexpr unsigned FULL = 0xffffffffu;
     __shared__ double red[DS3_WARPS];
     ClawCtl* ctl = a.ctl;
+    grid_dependency_sync();
     if (*(volatile int*)&ctl->done) return;
     const int cur = *(volatile int*)&ctl->cur;
     const double dt = *(volatile double*)&ctl->dt;
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(32 * DS3_WARPS, 2) split3_yz_kernel(const Spli
     using real = typename S::real;
     __shared__ double red[DS3_WARPS];
     ClawCtl* ctl = a.ctl;
+    grid_dependency_sync();
     if (*(volatile int*)&ctl->done) return;
     const int cur = *(volatile int*)&ctl->cur;
     const double dt = *(volatile double*)&ctl->dt;
