@@ -24,7 +24,13 @@
 
 namespace clawb200 {
 
-constexpr int T3A = 16, T3B = 16, NT3 = T3A * T3B;   // thread tile, incl. the halo ring
+#ifndef CLAW_T3B
+#define CLAW_T3B 16
+#endif
+#ifndef CLAW_SWEEP3_MINB
+#define CLAW_SWEEP3_MINB 1  // resident CTAs per SM the sweep kernels are compiled for
+#endif
+constexpr int T3A = 16, T3B = CLAW_T3B, NT3 = T3A * T3B;   // thread tile, incl. the halo ring
 constexpr int S3A = T3A + 2, S3B = T3B + 2, NS3 = S3A * S3B;  // aux tile, one more ring
 constexpr int SEG3 = 64;                              // cell positions per CTA march
 constexpr int RING3 = 4;                              // aux positions held in shared memory
@@ -131,7 +137,7 @@ constexpr int NT3P = 2 * NT3;
 // --fmad=false) and the contracted unit (1, --fmad=true): the same template
 // arguments in both would be one symbol with two different bodies.
 template <class S, int DIR, class M, bool LAST, int BUILD>
-__global__ void __launch_bounds__(NT3P, 1) sweep3p_kernel(const Sweep3Args<typename S::real> a) {
+__global__ void __launch_bounds__(NT3P, CLAW_SWEEP3_MINB) sweep3p_kernel(const Sweep3Args<typename S::real> a) {
     using real = typename S::real;
     using Split = typename S::Split;
     constexpr int AXN = DIR, AXA = DIR == 0 ? 1 : 0, AXB = DIR == 2 ? 1 : 2;

@@ -497,7 +497,7 @@ __device__ __forceinline__ double sweep3f_march(const Sweep3Args<typename S::rea
 }
 
 template <class S, int DIR, class M, bool LAST>
-__global__ void __launch_bounds__(NT3P, 1) sweep3f_kernel(const Sweep3Args<typename S::real> a) {
+__global__ void __launch_bounds__(NT3P, CLAW_SWEEP3_MINB) sweep3f_kernel(const Sweep3Args<typename S::real> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using real = typename S::real;
     double* red = reinterpret_cast<double*>(reinterpret_cast<real*>(smem_raw) +
