@@ -49,13 +49,29 @@ __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
     return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 
-// GELU(z) = z Phi(z) with Phi the standard normal CDF, and its derivative
-// Phi(z) + z phi(z).
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear Units",
+// 2016): GELU(z) = z/2 (1 + tanh(u)), u = sqrt(2/pi) (z + 0.044715 z^3), with
+// the hardware tanh (tanh.approx.f32, relative error about 2^-11).  It is
+// within 5e-4 of z Phi(z), below the resolution of the BF16 activations, and
+// costs about 7 instructions per value where the erf form costs several
+// times that: the convolution's epilogue applies it to every output.
+// Derivative: (1 + t)/2 + z/2 (1 - t^2) du/dz, du/dz = sqrt(2/pi) (1 + 3 0.044715 z^2).
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float GELU_K0 = 0.79788456080286536f;  // sqrt(2/pi)
+constexpr float GELU_K1 = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    const float t = tanh_hw(GELU_K0 * fmaf(GELU_K1 * z, z * z, z));
+    const float hz = 0.5f * z;
+    return fmaf(hz, t, hz);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-    return cdf + z * pdf;
+    const float t = tanh_hw(GELU_K0 * fmaf(GELU_K1 * z, z * z, z));
+    const float du = GELU_K0 * fmaf(3.0f * GELU_K1 * z, z, 1.0f);
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * du;
 }
 
 // Load a HALO x HALO x CP input tile (zero outside the image) into shared
@@ -243,16 +259,18 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
         const int m = gw * 32 + lane;
         const long long pix = ((long long)img * h + y0 + m / TW) * w + x0 + m % TW;
         const uint32_t trow = tslot + ((uint32_t)(gw * 32) << 16) + (uint32_t)(g * 64 + b * 32);
+        // every column of the accumulator in flight at once, one wait
+        uint32_t rr[COUT];
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) ld16(trow + c0, rr + c0);
+        wait_ld();
+        if (!ok) return;
 #pragma unroll
         for (int c0 = 0; c0 < COUT; c0 += 16) {
-            uint32_t rr[16];
-            ld16(trow + c0, rr);
-            wait_ld();
-            if (!ok) continue;
             float z[16], yv[16];
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
-                z[q] = __uint_as_float(rr[q]) + bs[c0 + q];
+                z[q] = __uint_as_float(rr[c0 + q]) + bs[c0 + q];
                 yv[q] = ACT ? gelu(z[q]) : z[q];
             }
             if (SAVEZ) {

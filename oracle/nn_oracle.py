@@ -13,7 +13,6 @@ Layouts follow include/claw_nn.h: activations NHWC [n][h][w][c], weights
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 
 def bf16(a):
@@ -59,12 +58,19 @@ def flip(w):
     return np.transpose(w[:, ::-1, :], (2, 1, 0))
 
 
+GELU_K0 = np.sqrt(2.0 / np.pi)
+GELU_K1 = 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks and Gimpel 2016), as the device
+    computes it: z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_K0 * (z + GELU_K1 * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_K0 * (z + GELU_K1 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_K0 * (1.0 + 3.0 * GELU_K1 * z * z)
 
 
 def forward(x, layers):
