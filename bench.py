@@ -30,7 +30,9 @@ The headline arithmetic is FP64 with fused multiply-adds in characteristic
 variables (precision "fp64_fma"): the same algorithm and dt sequence as the
 reference-order path, within 1e-12 relative of it over the full run.
 
---impl reference times that CPU restatement alone on the same metric.
+--impl reference times that CPU restatement alone on the same metric, on every
+host thread the process may use (the slices of a sweep spread over them; the
+reference's own 2D step is serial, and its one-core figure is reported beside).
 Under torchrun with N > 1 each rank runs an independent replica (the
 workload fits one GPU and does not shard), value = all ranks' cell-updates /
 max time over ranks.
@@ -224,21 +226,34 @@ def host_cpu():
     return {"model": model, "nproc": os.cpu_count()}
 
 
-def cpu_reference_sample(n, nsteps):
+def cpu_reference_sample(n, nsteps, threads=1):
     """Time the CPU restatement (oracle, speed build) on nsteps whole n^2
-    steps of the workload; returns (cell-updates/s, seconds, cores)."""
+    steps of the workload with `threads` host threads (the slices of a sweep
+    spread over them); returns (cell-updates/s, seconds, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from classic_b200 import problems
     from pyoracle import OracleGrid
     rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=n)
     g = OracleGrid(rd.clawdata, solver, params, variant="fast")
-    g.set_q(q0)
-    dt = 0.9 * (2.0 / n) / 2.0
-    t0 = time.perf_counter()
-    for _ in range(nsteps):
-        g.step(dt)
-    sec = time.perf_counter() - t0
-    return n * n * nsteps / sec, sec, 1
+    g.lib.orc_set_threads(threads)
+    try:
+        g.set_q(q0)
+        dt = 0.9 * (2.0 / n) / 2.0
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            g.step(dt)
+        sec = time.perf_counter() - t0
+    finally:
+        g.lib.orc_set_threads(1)
+    return n * n * nsteps / sec, sec, threads
+
+
+def host_threads():
+    """Host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
 
 
 def run_reference_arm(args):
@@ -246,14 +261,16 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     n = N_CELLS
+    nt = host_threads()
     for _ in range(args.warmup):
-        cpu_reference_sample(n, 1)
+        cpu_reference_sample(n, 1, nt)
     rates, secs = [], 0.0
     for _ in range(args.steps):
-        r, s, cores = cpu_reference_sample(n, 1)
+        r, s, cores = cpu_reference_sample(n, 1, nt)
         rates.append(r)
         secs += s
     value = n * n * args.steps / secs
+    r1, s1, _ = cpu_reference_sample(n, 1, 1)  # the reference's own serial step, for scale
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -261,9 +278,12 @@ def run_reference_arm(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"2D radial acoustics FP64 {n}^2, MC, transverse 2",
                    "step": f"one whole {n}^2 time step (bounded sample of a frame)"},
-        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-                         "sample": f"{args.steps} whole {n}^2 steps of the CPU restatement "
-                                   "(the reference's 2D step is serial)", "host": host_cpu()},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": nt, "kind": "port",
+                         "sample": f"{args.steps} whole {n}^2 steps of the CPU restatement with "
+                                   f"the slices of each sweep spread over {nt} host threads (the "
+                                   "reference's 2D step itself is serial)", "host": host_cpu(),
+                         "one_core": {"value": r1, "cores": 1,
+                                      "sample": f"1 whole {n}^2 step on one core ({s1:.1f} s)"}},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
