@@ -148,7 +148,10 @@ struct ColSrc {
 #define CLAW_CHAR_MINB 3  // FP64: 168 registers, 12 warps per SM, no spills (fastest measured)
 #endif
 #ifndef CLAW_CHAR_MINB_F32
-#define CLAW_CHAR_MINB_F32 4  // FP32: 121 registers, 16 warps per SM, no spills (10 % faster than 3)
+// FP32: 121 registers, 16 warps per SM, no spills; 10 % faster than 3 CTAs,
+// and faster than 5 (93 registers: 115 against 119 us per 4096^2 step) or 6
+// (spills: 138 us), whose more and shorter row blocks add halo rows
+#define CLAW_CHAR_MINB_F32 4
 #endif
 #ifndef CLAW_CHAR_UNROLL
 #define CLAW_CHAR_UNROLL 2
