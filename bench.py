@@ -22,7 +22,8 @@ cells / device time.
              this host on a bounded sample (whole 4096^2 steps; one core as
              the reference's serial step2, and all cores threaded beside it)
   other_configs : the other workloads (1D, 2D 1024^2, 3D 256^3 / 512^3, the
-             split steps, the Euler ensemble, the learned corrector), each
+             split steps, one 2048^2 Euler grid, the Euler ensemble, the
+             learned corrector, the time to an L1 error per precision), each
              with its roofline and, where the reference has a CPU path, a
              CPU baseline
 
@@ -525,6 +526,24 @@ def other_configs(peaks, cpu=True):
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
                         "roofline": roofline_entry(rate, nbytes, peaks, kern, fp64_peak)}
+        except Exception as e:
+            out[key] = {"error": str(e)}
+    # one 2048^2 Euler grid (four-quadrant data, seed 7) on the generic kernel:
+    # reference order and the contracted build; t 0 -> 0.02 warms up, the next
+    # 0.02 is timed
+    for prec in ("fp64", "fp64_fma"):
+        key = "euler_2d_2048_" + prec
+        try:
+            rd, solver, params, q0, _ = problems.euler_quadrants(n=2048, seed=7)
+            s = Solver(rd.clawdata, solver, params, precision=prec)
+            s.set_q(q0)
+            info, st = s.advance(0.0, 0.02, float(rd.clawdata.dt_initial))
+            info, st = s.advance(0.02, 0.04, st["dt_next"])
+            s.close()
+            rate = 2048 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
+            out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
+                        "kernel": "step2_kernel (Euler Roe, MC, transverse 2)",
+                        "roofline": roofline_entry(rate, 64, peaks)}
         except Exception as e:
             out[key] = {"error": str(e)}
     sizes = problems.euler_ensemble_sizes(256, seed=0)
