@@ -29,7 +29,6 @@ def test_radial_time_to_l1_small():
     assert rows[(128, "fp64")]["l1_p"] > 1.5 * rows[(256, "fp64")]["l1_p"]
 
 
-
 def test_ensemble_batched_equals_serial_and_is_faster():
     """Eight instances of the batched Euler workload: the batch reproduces one
     claw2 call per instance bit for bit (reference order) in less time."""
