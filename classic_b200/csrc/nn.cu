@@ -16,8 +16,10 @@
 // projection and a positivity fallback to the plain step.
 #include <algorithm>
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 #include "../../include/claw_nn.h"
@@ -164,29 +166,29 @@ __host__ __device__ constexpr int a_bytes() { return (CIN / 8) * NPX * 16; }
 // accumulators of its own.  In a pipeline, while the tensor core runs tile
 // i's 9 x CIN/16 MMAs into one accumulator, the group runs tile i-1's
 // epilogue (tcgen05.ld, bias, GELU, stores) from the other, then starts the
-// copies of tile i+2's halo into the third stage (cp.async, 16-byte chunks).
-// A stage is refilled only after the MMAs that read it have committed (the
-// epilogue's mbarrier wait); an accumulator is reused only after every
-// thread's tcgen05.ld of it has completed (tcgen05 fences around the group's
-// named barrier).  Every wait is bounded.
+// copy of tile i+2's halo into the third stage: TMA boxes issued by the
+// pipeline's first thread, completing on the stage's mbarrier, which that
+// thread alone waits on before it issues the tile's MMAs.  A stage is
+// refilled only after the MMAs that read it have committed (the epilogue's
+// mbarrier wait); an accumulator is reused only after every thread's
+// tcgen05.ld of it has completed (tcgen05 fences around the group's named
+// barrier).  Every wait is bounded.
 namespace tcp {
 constexpr int NST = 3;    // halo stages per pipeline
 constexpr int NPIPE = 4;  // pipelines (groups of 4 warps) per CTA
 constexpr int NTH = NPIPE * tc::NTH;
-__device__ __forceinline__ void cp16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(clawb200::smem_u32(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void wait_group1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void group_sync(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(tc::NTH) : "memory");
 }
+// one 8-channel plane of a halo tile, padded so that every TMA destination
+// starts on a 128-byte boundary
+constexpr int PLANE = ((tc::NPX * 16 + 127) / 128) * 128;
 template <int CIN>
-__host__ __device__ constexpr int stage_bytes() { return ((tc::a_bytes<CIN, 0>() + 127) / 128) * 128; }
+__host__ __device__ constexpr int stage_bytes() { return (CIN / 8) * PLANE; }
 template <int CIN, int COUT>
 __host__ __device__ constexpr int smem_bytes() {
-    return NPIPE * NST * stage_bytes<CIN>() + 9 * (CIN / 8) * COUT * 16 + COUT * 4;
+    // + 128: the base is rounded up to a 128-byte boundary in the kernel
+    return 128 + NPIPE * NST * stage_bytes<CIN>() + 9 * (CIN / 8) * COUT * 16 + COUT * 4;
 }
 }  // namespace tcp
 
@@ -195,15 +197,18 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
                                                             const __nv_bfloat16* __restrict__ wt,
                                                             const float* __restrict__ bias, void* out,
                                                             float* __restrict__ zsave, int n, int h,
-                                                            int w) {
+                                                            int w, const __grid_constant__ CUtensorMap tmx) {
     using namespace tc;
     static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "UMMA M128: N in {16, 32}, K in steps of 16");
     constexpr int KC = CIN / 8;
-    constexpr int APLANE = NPX * 16;
+    constexpr int APLANE = tcp::PLANE;
     constexpr int ASTAGE = tcp::stage_bytes<CIN>();
     constexpr int BPLANE = COUT * 16;
-    extern __shared__ __align__(16) unsigned char smem[];  // 16-byte alignment is all UMMA needs without swizzle
-    __shared__ uint64_t bar[tcp::NPIPE][2];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // TMA writes the halo planes: start them on a 128-byte boundary
+    unsigned char* smem = smem_raw + ((128u - (clawb200::smem_u32(smem_raw) & 127u)) & 127u);
+    __shared__ uint64_t bar[tcp::NPIPE][2];           // a tile's MMAs committed (per accumulator)
+    __shared__ uint64_t full[tcp::NPIPE][tcp::NST];   // a stage's halo landed (TMA bytes)
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = warp >> 2;               // pipeline of this thread
@@ -221,27 +226,27 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
             *reinterpret_cast<const uint4*>(wt + ((long long)co * 9 + tap) * CIN + kc * 8);
     }
     for (int e = tid; e < COUT; e += tcp::NTH) bs[e] = bias[e];
+    clawb200::fence_proxy_async_smem();  // the tensor core reads the weights these threads wrote
     if (warp == 0) alloc(&tslot, 64 * tcp::NPIPE);
     if (gt == 0) {
         clawb200::mbar_init(&bar[g][0], 1);
         clawb200::mbar_init(&bar[g][1], 1);
+        for (int st = 0; st < tcp::NST; ++st) clawb200::mbar_init(&full[g][st], 1);
         clawb200::fence_barrier_init();
     }
-    // halo tile of tile t into stage st of this pipeline (zeros outside the image)
+    // halo tile of tile t into stage st of this pipeline: KC boxes of 8
+    // channels x 10 x 18 pixels (NHWC), issued by the pipeline's first
+    // thread; the box starts one pixel up and left of the tile and the copy
+    // fills with zeros outside the image
     auto load_tile = [&](int t, int st) {
-        if (t >= ntiles) return;
+        if (t >= ntiles || gt != 0) return;
         const int img = t / tiles_img, r = t % tiles_img;
         const int y0 = (r / tiles_x) * TH, x0 = (r % tiles_x) * TW;
         unsigned char* A = As + st * ASTAGE;
-        for (int e = gt; e < NPX * KC; e += tc::NTH) {
-            const int pix = e / KC, kc = e % KC;
-            const int gy = y0 + pix / HW - 1, gx = x0 + pix % HW - 1;
-            unsigned char* dst = A + kc * APLANE + pix * 16;
-            if (gy >= 0 && gy < h && gx >= 0 && gx < w)
-                tcp::cp16(dst, x + (((long long)img * h + gy) * w + gx) * CIN + kc * 8);
-            else
-                *reinterpret_cast<uint4*>(dst) = make_uint4(0, 0, 0, 0);
-        }
+        clawb200::mbar_arrive_expect_tx(&full[g][st], (uint32_t)(KC * NPX * 16));
+#pragma unroll
+        for (int kc = 0; kc < KC; ++kc)
+            clawb200::tma_load_4d(A + kc * APLANE, &tmx, kc * 8, x0 - 1, y0 - 1, img, &full[g][st]);
     };
     bool ok = true;
     // epilogue of tile t, the j-th of this pipeline (accumulator j & 1)
@@ -297,25 +302,28 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
     };
 
     const int first = blockIdx.x * tcp::NPIPE + g, stride = gridDim.x * tcp::NPIPE;
-    load_tile(first, 0);
-    tcp::commit_group();
-    load_tile(first + stride, 1);
-    tcp::commit_group();
     fence_before();
-    __syncthreads();
+    __syncthreads();  // barriers initialised, weights in place, TMEM allocated
     fence_after();
+    load_tile(first, 0);
+    load_tile(first + stride, 1);
     const uint32_t tacc = tslot + (uint32_t)(g * 64);
     constexpr uint32_t idesc = idesc_bf16_f32(128, COUT);
     const uint32_t b0 = clawb200::smem_u32(Bs);
     int i = 0;
     for (int t = first; t < ntiles; t += stride, ++i) {
-        tcp::wait_group1();  // tile i's copies have landed (tile i+1's may be pending)
-        clawb200::fence_proxy_async_smem();  // the tensor core reads what the threads wrote
+        // accumulator i & 1 is free: every thread's tcgen05.ld of tile i-2 is done
         fence_before();
         tcp::group_sync(g);
         fence_after();
         if (gt == 0) {
-            const uint32_t a0 = clawb200::smem_u32(As + (i % tcp::NST) * ASTAGE);
+            // tile i's halo has landed (only the MMAs read it)
+            const int st = i % tcp::NST;
+            if (!clawb200::mbar_wait_bounded(&full[g][st], (uint32_t)((i / tcp::NST) & 1))) {
+                atomicOr(&g_nn_err, 1);  // never expected: record it, give the copy a second bound
+                (void)clawb200::mbar_wait_bounded(&full[g][st], (uint32_t)((i / tcp::NST) & 1));
+            }
+            const uint32_t a0 = clawb200::smem_u32(As + st * ASTAGE);
             const uint32_t acc_addr = tacc + (uint32_t)((i & 1) * 32);
             uint32_t acc = 0;
 #pragma unroll
@@ -332,12 +340,11 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
             commit(&bar[g][i & 1]);
         }
         if (i > 0) epilogue(t - stride, i - 1);
-        load_tile(t + 2 * stride, (i + 2) % tcp::NST);  // the stage tile i-1's MMAs read
-        tcp::commit_group();
+        // the stage tile i-1's MMAs read: they have committed (the epilogue waited)
+        load_tile(t + 2 * stride, (i + 2) % tcp::NST);
         fence_before();
     }
     if (i > 0) epilogue(first + (i - 1) * stride, i - 1);
-    asm volatile("cp.async.wait_all;" ::: "memory");
     fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -641,6 +648,34 @@ int grid_for(long long n) {
     return (int)(b < 592 ? (b > 0 ? b : 1) : 592);
 }
 
+// Tensor map of an NHWC BF16 activation tensor for the forward kernel's
+// halo boxes: dims (C, W, H, N), box (8 channels, 10, 18, 1), zero fill
+// outside the tensor.
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult qr;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+int halo_map(CUtensorMap* map, const void* x, int n, int h, int w, int c) {
+    auto fn = encode_tiled();
+    if (!fn || (reinterpret_cast<uintptr_t>(x) & 15u)) return NN_E_CUDA;
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)w * c * 2, (cuuint64_t)h * w * c * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)tc::HW, (cuuint32_t)tc::HH, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : NN_E_CUDA;
+}
+
 template <int CIN, int COUT, int ACT, bool OUTF32, bool SAVEZ>
 int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, int n, int h,
                int wd, cudaStream_t s) {
@@ -659,8 +694,10 @@ int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, 
     const long long ntiles = (long long)n * (h / tc::TH) * (wd / tc::TW);
     const long long groups = (ntiles + tcp::NPIPE - 1) / tcp::NPIPE;
     const int grid = (int)std::min<long long>(groups, (long long)nsm * per_sm);
+    CUtensorMap map;
+    if (halo_map(&map, x, n, h, wd, CIN) != 0) return NN_E_CUDA;
     k<<<grid, tcp::NTH, SM, s>>>(static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w),
-                                b, y, z, n, h, wd);
+                                b, y, z, n, h, wd, map);
     return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
 }
 
