@@ -171,14 +171,16 @@ __host__ __device__ constexpr int a_bytes() { return (CIN / 8) * NPX * 16; }
 // thread alone waits on before it issues the tile's MMAs.  A stage is
 // refilled only after the MMAs that read it have committed (the epilogue's
 // mbarrier wait); an accumulator is reused only after every thread's
-// tcgen05.ld of it has completed (tcgen05 fences around the group's named
-// barrier).  Every wait is bounded.
+// tcgen05.ld of it has completed: each thread arrives on the accumulator's
+// mbarrier after its loads (behind a tcgen05 fence) and the issuing thread
+// alone waits on it, so the group's warps never stop for one another.
+// Every wait is bounded.
 namespace tcp {
 constexpr int NST = 3;    // halo stages per pipeline
 constexpr int NPIPE = 4;  // pipelines (groups of 4 warps) per CTA
 constexpr int NTH = NPIPE * tc::NTH;
-__device__ __forceinline__ void group_sync(int g) {
-    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(tc::NTH) : "memory");
+__device__ __forceinline__ void arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(clawb200::smem_u32(bar)) : "memory");
 }
 // one 8-channel plane of a halo tile, padded so that every TMA destination
 // starts on a 128-byte boundary
@@ -209,6 +211,7 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
     unsigned char* smem = smem_raw + ((128u - (clawb200::smem_u32(smem_raw) & 127u)) & 127u);
     __shared__ uint64_t bar[tcp::NPIPE][2];           // a tile's MMAs committed (per accumulator)
     __shared__ uint64_t full[tcp::NPIPE][tcp::NST];   // a stage's halo landed (TMA bytes)
+    __shared__ uint64_t freed[tcp::NPIPE][2];         // every thread has read an accumulator
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = warp >> 2;               // pipeline of this thread
@@ -220,20 +223,19 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
     const int tiles_x = w / TW, tiles_img = tiles_x * (h / TH);
     const int ntiles = tiles_img * n;
 
-    for (int e = tid; e < COUT * 9 * KC; e += tcp::NTH) {  // wt[co][tap][ci] -> [tap][kc][co]
-        const int co = e / (9 * KC), r = e % (9 * KC), tap = r / KC, kc = r % KC;
-        *reinterpret_cast<uint4*>(Bs + (tap * KC + kc) * BPLANE + co * 16) =
-            *reinterpret_cast<const uint4*>(wt + ((long long)co * 9 + tap) * CIN + kc * 8);
-    }
-    for (int e = tid; e < COUT; e += tcp::NTH) bs[e] = bias[e];
-    clawb200::fence_proxy_async_smem();  // the tensor core reads the weights these threads wrote
     if (warp == 0) alloc(&tslot, 64 * tcp::NPIPE);
     if (gt == 0) {
         clawb200::mbar_init(&bar[g][0], 1);
         clawb200::mbar_init(&bar[g][1], 1);
         for (int st = 0; st < tcp::NST; ++st) clawb200::mbar_init(&full[g][st], 1);
+        clawb200::mbar_init(&freed[g][0], tc::NTH);
+        clawb200::mbar_init(&freed[g][1], tc::NTH);
         clawb200::fence_barrier_init();
     }
+    // Launched with programmatic dependent launch, this CTA may start while the
+    // previous launch drains: it waits here, before its first read of x, the
+    // weights or the bias and its first write, for that launch to complete.
+    clawb200::grid_dependency_sync();
     // halo tile of tile t into stage st of this pipeline: KC boxes of 8
     // channels x 10 x 18 pixels (NHWC), issued by the pipeline's first
     // thread; the box starts one pixel up and left of the tile and the copy
@@ -269,6 +271,8 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
 #pragma unroll
         for (int c0 = 0; c0 < COUT; c0 += 16) ld16(trow + c0, rr + c0);
         wait_ld();
+        fence_before();
+        tcp::arrive(&freed[g][b]);  // this thread is done with accumulator b
         if (!ok) return;
 #pragma unroll
         for (int c0 = 0; c0 < COUT; c0 += 16) {
@@ -302,21 +306,34 @@ __global__ void __launch_bounds__(tcp::NTH, 1) conv3x3_fwd_tcp(const __nv_bfloat
     };
 
     const int first = blockIdx.x * tcp::NPIPE + g, stride = gridDim.x * tcp::NPIPE;
+    // the first two halo copies fly while the weights are staged
+    load_tile(first, 0);
+    load_tile(first + stride, 1);
+    for (int e = tid; e < COUT * 9 * KC; e += tcp::NTH) {  // wt[co][tap][ci] -> [tap][kc][co]
+        const int co = e / (9 * KC), r = e % (9 * KC), tap = r / KC, kc = r % KC;
+        *reinterpret_cast<uint4*>(Bs + (tap * KC + kc) * BPLANE + co * 16) =
+            *reinterpret_cast<const uint4*>(wt + ((long long)co * 9 + tap) * CIN + kc * 8);
+    }
+    for (int e = tid; e < COUT; e += tcp::NTH) bs[e] = bias[e];
+    clawb200::fence_proxy_async_smem();  // the tensor core reads the weights these threads wrote
     fence_before();
     __syncthreads();  // barriers initialised, weights in place, TMEM allocated
     fence_after();
-    load_tile(first, 0);
-    load_tile(first + stride, 1);
     const uint32_t tacc = tslot + (uint32_t)(g * 64);
     constexpr uint32_t idesc = idesc_bf16_f32(128, COUT);
     const uint32_t b0 = clawb200::smem_u32(Bs);
     int i = 0;
     for (int t = first; t < ntiles; t += stride, ++i) {
-        // accumulator i & 1 is free: every thread's tcgen05.ld of tile i-2 is done
-        fence_before();
-        tcp::group_sync(g);
-        fence_after();
         if (gt == 0) {
+            // accumulator i & 1 is free: every thread's tcgen05.ld of tile i-2 is done
+            if (i >= 2) {
+                const uint32_t par = (uint32_t)(((i - 2) >> 1) & 1);
+                if (!clawb200::mbar_wait_bounded(&freed[g][i & 1], par)) {
+                    atomicOr(&g_nn_err, 1);
+                    (void)clawb200::mbar_wait_bounded(&freed[g][i & 1], par);
+                }
+                fence_after();
+            }
             // tile i's halo has landed (only the MMAs read it)
             const int st = i % tcp::NST;
             if (!clawb200::mbar_wait_bounded(&full[g][st], (uint32_t)((i / tcp::NST) & 1))) {
@@ -696,9 +713,27 @@ int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, 
     const int grid = (int)std::min<long long>(groups, (long long)nsm * per_sm);
     CUtensorMap map;
     if (halo_map(&map, x, n, h, wd, CIN) != 0) return NN_E_CUDA;
-    k<<<grid, tcp::NTH, SM, s>>>(static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w),
-                                b, y, z, n, h, wd, map);
+    const __nv_bfloat16* xb = static_cast<const __nv_bfloat16*>(x);
+    const __nv_bfloat16* wb = static_cast<const __nv_bfloat16*>(w);
+#if CLAW_PDL
+    // programmatic dependent launch: the CTAs' set-up overlaps the previous
+    // launch's tail (the kernel waits before touching its operands)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(tcp::NTH);
+    cfg.dynamicSmemBytes = SM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k, xb, wb, b, y, z, n, h, wd, map) != cudaSuccess) return NN_E_CUDA;
+    return 0;
+#else
+    k<<<grid, tcp::NTH, SM, s>>>(xb, wb, b, y, z, n, h, wd, map);
     return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+#endif
 }
 
 template <int CIN, int COUT>
