@@ -41,9 +41,11 @@ def _close(got, ref, rel):
 
 @pytest.mark.parametrize("cin,cout,act,outf", [(16, 32, 1, 0), (32, 32, 1, 0), (32, 16, 0, 1),
                                                (32, 32, 0, 0), (16, 32, 0, 0)])
-def test_forward_matches_oracle(cin, cout, act, outf):
-    rng = np.random.default_rng(cin + cout + act)
-    n, h, w = 2, 32, 48
+@pytest.mark.parametrize("n,h,w", [(2, 32, 48), (3, 16, 16)])
+def test_forward_matches_oracle(cin, cout, act, outf, n, h, w):
+    """The tcgen05 forward kernel against the oracle; 16 x 16 images make the
+    halo box (18 x 10 pixels) overhang the image on every side."""
+    rng = np.random.default_rng(cin + cout + act + h)
     x = O.bf16(rng.standard_normal((n, h, w, cin)))
     wt = O.bf16(rng.standard_normal((cout, 9, cin)) * 0.2)
     b = rng.standard_normal(cout).astype(np.float32) * 0.1
