@@ -477,7 +477,8 @@ def other_configs(peaks, cpu=True):
                 out[key] = {"error": str(e)}
     # other methods of the same workload on the characteristic kernel: transverse
     # 1; minmod, superbee and van Leer compiled in (FP64 contracted and FP32);
-    # MC / van Leer on the two waves (read at run time).  4096^2; a first frame
+    # MC / van Leer on the two waves (a compiled pair) and MC / none (read at
+    # run time).  4096^2; a first frame
     # (t 0 -> 0.02) warms up, the next (0.02 -> 0.05) is timed.
     char_kern = "step2_char_kernel"
     for key, trans, lims, prec, kern in (
@@ -487,6 +488,8 @@ def other_configs(peaks, cpu=True):
             ("radial_2d_4096_vanleer_fp64_fma", 2, ["vanleer", "vanleer"], "fp64_fma", char_kern),
             ("radial_2d_4096_vanleer_fp32", 2, ["vanleer", "vanleer"], "fp32", char_kern),
             ("radial_2d_4096_mixed_limiters_fp64_fma", 2, ["mc", "vanleer"], "fp64_fma",
+             char_kern + " (MC on wave 1, van Leer on wave 2, compiled in)"),
+            ("radial_2d_4096_runtime_limiters_fp64_fma", 2, ["mc", "none"], "fp64_fma",
              char_kern + " (limiters read at run time)")):
         try:
             rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)

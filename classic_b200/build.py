@@ -46,7 +46,9 @@ UNITS = [("claw_b200.cu", "--fmad=false"), ("noalloc.cu", "--fmad=false"),
          ("split2d_fast.cu", "--fmad=true"), ("probe.cu", "--fmad=true"),
          ("fma2d.cu", "--fmad=true"), ("batch2d_fast.cu", "--fmad=true"),
          ("fast2d_minmod.cu", "--fmad=true"), ("fast2d_superbee.cu", "--fmad=true"),
-         ("fast2d_vanleer.cu", "--fmad=true")]
+         ("fast2d_vanleer.cu", "--fmad=true"), ("fast2d_pairs_minmod.cu", "--fmad=true"),
+         ("fast2d_pairs_superbee.cu", "--fmad=true"), ("fast2d_pairs_vanleer.cu", "--fmad=true"),
+         ("fast2d_pairs_mc.cu", "--fmad=true")]
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:

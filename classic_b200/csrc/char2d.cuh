@@ -173,8 +173,9 @@ template <> struct Pair<float> { using type = float2; };
 
 // ORD = method(2) (1: first order, no correction fluxes), TRN = method(3)
 // (0: no transverse propagation; 1: the fluctuations alone are split; 2: with
-// the correction fluxes incorporated, flux2.f90:186-195).
-template <typename real, int LIM, int BCM, int ORD = 2, int TRN = 2>
+// the correction fluxes incorporated, flux2.f90:186-195).  LIM is wave 1's
+// limiter (mthlim(1)), LIM2 wave 2's (mthlim(2)); -1 reads it at run time.
+template <typename real, int LIM, int BCM, int ORD = 2, int TRN = 2, int LIM2 = LIM>
 __global__ void __launch_bounds__(32 * WARPS2D, sizeof(real) == 8 ? CLAW_CHAR_MINB : CLAW_CHAR_MINB_F32)
 step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     static_assert((ORD == 1 || ORD == 2) && TRN >= 0 && TRN <= ORD, "transverse_waves <= order");
@@ -373,9 +374,9 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 [[maybe_unused]] real Fp0 = real(0), Fu0 = real(0), Fp1 = real(0), Fu1 = real(0);
                 if constexpr (ORD == 2) {
                     const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
-                    const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, A.lim2);
+                    const real l2_0 = limited_strength<real, LIM2>(a2_0, a2_L, A.lim2);
                     const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
-                    const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, A.lim2);
+                    const real l2_1 = limited_strength<real, LIM2>(a2_1, a2_0, A.lim2);
                     Fp0 = fxp * (l2_0 - l1_0);
                     Fu0 = fxu * (l1_0 + l2_0);
                     Fp1 = fxp * (l2_1 - l1_1);
@@ -440,7 +441,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                     Fvy[k] = real(0);
                     if constexpr (ORD == 2) {
                         const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
-                        const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim2); // upwind t-1
+                        const real b2 = limited_strength<real, LIM2>(a2y[k], a2y_lo[k], A.lim2); // upwind t-1
                         Fpy[k] = fyp * (b2 - b1);
                         Fvy[k] = fyv * (b1 + b2);
                     }

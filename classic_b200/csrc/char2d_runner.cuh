@@ -17,7 +17,7 @@
 
 namespace clawb200 {
 
-template <typename real, int LIM, int BCM, int ORD, int TRN>
+template <typename real, int LIM, int BCM, int ORD, int TRN, int LIM2 = LIM>
 struct CharRunner : Runner {
     CharArgs<real> args;
     int grid = 1, smem = 0;
@@ -49,12 +49,12 @@ struct CharRunner : Runner {
             if (rc) return rc;
         }
         smem = R::SMEM;
-        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, BCM, ORD, TRN>,
+        CUDA_TRY(cudaFuncSetAttribute(step2_char_kernel<real, LIM, BCM, ORD, TRN, LIM2>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int dev = 0, nsm = 0, per_sm = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM, ORD, TRN>,
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step2_char_kernel<real, LIM, BCM, ORD, TRN, LIM2>,
                                                                32 * WARPS2D, smem));
         if (per_sm < 1) return fail(CLAW_E_CUDA, "characteristic kernel cannot be resident");
         const long long full = (long long)nsm * per_sm * WARPS2D;
@@ -65,7 +65,7 @@ struct CharRunner : Runner {
     }
 
     cudaError_t launch(cudaStream_t s) override {
-        return launch_step(step2_char_kernel<real, LIM, BCM, ORD, TRN>, dim3(grid), dim3(32 * WARPS2D), smem, s,
+        return launch_step(step2_char_kernel<real, LIM, BCM, ORD, TRN, LIM2>, dim3(grid), dim3(32 * WARPS2D), smem, s,
                            args);
     }
 };
@@ -97,5 +97,51 @@ std::unique_ptr<Runner> char_order2_limited(bool fp32, int bcm, int trans) {
 extern template std::unique_ptr<Runner> char_order2_limited<1>(bool, int, int);
 extern template std::unique_ptr<Runner> char_order2_limited<2>(bool, int, int);
 extern template std::unique_ptr<Runner> char_order2_limited<3>(bool, int, int);
+
+// Order 2, transverse 2 with limiter L1 on wave 1 and L2 on wave 2 (L1 != L2,
+// both of minmod 1, superbee 2, van Leer 3, MC 4), every boundary mode; the
+// pairs with wave 1's limiter L1 are compiled in fast2d_pairs_<L1>.cu.
+template <int L1, int L2>
+std::unique_ptr<Runner> char_pair_limited(bool fp32, int bcm) {
+    if (fp32) {
+        if (bcm == CHAR_BC_PERX) return std::unique_ptr<Runner>(new CharRunner<float, L1, CHAR_BC_PERX, 2, 2, L2>());
+        if (bcm == CHAR_BC_EXTRAP) return std::unique_ptr<Runner>(new CharRunner<float, L1, CHAR_BC_EXTRAP, 2, 2, L2>());
+        return std::unique_ptr<Runner>(new CharRunner<float, L1, CHAR_BC_WALLS, 2, 2, L2>());
+    }
+    if (bcm == CHAR_BC_PERX) return std::unique_ptr<Runner>(new CharRunner<double, L1, CHAR_BC_PERX, 2, 2, L2>());
+    if (bcm == CHAR_BC_EXTRAP) return std::unique_ptr<Runner>(new CharRunner<double, L1, CHAR_BC_EXTRAP, 2, 2, L2>());
+    return std::unique_ptr<Runner>(new CharRunner<double, L1, CHAR_BC_WALLS, 2, 2, L2>());
+}
+
+#define CLAW_CHAR_PAIRS_OF(L1, A, B, C)                                                   \
+    extern template std::unique_ptr<Runner> char_pair_limited<L1, A>(bool, int);          \
+    extern template std::unique_ptr<Runner> char_pair_limited<L1, B>(bool, int);          \
+    extern template std::unique_ptr<Runner> char_pair_limited<L1, C>(bool, int);
+CLAW_CHAR_PAIRS_OF(1, 2, 3, 4)
+CLAW_CHAR_PAIRS_OF(2, 1, 3, 4)
+CLAW_CHAR_PAIRS_OF(3, 1, 2, 4)
+CLAW_CHAR_PAIRS_OF(4, 1, 2, 3)
+#undef CLAW_CHAR_PAIRS_OF
+
+// The compiled runner for wave limiters l1 != l2 at order 2, transverse 2, or
+// nullptr (another pair or setting: the limiters are read at run time).
+inline std::unique_ptr<Runner> char_pair_runner(int l1, int l2, bool fp32, int bcm) {
+    if (l1 < 1 || l1 > 4 || l2 < 1 || l2 > 4 || l1 == l2) return nullptr;
+    switch (l1 * 10 + l2) {
+        case 12: return char_pair_limited<1, 2>(fp32, bcm);
+        case 13: return char_pair_limited<1, 3>(fp32, bcm);
+        case 14: return char_pair_limited<1, 4>(fp32, bcm);
+        case 21: return char_pair_limited<2, 1>(fp32, bcm);
+        case 23: return char_pair_limited<2, 3>(fp32, bcm);
+        case 24: return char_pair_limited<2, 4>(fp32, bcm);
+        case 31: return char_pair_limited<3, 1>(fp32, bcm);
+        case 32: return char_pair_limited<3, 2>(fp32, bcm);
+        case 34: return char_pair_limited<3, 4>(fp32, bcm);
+        case 41: return char_pair_limited<4, 1>(fp32, bcm);
+        case 42: return char_pair_limited<4, 2>(fp32, bcm);
+        case 43: return char_pair_limited<4, 3>(fp32, bcm);
+    }
+    return nullptr;
+}
 
 }  // namespace clawb200

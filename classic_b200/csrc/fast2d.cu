@@ -8,13 +8,20 @@ namespace clawb200 {
 namespace {
 
 // (order, transverse_waves): at order 2 one limiter on both waves is compiled
-// in (MC here; minmod, superbee and van Leer in their own units); two
-// different limiters, none or Beam-Warming are read at run time (LIM = -1);
+// in (MC here; minmod, superbee and van Leer in their own units), and at
+// transverse 2 so is every pair of two different ones of these four (the
+// fast2d_pairs_*.cu units); other settings -- none or Beam-Warming on a wave,
+// a pair at transverse 0 or 1 -- read the limiters at run time (LIM = -1);
 // order 1 uses none.
 template <typename real, int BCM>
-std::unique_ptr<Runner> pick_lim(int lim, int order, int trans) {
+std::unique_ptr<Runner> pick_lim(int l1, int l2, int order, int trans) {
+    const int lim = l1 == l2 ? l1 : -1;
     if (order == 2) {
         if (trans < 0 || trans > 2) return nullptr;
+        if (lim == -1 && trans == 2) {
+            auto r = char_pair_runner(l1, l2, sizeof(real) == 4, BCM);
+            if (r) return r;
+        }
         if (lim == 4) return char_order2<real, 4, BCM>(trans);
         if (lim >= 1 && lim <= 3) {
             constexpr bool f32 = sizeof(real) == 4;
@@ -35,11 +42,10 @@ std::unique_ptr<Runner> pick(const claw_config& cfg) {
     bool extrap = true;
     for (int d = 0; d < 2; ++d) extrap = extrap && cfg.bc_lower[d] == BC_EXTRAP && cfg.bc_upper[d] == BC_EXTRAP;
     const int o = cfg.order, tr = cfg.transverse_waves;
-    // one limiter for both waves can be compiled in; two different ones are read at run time
-    const int lim = cfg.limiter[0] == cfg.limiter[1] ? cfg.limiter[0] : -1;
-    if (px) return pick_lim<real, CHAR_BC_PERX>(lim, o, tr);
-    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(lim, o, tr);
-    return pick_lim<real, CHAR_BC_WALLS>(lim, o, tr);
+    const int l1 = cfg.limiter[0], l2 = cfg.limiter[1];
+    if (px) return pick_lim<real, CHAR_BC_PERX>(l1, l2, o, tr);
+    if (extrap) return pick_lim<real, CHAR_BC_EXTRAP>(l1, l2, o, tr);
+    return pick_lim<real, CHAR_BC_WALLS>(l1, l2, o, tr);
 }
 
 }  // namespace

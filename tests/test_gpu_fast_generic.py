@@ -35,14 +35,16 @@ def _pair(rd, solver, params, q0, aux=None):
 
 
 @pytest.mark.parametrize("lim", ["minmod", "superbee", "vanleer", "mc", ("mc", "vanleer"),
+                                 ("superbee", "minmod"), ("vanleer", "mc"), ("minmod", "superbee"),
                                  ("none", "superbee"), ("minmod", 5)])
 @pytest.mark.parametrize("order,trans", [(1, 0), (1, 1), (2, 1), (2, 0), (2, 2)])
 @pytest.mark.parametrize("bc", [("wall", "extrap", "periodic", "periodic"), ("extrap",) * 4,
                                 ("periodic", "periodic", "wall", "wall")])
 def test_acoustics_fast(lim, order, trans, bc):
     """The characteristic kernel, with one limiter compiled in (minmod,
-    superbee, van Leer, MC) or a limiter per wave read at run time (any pair,
-    none and Beam-Warming included)."""
+    superbee, van Leer, MC), a pair of them compiled in (transverse 2), or the
+    limiters read at run time (pairs at transverse 0 and 1, none and
+    Beam-Warming)."""
     rd, solver, params, q0, _ = problems.random_acoustics_2d(
         45, 38, seed=9, limiter="mc", order=order, trans=trans, bc=bc)
     rd.clawdata.limiter = list(lim) if isinstance(lim, tuple) else [lim, lim]
