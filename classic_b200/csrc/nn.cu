@@ -154,8 +154,6 @@ __device__ __forceinline__ void ld16(uint32_t taddr, uint32_t* r) {
 }
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-template <int CIN, int COUT>
-__host__ __device__ constexpr int a_bytes() { return (CIN / 8) * NPX * 16; }
 }  // namespace tc
 
 // ------------------------------------- forward conv, tcgen05, persistent ---
