@@ -506,10 +506,12 @@ def other_configs(peaks, cpu=True):
                         "roofline": roofline_entry(rate, 48 if prec != "fp32" else 24, peaks)}
         except Exception as e:
             out[key] = {"error": str(e)}
-    # dimensionally split steps (dimsp2 / dimsp3), FP64 reference order
-    for key, dim, split in (("radial_2d_4096_godunov_split_fp64", 2, "godunov"),
-                            ("radial_2d_4096_strang_split_fp64", 2, "strang"),
-                            ("hetero_acoustics_3d_256_split_fp64", 3, "godunov")):
+    # dimensionally split steps (dimsp2 / dimsp3): FP64 reference order, and the
+    # contracted build of the 2D Godunov split
+    for key, dim, split, sprec in (("radial_2d_4096_godunov_split_fp64", 2, "godunov", "fp64"),
+                                   ("radial_2d_4096_godunov_split_fp64_fma", 2, "godunov", "fp64_fma"),
+                                   ("radial_2d_4096_strang_split_fp64", 2, "strang", "fp64"),
+                                   ("hetero_acoustics_3d_256_split_fp64", 3, "godunov", "fp64")):
         try:
             if dim == 2:
                 rd, solver, params, q0, aux = problems.radial_acoustics_2d(n=4096)
@@ -518,14 +520,14 @@ def other_configs(peaks, cpu=True):
                 rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=256)
                 t1, dt0, cells, nbytes = 0.1, 0.01, 256 ** 3, 80
             rd.clawdata.dimensional_split = split
-            s = Solver(rd.clawdata, solver, params, precision="fp64")
+            s = Solver(rd.clawdata, solver, params, precision=sprec)
             s.set_q(q0)
             if aux is not None:
                 s.set_aux(aux)
             info, st = s.advance(0.0, t1, dt0)
             s.close()
             rate = cells * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
-            kern = "split2_kernel_fp64" if split == "godunov" and dim == 2 else None
+            kern = "split2_kernel_fp64" if split == "godunov" and dim == 2 and sprec == "fp64" else None
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
                         "roofline": roofline_entry(rate, nbytes, peaks, kern, fp64_peak)}
