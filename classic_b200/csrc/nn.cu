@@ -15,6 +15,7 @@
 // targets, and the corrector's application with a per-tile conservative
 // projection and a positivity fallback to the plain step.
 #include <algorithm>
+#include <atomic>
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -696,42 +697,62 @@ int launch_fwd(const void* x, const void* w, const float* b, void* y, float* z, 
                int wd, cudaStream_t s) {
     constexpr int SM = tcp::smem_bytes<CIN, COUT>();
     auto k = conv3x3_fwd_tcp<CIN, COUT, ACT, OUTF32, SAVEZ>;
-    // one persistent CTA per SM (the driver's limit for a TMEM-allocating kernel)
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess ||
-        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
-        return NN_E_CUDA;
-    int dev = 0, nsm = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tcp::NTH, SM) != cudaSuccess || per_sm < 1)
-        return NN_E_CUDA;
-    const long long ntiles = (long long)n * (h / tc::TH) * (wd / tc::TW);
-    const long long groups = (ntiles + tcp::NPIPE - 1) / tcp::NPIPE;
-    const int grid = (int)std::min<long long>(groups, (long long)nsm * per_sm);
+    // One persistent CTA per SM (the driver's limit for a TMEM-allocating
+    // kernel).  The function attributes and the resident CTA count are set up
+    // once per device and instantiation (0 = not yet); a launch that fails
+    // with a cached set-up (a new context after cudaDeviceReset has lost the
+    // attributes) sets it up again and retries once.
+    constexpr int MAXDEV = 64;
+    static std::atomic<long long> resident[MAXDEV];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) return NN_E_CUDA;
+    auto setup = [&]() -> long long {
+        int nsm = 0, per_sm = 0;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SM) != cudaSuccess ||
+            cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tcp::NTH, SM) != cudaSuccess || per_sm < 1)
+            return 0;
+        const long long cap = (long long)nsm * per_sm;
+        resident[dev].store(cap, std::memory_order_release);
+        return cap;
+    };
     CUtensorMap map;
     if (halo_map(&map, x, n, h, wd, CIN) != 0) return NN_E_CUDA;
     const __nv_bfloat16* xb = static_cast<const __nv_bfloat16*>(x);
     const __nv_bfloat16* wb = static_cast<const __nv_bfloat16*>(w);
+    const long long ntiles = (long long)n * (h / tc::TH) * (wd / tc::TW);
+    const long long groups = (ntiles + tcp::NPIPE - 1) / tcp::NPIPE;
+    long long cap = resident[dev].load(std::memory_order_acquire);
+    const bool cached = cap != 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if (cap == 0 && (cap = setup()) == 0) return NN_E_CUDA;
+        const int grid = (int)std::min<long long>(groups, cap);
+        cudaError_t e;
 #if CLAW_PDL
-    // programmatic dependent launch: the CTAs' set-up overlaps the previous
-    // launch's tail (the kernel waits before touching its operands)
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(tcp::NTH);
-    cfg.dynamicSmemBytes = SM;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k, xb, wb, b, y, z, n, h, wd, map) != cudaSuccess) return NN_E_CUDA;
-    return 0;
+        // programmatic dependent launch: the CTAs' set-up overlaps the previous
+        // launch's tail (the kernel waits before touching its operands)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(tcp::NTH);
+        cfg.dynamicSmemBytes = SM;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, k, xb, wb, b, y, z, n, h, wd, map);
 #else
-    k<<<grid, tcp::NTH, SM, s>>>(xb, wb, b, y, z, n, h, wd, map);
-    return cudaGetLastError() == cudaSuccess ? 0 : NN_E_CUDA;
+        k<<<grid, tcp::NTH, SM, s>>>(xb, wb, b, y, z, n, h, wd, map);
+        e = cudaGetLastError();
 #endif
+        if (e == cudaSuccess) return 0;
+        if (!cached || attempt == 1) return NN_E_CUDA;
+        cap = 0;  // the cached set-up may be stale: redo it once
+    }
+    return NN_E_CUDA;
 }
 
 template <int CIN, int COUT>
