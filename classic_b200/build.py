@@ -48,7 +48,7 @@ UNITS = [("claw_b200.cu", "--fmad=false"), ("noalloc.cu", "--fmad=false"),
          ("fast2d_minmod.cu", "--fmad=true"), ("fast2d_superbee.cu", "--fmad=true"),
          ("fast2d_vanleer.cu", "--fmad=true"), ("fast2d_pairs_minmod.cu", "--fmad=true"),
          ("fast2d_pairs_superbee.cu", "--fmad=true"), ("fast2d_pairs_vanleer.cu", "--fmad=true"),
-         ("fast2d_pairs_mc.cu", "--fmad=true")]
+         ("fast2d_pairs_mc.cu", "--fmad=true"), ("split2d_char.cu", "--fmad=true")]
 
 
 def build_library(force: bool = False, verbose: bool = False) -> str:

@@ -95,6 +95,9 @@ std::unique_ptr<Runner> make_fast_runner2d(const claw_config& cfg);
 std::unique_ptr<Runner> make_split_runner(const claw_config& cfg);
 // its fused-multiply-add / FP32 build (split2d_fast.cu)
 std::unique_ptr<Runner> make_fast_split_runner(const claw_config& cfg);
+// characteristic-variable split step for 2D constant-coefficient acoustics
+// (split2d_char.cu), or nullptr
+std::unique_ptr<Runner> make_char_split_runner(const claw_config& cfg);
 
 // 3D step (step3d.cuh: one launch per sweep); nullptr if cfg is not served.
 std::unique_ptr<Runner> make_runner3d(const claw_config& cfg);

@@ -278,6 +278,74 @@ def test_fused_fp64_within_1e12(split):
     g.close()
 
 
+# Characteristic-variable split kernel (constant-coefficient acoustics in the
+# contracted FP64 and FP32 builds, char2ds.cuh): the same dimsp2 sweeps, q
+# within 1e-12 of the oracle, Courant numbers and dt sequence identical.
+@pytest.mark.parametrize("split", SPLITS)
+@pytest.mark.parametrize("mx,my", SIZES + [(121, 47), (300, 9)])
+@pytest.mark.parametrize("bc", BCS)
+def test_char_split_steps_within_1e12(split, mx, my, bc):
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(mx, my, seed=3 * mx + my, bc=bc)
+    rd.clawdata.dimensional_split = split
+    g, o = _pair(rd, solver, params, q0, precision="fp64_fma")
+    # Courant numbers 0.8 and 0.9 (c = 2 on [-1, 1]^2): a sweep above cfl_max
+    # would end dimsp2's step early, which claw2 then rejects
+    for frac in (0.8, 0.9):
+        dt = frac / max(mx, my)
+        cg, co = g.step(dt), o.step(dt)
+        assert cg == co
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 1e-12)
+    g.close()
+
+
+@pytest.mark.parametrize("split", SPLITS)
+@pytest.mark.parametrize("lim", ["none", "minmod", "superbee", "vanleer", "mc", ("mc", "vanleer"), ("minmod", 5)])
+def test_char_split_limiters_within_1e12(split, lim):
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(130, 67, seed=11,
+                                                            bc=("wall", "extrap", "periodic", "periodic"))
+    rd.clawdata.dimensional_split = split
+    rd.clawdata.limiter = list(lim) if isinstance(lim, tuple) else [lim, lim]
+    g, o = _pair(rd, solver, params, q0, precision="fp64_fma")
+    for _ in range(4):
+        assert g.step(0.005) == o.step(0.005)
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 1e-12)
+    g.close()
+
+
+@pytest.mark.parametrize("split", SPLITS)
+def test_char_split_advance_reject_and_abandon(split):
+    """claw2 with dimsp2 on the characteristic split kernel: a first dt far too
+    large (an abandoned sweep, then retries), then variable dt over three
+    frames; every statistic equal to the oracle's."""
+    rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=96, dt_initial=0.5)
+    rd.clawdata.dimensional_split = split
+    g, o = _pair(rd, solver, params, q0, precision="fp64_fma")
+    t, dg, do = 0.0, 0.5, 0.5
+    for _ in range(3):
+        ig, sg = g.advance(t, t + 0.1, dg)
+        io, so = o.advance(t, t + 0.1, do)
+        assert ig == io == 0
+        for key in ("t_reached", "dt_min", "dt_max_taken", "dt_next", "cfl_max_seen", "cfl_last",
+                    "steps_taken"):
+            assert sg[key] == so[key], key
+        assert np.all(rel_diff(g.get_q(), o.get_q()) <= 1e-12)
+        t, dg, do = sg["t_reached"], sg["dt_next"], so["dt_next"]
+    g.close()
+
+
+@pytest.mark.parametrize("split", SPLITS)
+@pytest.mark.parametrize("bc", BCS)
+def test_char_split_fp32_all_bcs(split, bc):
+    rd, solver, params, q0, _ = problems.random_acoustics_2d(90, 41, seed=5, bc=bc)
+    rd.clawdata.dimensional_split = split
+    g, o = _pair(rd, solver, params, q0, precision="fp32")
+    for _ in range(3):
+        cg, co = g.step(0.005), o.step(0.005)
+        assert abs(cg - co) <= 1e-12
+    assert np.all(rel_diff(g.get_q(), o.get_q()) <= 5e-6)
+    g.close()
+
+
 def test_3d_fused_fp64_within_1e12():
     rd, solver, params, q0, aux = problems.heterogeneous_acoustics_3d(n=40)
     rd.clawdata.dimensional_split = "godunov"
