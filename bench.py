@@ -507,10 +507,11 @@ def other_configs(peaks, cpu=True):
         except Exception as e:
             out[key] = {"error": str(e)}
     # dimensionally split steps (dimsp2 / dimsp3): FP64 reference order, and the
-    # contracted build of the 2D Godunov split
+    # 2D splits in characteristic variables (contracted FP64)
     for key, dim, split, sprec in (("radial_2d_4096_godunov_split_fp64", 2, "godunov", "fp64"),
                                    ("radial_2d_4096_godunov_split_fp64_fma", 2, "godunov", "fp64_fma"),
                                    ("radial_2d_4096_strang_split_fp64", 2, "strang", "fp64"),
+                                   ("radial_2d_4096_strang_split_fp64_fma", 2, "strang", "fp64_fma"),
                                    ("hetero_acoustics_3d_256_split_fp64", 3, "godunov", "fp64")):
         try:
             if dim == 2:
