@@ -528,7 +528,9 @@ def other_configs(peaks, cpu=True):
             info, st = s.advance(0.0, t1, dt0)
             s.close()
             rate = cells * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
-            kern = "split2_kernel_fp64" if split == "godunov" and dim == 2 and sprec == "fp64" else None
+            kern = None
+            if split == "godunov" and dim == 2:
+                kern = "split2_kernel_fp64" if sprec == "fp64" else "step2s_char_kernel_fp64_fma"
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
                         "roofline": roofline_entry(rate, nbytes, peaks, kern, fp64_peak)}
