@@ -1,5 +1,5 @@
 """Rollouts of the trained corrector on unseen seeds of the Euler
-four-quadrant family (coarse 256^2, judged against the block-averaged 1024^2
+four-quadrant family (coarse 256^2, measured against the block-averaged 1024^2
 FP64 plain run).
 
 The shipped network (classic_b200/data/corrector_euler_256.npz) was trained
