@@ -392,7 +392,8 @@ def other_configs(peaks, cpu=True):
         s.close()
         rate = 800 * steps / (ms * 1e-3)
         e = {"cell_updates_per_s": rate, "steps": steps, "device_ms": ms,
-             "note": "one CTA runs the whole claw1 loop per frame (latency-bound, one SM)",
+             "note": "one CTA runs the whole claw1 loop per frame (latency-bound, one SM); "
+                     "q (12.8 KB) stays on chip, so no DRAM traffic figure applies",
              "roofline": roofline_entry(rate, 32, peaks)}
         if cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -481,16 +482,21 @@ def other_configs(peaks, cpu=True):
     # run time).  4096^2; a first frame
     # (t 0 -> 0.02) warms up, the next (0.02 -> 0.05) is timed.
     char_kern = "step2_char_kernel"
-    for key, trans, lims, prec, kern in (
-            ("radial_2d_4096_trans1_fp64_fma", 1, ["mc", "mc"], "fp64_fma", char_kern + " (order 2, transverse 1)"),
-            ("radial_2d_4096_minmod_fp64_fma", 2, ["minmod", "minmod"], "fp64_fma", char_kern),
-            ("radial_2d_4096_superbee_fp64_fma", 2, ["superbee", "superbee"], "fp64_fma", char_kern),
-            ("radial_2d_4096_vanleer_fp64_fma", 2, ["vanleer", "vanleer"], "fp64_fma", char_kern),
-            ("radial_2d_4096_vanleer_fp32", 2, ["vanleer", "vanleer"], "fp32", char_kern),
+    for key, trans, lims, prec, kern, tkey in (
+            ("radial_2d_4096_trans1_fp64_fma", 1, ["mc", "mc"], "fp64_fma", char_kern + " (order 2, transverse 1)",
+             "step2_char_kernel_fp64_fma_trans1"),
+            ("radial_2d_4096_minmod_fp64_fma", 2, ["minmod", "minmod"], "fp64_fma", char_kern,
+             "step2_char_kernel_fp64_fma_minmod"),
+            ("radial_2d_4096_superbee_fp64_fma", 2, ["superbee", "superbee"], "fp64_fma", char_kern,
+             "step2_char_kernel_fp64_fma_superbee"),
+            ("radial_2d_4096_vanleer_fp64_fma", 2, ["vanleer", "vanleer"], "fp64_fma", char_kern,
+             "step2_char_kernel_fp64_fma_vanleer"),
+            ("radial_2d_4096_vanleer_fp32", 2, ["vanleer", "vanleer"], "fp32", char_kern,
+             "step2_char_kernel_fp32_vanleer"),
             ("radial_2d_4096_mixed_limiters_fp64_fma", 2, ["mc", "vanleer"], "fp64_fma",
-             char_kern + " (MC on wave 1, van Leer on wave 2, compiled in)"),
+             char_kern + " (MC on wave 1, van Leer on wave 2, compiled in)", "step2_char_kernel_fp64_fma_mc_vanleer"),
             ("radial_2d_4096_runtime_limiters_fp64_fma", 2, ["mc", "none"], "fp64_fma",
-             char_kern + " (limiters read at run time)")):
+             char_kern + " (limiters read at run time)", "step2_char_kernel_fp64_fma_runtime")):
         try:
             rd, solver, params, q0, _ = problems.radial_acoustics_2d(n=4096)
             rd.clawdata.transverse_waves = trans
@@ -503,7 +509,8 @@ def other_configs(peaks, cpu=True):
             rate = 4096 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
                         "kernel": kern, "limiters": lims,
-                        "roofline": roofline_entry(rate, 48 if prec != "fp32" else 24, peaks)}
+                        "roofline": roofline_entry(rate, 48 if prec != "fp32" else 24, peaks, tkey,
+                                                   fp64_peak)}
         except Exception as e:
             out[key] = {"error": str(e)}
     # dimensionally split steps (dimsp2 / dimsp3): FP64 reference order, and the
@@ -528,9 +535,12 @@ def other_configs(peaks, cpu=True):
             info, st = s.advance(0.0, t1, dt0)
             s.close()
             rate = cells * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
-            kern = None
-            if split == "godunov" and dim == 2:
+            if dim == 3:
+                kern = "split3_fp64"
+            elif split == "godunov":
                 kern = "split2_kernel_fp64" if sprec == "fp64" else "step2s_char_kernel_fp64_fma"
+            else:
+                kern = "split2_kernel_fp64_strang" if sprec == "fp64" else "step2s_char_kernel_fp64_fma_strang"
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"],
                         "device_ms": st["device_ms"],
                         "roofline": roofline_entry(rate, nbytes, peaks, kern, fp64_peak)}
@@ -551,7 +561,7 @@ def other_configs(peaks, cpu=True):
             rate = 2048 ** 2 * (st["steps_taken"] + st["steps_rejected"]) / (st["device_ms"] * 1e-3)
             out[key] = {"cell_updates_per_s": rate, "steps": st["steps_taken"], "device_ms": st["device_ms"],
                         "kernel": "step2_kernel (Euler Roe, MC, transverse 2)",
-                        "roofline": roofline_entry(rate, 64, peaks)}
+                        "roofline": roofline_entry(rate, 64, peaks, "step2_kernel_euler_" + prec, fp64_peak)}
         except Exception as e:
             out[key] = {"error": str(e)}
     sizes = problems.euler_ensemble_sizes(256, seed=0)

@@ -6,6 +6,15 @@
     python -m classic_b200.profile_step --n 2048 --split godunov --precision fp64
     python -m classic_b200.profile_step --nn --n 256 --steps 3
     python -m classic_b200.profile_step --batch 16 --n 512 --steps 3 --precision fp64_fma
+    python -m classic_b200.profile_step --n 3072 --limiter mc vanleer --transverse 1
+    python -m classic_b200.profile_step --euler --n 2048 --steps 3 --precision fp64
+
+--limiter takes one name (both waves) or two (wave 1, wave 2); --transverse
+sets transverse_waves (2D).
+
+With --euler each step is one claw_step of a single seeded four-quadrant Euler
+grid (seed 7, the generic kernel) at fixed dt = 0.6 dx / max(|u| + c) of the
+initial data.
 
 With --batch K each step is one launch of the batched Euler ensemble kernel
 over K seeded four-quadrant instances of n^2 cells (one claw_batch_advance
@@ -32,7 +41,31 @@ def main():
     ap.add_argument("--split", default="unsplit", choices=["unsplit", "godunov", "strang"])
     ap.add_argument("--nn", action="store_true", help="the corrector network's forward pass")
     ap.add_argument("--batch", type=int, default=0, help="Euler ensemble of this many instances")
+    ap.add_argument("--euler", action="store_true", help="one four-quadrant Euler grid")
+    ap.add_argument("--limiter", nargs="+", default=None,
+                    help="limiter name for both waves, or one per wave")
+    ap.add_argument("--transverse", type=int, default=2, choices=[0, 1, 2])
     args = ap.parse_args()
+    if args.limiter is not None and len(args.limiter) not in (1, 2):
+        ap.error("--limiter takes one or two names")
+    if args.euler:
+        import numpy as np
+        rd, solver, params, q0, aux = problems.euler_quadrants(n=args.n, seed=7)
+        gamma = float(params["gamma"])
+        rho, mu, mv, en = (np.asarray(q0[k], dtype=np.float64) for k in range(4))
+        u, v = mu / rho, mv / rho
+        p = (gamma - 1.0) * (en - 0.5 * rho * (u * u + v * v))
+        c = np.sqrt(gamma * p / rho)
+        smax = float(np.max(np.maximum(np.abs(u), np.abs(v)) + c))
+        s = Solver(rd.clawdata, solver, params, precision=args.precision)
+        s.set_q(q0)
+        dt = 0.6 * (1.0 / args.n) / smax
+        for _ in range(args.steps):
+            s.step(dt)
+        print(f"{args.steps} Euler steps of {args.n}^2 ({args.precision}), "
+              f"sum rho = {s.get_q()[0].sum():.12e}")
+        s.close()
+        return
     if args.batch:
         from .solver import BatchSolver
         insts = [problems.euler_quadrants(n=args.n, seed=1000 + k) for k in range(args.batch)]
@@ -66,6 +99,11 @@ def main():
         cmax = 1.0
         prec = args.precision
     rd.clawdata.dimensional_split = args.split
+    if args.limiter is not None:
+        lims = args.limiter if len(args.limiter) == 2 else args.limiter * 2
+        rd.clawdata.limiter = lims
+    if args.dim == 2:
+        rd.clawdata.transverse_waves = args.transverse
     s = Solver(rd.clawdata, solver, params, precision=prec)
     s.set_q(q0)
     if aux is not None:
