@@ -792,6 +792,15 @@ def main():
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
         configs = other_configs(peaks, cpu=args.cpu_steps > 0)
+        # the step kernel's FP64 pipe beside its HBM fraction: FP64
+        # thread-instructions per cell (ncu) at the timed rate against the probe
+        probe = configs.get("fp64_fma_probe", {}).get("tflops")
+        _, fp64_per_cell = kernel_stats({"fp64_fma": "step2_char_kernel_fp64_fma",
+                                         "fp64": "step2_kernel_fp64"}.get(args.precision, ""))
+        if probe and fp64_per_cell:
+            rate = cells / (per_launch_ms * 1e-3)
+            roofline["fp64_inst_per_cell"] = fp64_per_cell
+            roofline["fp64_frac"] = rate * fp64_per_cell / (probe / 2.0 * 1e12)
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_steps > 0:
