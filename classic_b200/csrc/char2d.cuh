@@ -198,17 +198,24 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     real* __restrict__ qnew = A.q[cur ^ 1];
     const CUtensorMap* tmq = &A.tmq[cur];
     const real c = A.s.cc, Z = A.s.zz, h = A.s.hz;
-    const real cZ = c * Z;
     // kappa = c(1 - c dt/dx): second-order coefficient (flux2.f90:156-157);
     // fadd = kappa/2 (Z(b2-b1), b1+b2); transverse gamma = (dt/dx) c/4,
     // delta = (dt/dx) c/(4Z), each scaled by the other direction's dt/d.
     const real kx = c * (real(1) - c * dtdx), ky = c * (real(1) - c * dtdy);
-    const real fxp = real(0.5) * kx * Z, fxu = real(0.5) * kx;
-    const real fyp = real(0.5) * ky * Z, fyv = real(0.5) * ky;
     const real gx = dtdy * (dtdx * c * real(0.25)), dx4 = dtdy * (dtdx * c * real(0.25) / Z);
     const real gy = dtdx * (dtdy * c * real(0.25)), dy4 = dtdx * (dtdy * c * real(0.25) / Z);
-    const real qpx = dtdx * cZ, qux = dtdx * c;
-    const real qpy = dtdy * cZ, qvy = dtdy * c;
+    // The march carries the strengths unscaled, 2Z a1 = Z du - dp and
+    // 2Z a2 = Z du + dp, and the correction fluxes doubled, F' = 2 F
+    // (fadd above): every limiter is positively homogeneous of degree one and
+    // every use of a strength or a flux is linear, so the factors 1/(2Z) and
+    // 2 sit in these coefficients instead of costing a multiply per interface
+    // (Z / (2Z) = 1/2).
+    const real fxp2 = real(0.5) * kx, fxu2 = kx * h;                // Fp', Fu'
+    const real fyp2 = real(0.5) * ky, fyv2 = ky * h;                // Fp', Fv'
+    const real qpxh = real(0.5) * (dtdx * c), quxh = dtdx * c * h;  // dt/dx cZ, dt/dx c over 2Z
+    const real qpyh = real(0.5) * (dtdy * c), qvyh = dtdy * c * h;
+    const real cZh = real(0.5) * c;                                  // cZ over 2Z
+    const real dtdx2 = real(0.5) * dtdx, dtdy2 = real(0.5) * dtdy;  // dt/d on F' differences
 
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -338,8 +345,8 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 for (int k = 0; k < 2; ++k) {
                     const real dp = pc[k] - p0[k];
                     const real dv = vc[k] - v0[k];
-                    a1y[k] = (Z * dv - dp) * h;
-                    a2y[k] = (Z * dv + dp) * h;
+                    a1y[k] = Z * dv - dp;
+                    a2y[k] = Z * dv + dp;
                 }
             }
 
@@ -364,10 +371,10 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 fetch2(qn, srn, ngn, 2, vn[0], vn[1]);
 
                 // ---- x-slice t: interfaces I0 = (c0-1 | c0) and I1 = (c0 | c1) ----
-                const real a1_0 = (Z * (u[0] - uM) - (p[0] - pM)) * h;
-                const real a2_0 = (Z * (u[0] - uM) + (p[0] - pM)) * h;
-                const real a1_1 = (Z * (u[1] - u[0]) - (p[1] - p[0])) * h;
-                const real a2_1 = (Z * (u[1] - u[0]) + (p[1] - p[0])) * h;
+                const real a1_0 = Z * (u[0] - uM) - (p[0] - pM);
+                const real a2_0 = Z * (u[0] - uM) + (p[0] - pM);
+                const real a1_1 = Z * (u[1] - u[0]) - (p[1] - p[0]);
+                const real a2_1 = Z * (u[1] - u[0]) + (p[1] - p[0]);
                 const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
                 const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
                 // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
@@ -377,19 +384,19 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                     const real l2_0 = limited_strength<real, LIM2>(a2_0, a2_L, A.lim2);
                     const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
                     const real l2_1 = limited_strength<real, LIM2>(a2_1, a2_0, A.lim2);
-                    Fp0 = fxp * (l2_0 - l1_0);
-                    Fu0 = fxu * (l1_0 + l2_0);
-                    Fp1 = fxp * (l2_1 - l1_1);
-                    Fu1 = fxu * (l1_1 + l2_1);
+                    Fp0 = fxp2 * (l2_0 - l1_0);
+                    Fu0 = fxu2 * (l1_0 + l2_0);
+                    Fp1 = fxp2 * (l2_1 - l1_1);
+                    Fu1 = fxu2 * (l1_1 + l2_1);
                 }
                 // pressure parts of amdq (+ cqxx) and apdq (- cqxx), the fluctuations rpt2 splits
                 auto amq = [&](real a, real F) -> real {
-                    if constexpr (TRN == 2) return fma(cZ, a, real(2) * F);
-                    else return cZ * a;
+                    if constexpr (TRN == 2) return fma(cZh, a, F);
+                    else return cZh * a;
                 };
                 auto apq = [&](real a, real F) -> real {
-                    if constexpr (TRN == 2) return fma(cZ, a, real(-2) * F);
-                    else return cZ * a;
+                    if constexpr (TRN == 2) return fma(cZh, a, -F);
+                    else return cZh * a;
                 };
                 [[maybe_unused]] real FpR = real(0), FuR = real(0);
                 if constexpr (ORD == 2) {
@@ -399,17 +406,17 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0
                 real q3[2][3];
                 {
-                    real n00 = (p[0] + axp[0]) - qpx * (a2_0 + a1_1);
-                    real n01 = u[0] + qux * (a1_1 - a2_0);
+                    real n00 = (p[0] + axp[0]) - qpxh * (a2_0 + a1_1);
+                    real n01 = u[0] + quxh * (a1_1 - a2_0);
                     const real n02 = v[0] + axv[0];
-                    real n10 = (p[1] + axp[1]) - qpx * (a2_1 + a1_R);
-                    real n11 = u[1] + qux * (a1_R - a2_1);
+                    real n10 = (p[1] + axp[1]) - qpxh * (a2_1 + a1_R);
+                    real n11 = u[1] + quxh * (a1_R - a2_1);
                     const real n12 = v[1] + axv[1];
                     if constexpr (ORD == 2) {
-                        n00 = n00 - dtdx * (Fp1 - Fp0);
-                        n01 = n01 - dtdx * (Fu1 - Fu0);
-                        n10 = n10 - dtdx * (FpR - Fp1);
-                        n11 = n11 - dtdx * (FuR - Fu1);
+                        n00 = n00 - dtdx2 * (Fp1 - Fp0);
+                        n01 = n01 - dtdx2 * (Fu1 - Fu0);
+                        n10 = n10 - dtdx2 * (FpR - Fp1);
+                        n11 = n11 - dtdx2 * (FuR - Fu1);
                     }
                     if constexpr (TRN > 0) {
                         const real A1R = __shfl_down_sync(FULL, amq(a1_0, Fp0), 1);
@@ -435,24 +442,24 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const real dp = pn[k] - p[k], dv = vn[k] - v[k];
-                    a1n[k] = (Z * dv - dp) * h;
-                    a2n[k] = (Z * dv + dp) * h;
+                    a1n[k] = Z * dv - dp;
+                    a2n[k] = Z * dv + dp;
                     Fpy[k] = real(0);
                     Fvy[k] = real(0);
                     if constexpr (ORD == 2) {
                         const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
                         const real b2 = limited_strength<real, LIM2>(a2y[k], a2y_lo[k], A.lim2); // upwind t-1
-                        Fpy[k] = fyp * (b2 - b1);
-                        Fvy[k] = fyv * (b1 + b2);
+                        Fpy[k] = fyp2 * (b2 - b1);
+                        Fvy[k] = fyv2 * (b1 + b2);
                     }
                     const real A1y = amq(a1y[k], Fpy[k]);  // into cell t-1
                     A2y[k] = apq(a2y[k], Fpy[k]);          // into cell t
-                    o[k][0] = q3[k][0] - qpy * (a2y_lo[k] + a1y[k]);
+                    o[k][0] = q3[k][0] - qpyh * (a2y_lo[k] + a1y[k]);
                     o[k][1] = q3[k][1];
-                    o[k][2] = q3[k][2] + qvy * (a1y[k] - a2y_lo[k]);
+                    o[k][2] = q3[k][2] + qvyh * (a1y[k] - a2y_lo[k]);
                     if constexpr (ORD == 2) {
-                        o[k][0] = o[k][0] - dtdy * (Fpy[k] - Fpy_lo[k]);
-                        o[k][2] = o[k][2] - dtdy * (Fvy[k] - Fvy_lo[k]);
+                        o[k][0] = o[k][0] - dtdy2 * (Fpy[k] - Fpy_lo[k]);
+                        o[k][2] = o[k][2] - dtdy2 * (Fvy[k] - Fvy_lo[k]);
                     }
                     hS[k] = kS[k] = real(0);
                     if constexpr (TRN > 0) {
