@@ -205,17 +205,18 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     const real gx = dtdy * (dtdx * c * real(0.25)), dx4 = dtdy * (dtdx * c * real(0.25) / Z);
     const real gy = dtdx * (dtdy * c * real(0.25)), dy4 = dtdx * (dtdy * c * real(0.25) / Z);
     // The march carries the strengths unscaled, 2Z a1 = Z du - dp and
-    // 2Z a2 = Z du + dp, and the correction fluxes doubled, F' = 2 F
-    // (fadd above): every limiter is positively homogeneous of degree one and
-    // every use of a strength or a flux is linear, so the factors 1/(2Z) and
-    // 2 sit in these coefficients instead of costing a multiply per interface
-    // (Z / (2Z) = 1/2).
-    const real fxp2 = real(0.5) * kx, fxu2 = kx * h;                // Fp', Fu'
-    const real fyp2 = real(0.5) * ky, fyv2 = ky * h;                // Fp', Fv'
+    // 2Z a2 = Z du + dp; the pressure correction flux doubled, Fp' = 2 Fp;
+    // and for the velocity correction flux, which enters only its own
+    // difference, the bare sum s = b1 + b2.  Every limiter is positively
+    // homogeneous of degree one and every use of a strength or a flux is
+    // linear, so the factors 1/(2Z), 2 and kappa/2 sit in these coefficients
+    // instead of costing a multiply per interface (Z / (2Z) = 1/2).
+    const real fxp2 = real(0.5) * kx, fyp2 = real(0.5) * ky;        // Fp' per (b2 - b1)
+    const real kux = real(0.5) * (dtdx * kx * h), kvy = real(0.5) * (dtdy * ky * h);  // dt/d Fu per s
     const real qpxh = real(0.5) * (dtdx * c), quxh = dtdx * c * h;  // dt/dx cZ, dt/dx c over 2Z
     const real qpyh = real(0.5) * (dtdy * c), qvyh = dtdy * c * h;
     const real cZh = real(0.5) * c;                                  // cZ over 2Z
-    const real dtdx2 = real(0.5) * dtdx, dtdy2 = real(0.5) * dtdy;  // dt/d on F' differences
+    const real dtdx2 = real(0.5) * dtdx, dtdy2 = real(0.5) * dtdy;  // dt/d on Fp' differences
 
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -324,7 +325,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
             real q2p[2][3] = {};            // x-part of (c_k, t) awaiting row t+1's transfer
             real axp[2] = {}, axv[2] = {};  // x-slice t-1 -> row t (p, v)
             real a1y[2] = {}, a2y[2] = {};  // y-interface t strengths
-            real a2y_lo[2] = {}, A2y_lo[2] = {}, Fpy_lo[2] = {}, Fvy_lo[2] = {};  // y-interface t-1
+            real a2y_lo[2] = {}, Fpy_lo[2] = {}, Svy_lo[2] = {};  // y-interface t-1
             real pc[2] = {}, vc[2] = {};    // p, v of row t (row t+1 of the previous trip)
             int last_issued = rfirst + (nrows < RING ? nrows : RING) - 1;
             int fail_row = rlast + 1;
@@ -378,49 +379,51 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
                 const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
                 // wave 1 (speed -c) looks right, wave 2 (speed +c) looks left
-                [[maybe_unused]] real Fp0 = real(0), Fu0 = real(0), Fp1 = real(0), Fu1 = real(0);
+                [[maybe_unused]] real Fp0 = real(0), Su0 = real(0), Fp1 = real(0), Su1 = real(0);
                 if constexpr (ORD == 2) {
                     const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, A.lim);
                     const real l2_0 = limited_strength<real, LIM2>(a2_0, a2_L, A.lim2);
                     const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, A.lim);
                     const real l2_1 = limited_strength<real, LIM2>(a2_1, a2_0, A.lim2);
                     Fp0 = fxp2 * (l2_0 - l1_0);
-                    Fu0 = fxu2 * (l1_0 + l2_0);
+                    Su0 = l1_0 + l2_0;
                     Fp1 = fxp2 * (l2_1 - l1_1);
-                    Fu1 = fxu2 * (l1_1 + l2_1);
+                    Su1 = l1_1 + l2_1;
                 }
-                // pressure parts of amdq (+ cqxx) and apdq (- cqxx), the fluctuations rpt2 splits
-                auto amq = [&](real a, real F) -> real {
-                    if constexpr (TRN == 2) return fma(cZh, a, F);
-                    else return cZh * a;
-                };
-                auto apq = [&](real a, real F) -> real {
-                    if constexpr (TRN == 2) return fma(cZh, a, -F);
-                    else return cZh * a;
-                };
-                [[maybe_unused]] real FpR = real(0), FuR = real(0);
+                [[maybe_unused]] real FpR = real(0), SuR = real(0);
                 if constexpr (ORD == 2) {
                     FpR = __shfl_down_sync(FULL, Fp0, 1);
-                    FuR = __shfl_down_sync(FULL, Fu0, 1);
+                    SuR = __shfl_down_sync(FULL, Su0, 1);
                 }
-                // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0
+                // cell c0: interfaces I0 (left) and I1 (right); cell c1: I1 and lane+1's I0.
+                // X = the strengths entering the cell (apdq of its left interface,
+                // amdq of its right one), D = the difference of its Fp'.
                 real q3[2][3];
                 {
-                    real n00 = (p[0] + axp[0]) - qpxh * (a2_0 + a1_1);
+                    const real X0 = a2_0 + a1_1, X1 = a2_1 + a1_R;
+                    [[maybe_unused]] real D0 = real(0), D1 = real(0);
+                    if constexpr (ORD == 2) {
+                        D0 = Fp1 - Fp0;
+                        D1 = FpR - Fp1;
+                    }
+                    real n00 = (p[0] + axp[0]) - qpxh * X0;
                     real n01 = u[0] + quxh * (a1_1 - a2_0);
                     const real n02 = v[0] + axv[0];
-                    real n10 = (p[1] + axp[1]) - qpxh * (a2_1 + a1_R);
+                    real n10 = (p[1] + axp[1]) - qpxh * X1;
                     real n11 = u[1] + quxh * (a1_R - a2_1);
                     const real n12 = v[1] + axv[1];
                     if constexpr (ORD == 2) {
-                        n00 = n00 - dtdx2 * (Fp1 - Fp0);
-                        n01 = n01 - dtdx2 * (Fu1 - Fu0);
-                        n10 = n10 - dtdx2 * (FpR - Fp1);
-                        n11 = n11 - dtdx2 * (FuR - Fu1);
+                        n00 = n00 - dtdx2 * D0;
+                        n01 = n01 - kux * (Su1 - Su0);
+                        n10 = n10 - dtdx2 * D1;
+                        n11 = n11 - kux * (SuR - Su1);
                     }
                     if constexpr (TRN > 0) {
-                        const real A1R = __shfl_down_sync(FULL, amq(a1_0, Fp0), 1);
-                        const real S0 = amq(a1_1, Fp1) + apq(a2_0, Fp0), S1 = A1R + apq(a2_1, Fp1);
+                        // pressure part of the cell's amdq(right) + apdq(left), the
+                        // fluctuations rpt2 splits (with + cqxx and - cqxx at
+                        // transverse 2): cZ/(2Z) X (+ D)
+                        const real S0 = TRN == 2 ? fma(cZh, X0, D0) : cZh * X0;
+                        const real S1 = TRN == 2 ? fma(cZh, X1, D1) : cZh * X1;
                         const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
                         n00 = n00 + real(2) * gS0;
                         n10 = n10 + real(2) * gS1;
@@ -438,32 +441,34 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 }
 
                 // ---- y: interface t+1 raw, interface t limited, y-part of (c_k, t-1) ----
-                real hS[2], kS[2], o[2][3], Fpy[2], Fvy[2], A2y[2], a1n[2], a2n[2];
+                real hS[2], kS[2], o[2][3], Fpy[2], Svy[2], a1n[2], a2n[2];
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const real dp = pn[k] - p[k], dv = vn[k] - v[k];
                     a1n[k] = Z * dv - dp;
                     a2n[k] = Z * dv + dp;
                     Fpy[k] = real(0);
-                    Fvy[k] = real(0);
+                    Svy[k] = real(0);
                     if constexpr (ORD == 2) {
                         const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);    // upwind t+1
                         const real b2 = limited_strength<real, LIM2>(a2y[k], a2y_lo[k], A.lim2); // upwind t-1
                         Fpy[k] = fyp2 * (b2 - b1);
-                        Fvy[k] = fyv2 * (b1 + b2);
+                        Svy[k] = b1 + b2;
                     }
-                    const real A1y = amq(a1y[k], Fpy[k]);  // into cell t-1
-                    A2y[k] = apq(a2y[k], Fpy[k]);          // into cell t
-                    o[k][0] = q3[k][0] - qpyh * (a2y_lo[k] + a1y[k]);
+                    // cell t-1: amdq of interface t and apdq of interface t-1 enter it
+                    const real Y = a2y_lo[k] + a1y[k];
+                    [[maybe_unused]] real Dy = real(0);
+                    if constexpr (ORD == 2) Dy = Fpy[k] - Fpy_lo[k];
+                    o[k][0] = q3[k][0] - qpyh * Y;
                     o[k][1] = q3[k][1];
                     o[k][2] = q3[k][2] + qvyh * (a1y[k] - a2y_lo[k]);
                     if constexpr (ORD == 2) {
-                        o[k][0] = o[k][0] - dtdy2 * (Fpy[k] - Fpy_lo[k]);
-                        o[k][2] = o[k][2] - dtdy2 * (Fvy[k] - Fvy_lo[k]);
+                        o[k][0] = o[k][0] - dtdy2 * Dy;
+                        o[k][2] = o[k][2] - kvy * (Svy[k] - Svy_lo[k]);
                     }
                     hS[k] = kS[k] = real(0);
                     if constexpr (TRN > 0) {
-                        const real Sy = A1y + A2y_lo[k];
+                        const real Sy = TRN == 2 ? fma(cZh, Y, Dy) : cZh * Y;
                         hS[k] = gy * Sy;
                         kS[k] = dy4 * Sy;
                         o[k][0] = o[k][0] + real(2) * hS[k];
@@ -495,9 +500,8 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     a2y_lo[k] = a2y[k];
-                    A2y_lo[k] = A2y[k];
                     Fpy_lo[k] = Fpy[k];
-                    Fvy_lo[k] = Fvy[k];
+                    Svy_lo[k] = Svy[k];
                     a1y[k] = a1n[k];
                     a2y[k] = a2n[k];
                     pc[k] = pn[k];
