@@ -35,21 +35,27 @@
 
 namespace clawb200 {
 
+// Coefficients of one x-sweep.  The sweep carries the wave strengths
+// unscaled (2Z a1 = Z du - dp, 2Z a2 = Z du + dp) and the correction fluxes as
+// the bare limited sums d = b2 - b1 (pressure) and s = b1 + b2 (velocity):
+// every limiter is positively homogeneous of degree one and each flux enters
+// only its own difference, so 1/(2Z) and kappa/2 sit in these coefficients
+// (Z / (2Z) = 1/2).
 template <typename real>
 struct CharSplitConsts {
-    real dtdx, qpx, qux, fxp, fxu;  // one x-sweep
+    real qpxh, quxh;  // dt/dx cZ and dt/dx c, over 2Z
+    real kpx, kux;    // dt/dx kappa Z/2 and dt/dx kappa/2, over 2Z
 };
 
 template <typename real>
 __device__ __forceinline__ CharSplitConsts<real> char_xsweep_consts(double dtdx_d, const CharAcoustics2D<real>& S) {
     CharSplitConsts<real> k;
-    const real dtdx = (real)dtdx_d, c = S.cc, Z = S.zz;
+    const real dtdx = (real)dtdx_d, c = S.cc, h = S.hz;
     const real kx = c * (real(1) - c * dtdx);
-    k.dtdx = dtdx;
-    k.qpx = dtdx * (c * Z);
-    k.qux = dtdx * c;
-    k.fxp = real(0.5) * kx * Z;
-    k.fxu = real(0.5) * kx;
+    k.qpxh = real(0.5) * (dtdx * c);
+    k.quxh = dtdx * c * h;
+    k.kpx = real(0.25) * (dtdx * kx);
+    k.kux = real(0.5) * (dtdx * kx * h);
     return k;
 }
 
@@ -62,24 +68,24 @@ __device__ __forceinline__ void char_xsweep(real pM, real uM, real p0, real u0, 
                                             const CharSplitConsts<real>& K, const CharAcoustics2D<real>& S,
                                             int lim, int lim2, real& xp0, real& xu0, real& xp1, real& xu1) {
     constexpr unsigned FULL = 0xffffffffu;
-    const real Z = S.zz, h = S.hz;
-    const real a1_0 = (Z * (u0 - uM) - (p0 - pM)) * h;
-    const real a2_0 = (Z * (u0 - uM) + (p0 - pM)) * h;
-    const real a1_1 = (Z * (u1 - u0) - (p1 - p0)) * h;
-    const real a2_1 = (Z * (u1 - u0) + (p1 - p0)) * h;
+    const real Z = S.zz;
+    const real a1_0 = Z * (u0 - uM) - (p0 - pM);
+    const real a2_0 = Z * (u0 - uM) + (p0 - pM);
+    const real a1_1 = Z * (u1 - u0) - (p1 - p0);
+    const real a2_1 = Z * (u1 - u0) + (p1 - p0);
     const real a1_R = __shfl_down_sync(FULL, a1_0, 1);  // interface c1+1 (lane+1's I0)
     const real a2_L = __shfl_up_sync(FULL, a2_1, 1);    // interface c0-1 (lane-1's I1)
     const real l1_0 = limited_strength<real, LIM>(a1_0, a1_1, lim);
     const real l2_0 = limited_strength<real, LIM>(a2_0, a2_L, lim2);
     const real l1_1 = limited_strength<real, LIM>(a1_1, a1_R, lim);
     const real l2_1 = limited_strength<real, LIM>(a2_1, a2_0, lim2);
-    const real Fp0 = K.fxp * (l2_0 - l1_0), Fu0 = K.fxu * (l1_0 + l2_0);
-    const real Fp1 = K.fxp * (l2_1 - l1_1), Fu1 = K.fxu * (l1_1 + l2_1);
-    const real FpR = __shfl_down_sync(FULL, Fp0, 1), FuR = __shfl_down_sync(FULL, Fu0, 1);
-    xp0 = (p0 - K.qpx * (a2_0 + a1_1)) - K.dtdx * (Fp1 - Fp0);
-    xu0 = (u0 + K.qux * (a1_1 - a2_0)) - K.dtdx * (Fu1 - Fu0);
-    xp1 = (p1 - K.qpx * (a2_1 + a1_R)) - K.dtdx * (FpR - Fp1);
-    xu1 = (u1 + K.qux * (a1_R - a2_1)) - K.dtdx * (FuR - Fu1);
+    const real d0 = l2_0 - l1_0, s0 = l1_0 + l2_0;
+    const real d1 = l2_1 - l1_1, s1 = l1_1 + l2_1;
+    const real dR = __shfl_down_sync(FULL, d0, 1), sR = __shfl_down_sync(FULL, s0, 1);
+    xp0 = (p0 - K.qpxh * (a2_0 + a1_1)) - K.kpx * (d1 - d0);
+    xu0 = (u0 + K.quxh * (a1_1 - a2_0)) - K.kux * (s1 - s0);
+    xp1 = (p1 - K.qpxh * (a2_1 + a1_R)) - K.kpx * (dR - d1);
+    xu1 = (u1 + K.quxh * (a1_R - a2_1)) - K.kux * (sR - s1);
 }
 
 constexpr int STRIP_STRANG = 56;  // output columns of a Strang strip (lanes 2..29)
@@ -111,8 +117,9 @@ step2s_char_kernel(const __grid_constant__ CharArgs<real> A) {
     const real c = A.s.cc, Z = A.s.zz, h = A.s.hz;
     const real dtdy = (real)dtdy_d;
     const real ky = c * (real(1) - c * dtdy);
-    const real fyp = real(0.5) * ky * Z, fyv = real(0.5) * ky;
-    const real qpy = dtdy * (c * Z), qvy = dtdy * c;
+    // the y-sweep's coefficients, scaled as the x-sweep's (char_xsweep_consts)
+    const real qpyh = real(0.5) * (dtdy * c), qvyh = dtdy * c * h;
+    const real kpy = real(0.25) * (dtdy * ky), kvy = real(0.5) * (dtdy * ky * h);
     const real* __restrict__ qold = A.q[cur];
     real* __restrict__ qnew = A.q[cur ^ 1];
     const CUtensorMap* tmq = &A.tmq[cur];
@@ -240,7 +247,7 @@ step2s_char_kernel(const __grid_constant__ CharArgs<real> A) {
             // t (between them) and t-1 (below)
             real xb[2][3], xc[2][3];
             real a1y[2], a2y[2];
-            real a2y_lo[2] = {}, Fpy_lo[2] = {}, Fvy_lo[2] = {};
+            real a2y_lo[2] = {}, dy_lo[2] = {}, sy_lo[2] = {};
             int last_issued = rfirst + (nrows < RING ? nrows : RING) - 1;
             int fail_row = rlast + 1;
 
@@ -251,8 +258,8 @@ step2s_char_kernel(const __grid_constant__ CharArgs<real> A) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const real dp = xc[k][0] - xb[k][0], dv = xc[k][2] - xb[k][2];
-                    a1y[k] = (Z * dv - dp) * h;
-                    a2y[k] = (Z * dv + dp) * h;
+                    a1y[k] = Z * dv - dp;
+                    a2y[k] = Z * dv + dp;
                 }
             }
 
@@ -261,19 +268,19 @@ step2s_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 real xn[2][3];
                 stage_a(t + 1, xn);
                 // ---- stage B: interface t+1 raw, interface t limited, row t-1 updated
-                real o[2][3], Fpy[2], Fvy[2], a1n[2], a2n[2];
+                real o[2][3], dyk[2], syk[2], a1n[2], a2n[2];
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const real dp = xn[k][0] - xc[k][0], dv = xn[k][2] - xc[k][2];
-                    a1n[k] = (Z * dv - dp) * h;
-                    a2n[k] = (Z * dv + dp) * h;
+                    a1n[k] = Z * dv - dp;
+                    a2n[k] = Z * dv + dp;
                     const real b1 = limited_strength<real, LIM>(a1y[k], a1n[k], A.lim);      // upwind t+1
                     const real b2 = limited_strength<real, LIM>(a2y[k], a2y_lo[k], A.lim2);  // upwind t-1
-                    Fpy[k] = fyp * (b2 - b1);
-                    Fvy[k] = fyv * (b1 + b2);
-                    o[k][0] = (xb[k][0] - qpy * (a2y_lo[k] + a1y[k])) - dtdy * (Fpy[k] - Fpy_lo[k]);
+                    dyk[k] = b2 - b1;
+                    syk[k] = b1 + b2;
+                    o[k][0] = (xb[k][0] - qpyh * (a2y_lo[k] + a1y[k])) - kpy * (dyk[k] - dy_lo[k]);
                     o[k][1] = xb[k][1];
-                    o[k][2] = (xb[k][2] + qvy * (a1y[k] - a2y_lo[k])) - dtdy * (Fvy[k] - Fvy_lo[k]);
+                    o[k][2] = (xb[k][2] + qvyh * (a1y[k] - a2y_lo[k])) - kvy * (syk[k] - sy_lo[k]);
                 }
                 if constexpr (STRANG) {
                     // ---- stage C: the y-swept row t-1 x-swept with dt/2; column
@@ -301,8 +308,8 @@ step2s_char_kernel(const __grid_constant__ CharArgs<real> A) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     a2y_lo[k] = a2y[k];
-                    Fpy_lo[k] = Fpy[k];
-                    Fvy_lo[k] = Fvy[k];
+                    dy_lo[k] = dyk[k];
+                    sy_lo[k] = syk[k];
                     a1y[k] = a1n[k];
                     a2y[k] = a2n[k];
 #pragma unroll
