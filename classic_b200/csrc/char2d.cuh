@@ -204,6 +204,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
     const real kx = c * (real(1) - c * dtdx), ky = c * (real(1) - c * dtdy);
     const real gx = dtdy * (dtdx * c * real(0.25)), dx4 = dtdy * (dtdx * c * real(0.25) / Z);
     const real gy = dtdx * (dtdy * c * real(0.25)), dy4 = dtdx * (dtdy * c * real(0.25) / Z);
+    const real gx2 = real(2) * gx, gy2 = real(2) * gy;
     // The march carries the strengths unscaled, 2Z a1 = Z du - dp and
     // 2Z a2 = Z du + dp; the pressure correction flux doubled, Fp' = 2 Fp;
     // and for the velocity correction flux, which enters only its own
@@ -323,7 +324,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
 
             // carried per column k = 0, 1
             real q2p[2][3] = {};            // x-part of (c_k, t) awaiting row t+1's transfer
-            real axp[2] = {}, axv[2] = {};  // x-slice t-1 -> row t (p, v)
+            [[maybe_unused]] real sxp[2] = {};  // x-slice t-1's transverse sum S, whose split reaches row t
             real a1y[2] = {}, a2y[2] = {};  // y-interface t strengths
             real a2y_lo[2] = {}, Fpy_lo[2] = {}, Svy_lo[2] = {};  // y-interface t-1
             real pc[2] = {}, vc[2] = {};    // p, v of row t (row t+1 of the previous trip)
@@ -406,12 +407,19 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                         D0 = Fp1 - Fp0;
                         D1 = FpR - Fp1;
                     }
-                    real n00 = (p[0] + axp[0]) - qpxh * X0;
+                    real pt0 = p[0], pt1 = p[1], vt0 = v[0], vt1 = v[1];
+                    if constexpr (TRN > 0) {  // row t's share of the split of slice t-1
+                        pt0 = fma(-gx, sxp[0], pt0);
+                        pt1 = fma(-gx, sxp[1], pt1);
+                        vt0 = fma(-dx4, sxp[0], vt0);
+                        vt1 = fma(-dx4, sxp[1], vt1);
+                    }
+                    real n00 = pt0 - qpxh * X0;
                     real n01 = u[0] + quxh * (a1_1 - a2_0);
-                    const real n02 = v[0] + axv[0];
-                    real n10 = (p[1] + axp[1]) - qpxh * X1;
+                    const real n02 = vt0;
+                    real n10 = pt1 - qpxh * X1;
                     real n11 = u[1] + quxh * (a1_R - a2_1);
-                    const real n12 = v[1] + axv[1];
+                    const real n12 = vt1;
                     if constexpr (ORD == 2) {
                         n00 = n00 - dtdx2 * D0;
                         n01 = n01 - kux * (Su1 - Su0);
@@ -424,13 +432,13 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                         // transverse 2): cZ/(2Z) X (+ D)
                         const real S0 = TRN == 2 ? fma(cZh, X0, D0) : cZh * X0;
                         const real S1 = TRN == 2 ? fma(cZh, X1, D1) : cZh * X1;
-                        const real gS0 = gx * S0, dS0 = dx4 * S0, gS1 = gx * S1, dS1 = dx4 * S1;
-                        n00 = n00 + real(2) * gS0;
-                        n10 = n10 + real(2) * gS1;
-                        q3[0][0] = q2p[0][0] - gS0; q3[0][1] = q2p[0][1]; q3[0][2] = q2p[0][2] + dS0;
-                        q3[1][0] = q2p[1][0] - gS1; q3[1][1] = q2p[1][1]; q3[1][2] = q2p[1][2] + dS1;
-                        axp[0] = -gS0; axv[0] = -dS0;
-                        axp[1] = -gS1; axv[1] = -dS1;
+                        // split into rows t-1 (gamma, delta), t (-2 gamma) and t+1 (carried)
+                        n00 = fma(gx2, S0, n00);
+                        n10 = fma(gx2, S1, n10);
+                        q3[0][0] = fma(-gx, S0, q2p[0][0]); q3[0][1] = q2p[0][1]; q3[0][2] = fma(dx4, S0, q2p[0][2]);
+                        q3[1][0] = fma(-gx, S1, q2p[1][0]); q3[1][1] = q2p[1][1]; q3[1][2] = fma(dx4, S1, q2p[1][2]);
+                        sxp[0] = S0;
+                        sxp[1] = S1;
                     } else {
 #pragma unroll
                         for (int k = 0; k < 2; ++k)
@@ -441,7 +449,7 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                 }
 
                 // ---- y: interface t+1 raw, interface t limited, y-part of (c_k, t-1) ----
-                real hS[2], kS[2], o[2][3], Fpy[2], Svy[2], a1n[2], a2n[2];
+                real Sy[2], o[2][3], Fpy[2], Svy[2], a1n[2], a2n[2];
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const real dp = pn[k] - p[k], dv = vn[k] - v[k];
@@ -466,23 +474,21 @@ step2_char_kernel(const __grid_constant__ CharArgs<real> A) {
                         o[k][0] = o[k][0] - dtdy2 * Dy;
                         o[k][2] = o[k][2] - kvy * (Svy[k] - Svy_lo[k]);
                     }
-                    hS[k] = kS[k] = real(0);
+                    Sy[k] = real(0);
                     if constexpr (TRN > 0) {
-                        const real Sy = TRN == 2 ? fma(cZh, Y, Dy) : cZh * Y;
-                        hS[k] = gy * Sy;
-                        kS[k] = dy4 * Sy;
-                        o[k][0] = o[k][0] + real(2) * hS[k];
+                        Sy[k] = TRN == 2 ? fma(cZh, Y, Dy) : cZh * Y;
+                        o[k][0] = fma(gy2, Sy[k], o[k][0]);
                     }
                 }
                 if constexpr (TRN > 0) {
                     // transverse transfers: column c0 from c0-1 (lane-1's c1) and c1;
-                    // column c1 from c0 and c1+1 (lane+1's c0)
-                    const real hL = __shfl_up_sync(FULL, hS[1], 1), kL = __shfl_up_sync(FULL, kS[1], 1);
-                    const real hR = __shfl_down_sync(FULL, hS[0], 1), kR = __shfl_down_sync(FULL, kS[0], 1);
-                    o[0][0] = o[0][0] - hL - hS[1];
-                    o[0][1] = o[0][1] - kL + kS[1];
-                    o[1][0] = o[1][0] - hS[0] - hR;
-                    o[1][1] = o[1][1] - kS[0] + kR;
+                    // column c1 from c0 and c1+1 (lane+1's c0): -gamma S into p,
+                    // -+delta S into u
+                    const real SL = __shfl_up_sync(FULL, Sy[1], 1), SR = __shfl_down_sync(FULL, Sy[0], 1);
+                    o[0][0] = fma(-gy, SL + Sy[1], o[0][0]);
+                    o[0][1] = fma(dy4, Sy[1] - SL, o[0][1]);
+                    o[1][0] = fma(-gy, Sy[0] + SR, o[1][0]);
+                    o[1][1] = fma(dy4, SR - Sy[0], o[1][1]);
                 }
                 if (t - 1 >= r0) {
                     real* dst = qnew + (long long)(t - 1) * A.ld + c0;
